@@ -1,0 +1,357 @@
+"""Benchmark of the DSGD++ epoch on B200: SGD updates/s, HBM GB/s, roofline.
+
+One step = one DSGD++ epoch (2d sub-epochs over all training entries) of the
+100M-entry workload (2,000,000 x 500,000, Zipf(1.1) rows and columns, rank
+32, FP32 factors, Nzsl_L2(1) update, L2(0.05) regularize, d x 2d blocking).
+
+* value:   updates/s over K epochs, device time (CUDA events on the library's
+           stream), inputs resident in HBM;
+* e2e:     the same metric through the C ABI from pinned host buffers: the
+           training/test entries and the factors are uploaded and blocked, K
+           epochs each followed by the training and test loss read back to the
+           host, then the factors read back -- all inside the timed region;
+* roofline: the Hogwild sub-epoch kernel's algorithmic bytes per launch
+           (12 B entry + 4 r 4 B of factor rows/columns + 8 B inverse counts per
+           update) over its event-timed average launch duration;
+* cpu_baseline: the CPU restatement of the reference (oracle, threaded mode,
+           one thread per task, d = threads) timed on a 10M-entry sample.
+
+`--impl reference` times only the CPU restatement of the reference path (all
+host cores) on the same sample and prints its own line.
+Under torchrun every rank runs an independent replica of the job (the path is
+one GPU per job); value is the sum over ranks / the max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: m, n, nnz, nnz_test, rank, zipf s (rows, cols), d, noise
+    "c2": dict(m=2_000_000, n=500_000, nnz=100_000_000, nnz_test=1_000_000, rank=32,
+               s=1.1, d=64, noise=0.2,
+               text="2,000,000 x 500,000, 100M entries (+1M test), Zipf(1.1) rows and columns, "
+                    "rank 32, Nzsl_L2(1) update, L2(0.05) regularize, BoldDriver(0.001) first step"),
+    "c1": dict(m=100_000, n=100_000, nnz=1_000_000, nnz_test=100_000, rank=10, s=None, d=4,
+               noise=0.1,
+               text="100,000 x 100,000, 1M uniform entries (+100k test), rank 10, "
+                    "Nzsl_L2(1) update, no regularize"),
+}
+CPU_SAMPLE = 10_000_000
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                                      f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 3 + k and r[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def algorithmic_bytes_per_update(r, precision, update):
+    s_f = {"fp64": 8, "fp32": 4, "bf16": 2}[precision]
+    return 12 + 4 * r * s_f + (8 if update == "Nzsl_L2" else 0)
+
+
+def traffic_per_launch(name):
+    """DRAM bytes per launch of the Hogwild kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_launch_scaled:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+def cpu_sample(data, count, seed=1):
+    nnz = len(data["vals"])
+    k = min(count, nnz)
+    # the training entries are in random order already: a prefix is a uniform sample
+    return data["rows"][:k], data["cols"][:k], data["vals"][:k]
+
+
+def time_cpu_reference(data, wl, steps, warmup, threads=None):
+    """The oracle's threaded epoch (one thread per task, d = threads) on a sample."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
+    prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals)
+    prob.configure(update="Nzsl_L2", update_lambda=1.0,
+                   regularize="L2" if wl is WORKLOADS["c2"] else "None",
+                   regularize_lambda=0.05, loss="Nzsl_L2", loss_lambda=1.0)
+    prob.set_factors(data["W0"], data["H0"])
+    prob.seed(1)
+    times = []
+    for e in range(warmup + steps):
+        ns = prob.epoch(0.001, threads=threads)
+        if e >= warmup:
+            times.append(ns * 1e-9)
+    t = statistics.median(times)
+    return dict(value=len(vals) / t, unit="updates/s", cores=threads, kind="port",
+                sample=f"{len(vals):,} training entries of the workload (prefix of the random-order "
+                       f"entries), FP64, d={threads} tasks x {2 * threads} column blocks, "
+                       f"median of {steps} epochs", epoch_s=t)
+
+
+def generate(wl, seed):
+    import torch
+    from dsgdpp_b200 import synth_gpu
+    t0 = time.time()
+    data = synth_gpu.make(wl["m"], wl["n"], wl["nnz"], wl["nnz_test"], rank_true=wl["rank"],
+                          r=wl["rank"], noise=wl["noise"], seed=seed, s_row=wl["s"],
+                          s_col=wl["s"], device=f"cuda:{torch.cuda.current_device()}")
+    return data, time.time() - t0
+
+
+def pinned(a):
+    import torch
+    t = torch.from_numpy(a).pin_memory()
+    return t.numpy()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    import torch
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+
+
+def run_reference(args, world, rank, pg):
+    wl = WORKLOADS[args.workload]
+    if rank != 0:
+        return 0
+    data, _ = generate(wl, args.seed)
+    ref = time_cpu_reference(data, wl, args.steps, args.warmup)
+    line = {"metric": "SGD updates/s (DSGD++ epoch)", "value": ref["value"], "unit": "updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ref["epoch_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": wl["text"] + f"; CPU sample of {CPU_SAMPLE:,} entries"},
+            "impl": "reference",
+            "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": ref["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--d", type=int, default=0)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "fp64"])
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--vecs", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
+
+    import dsgdpp_b200 as P
+    wl = WORKLOADS[args.workload]
+    d = args.d or wl["d"]
+    data, gen_s = generate(wl, args.seed + rank)
+    l2 = args.workload == "c2"
+    cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=args.precision,
+                   exec="hogwild", launch="graph", update="Nzsl_L2", update_lambda=1.0,
+                   regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,
+                   loss="Nzsl_L2", loss_lambda=1.0, lanes_per_nnz=args.lanes,
+                   vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local)
+    host = {k: pinned(np.ascontiguousarray(v)) for k, v in data.items()}
+    ctx = P.Context(cfg)
+    t0 = time.time()
+    ctx.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
+    ctx.set_matrix(P.TEST, host["trows"], host["tcols"], host["tvals"])
+    ctx.set_factors(host["W0"], host["H0"])
+    setup_s = time.time() - t0
+    nnz = int(ctx.block_nnz(P.TRAIN).sum())
+    lanes, vecs, grid = ctx.launch_shape()
+    ctx.seed(args.seed)
+    eps = 0.001
+
+    # ---- device-timed epochs (value) ----
+    for _ in range(args.warmup):
+        ctx.epoch(eps)
+    ctx.sync()
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev_ms = []
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.epoch(eps)
+        dev_ms.append(ctx.last_epoch_ms())
+    ctx.sync()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    barrier(pg)
+    t_dev = allreduce_max(pg, sum(dev_ms) / 1e3)
+    value = nnz * args.steps * world / t_dev
+
+    # ---- per-kernel timing of the sub-epoch kernel (roofline) ----
+    ctx.set_kernel_timing(True)
+    for _ in range(2):
+        ctx.epoch(eps)
+    k_ms, k_launches = ctx.kernel_timing()
+    ctx.set_kernel_timing(False)
+    bpu = algorithmic_bytes_per_update(wl["rank"], args.precision, "Nzsl_L2")
+    bytes_per_launch = nnz * bpu / (2 * d)
+    avg_launch_s = k_ms / 1e3 / max(k_launches, 1)
+    hbm, peak_kind = peaks()
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    traffic = traffic_per_launch(f"hogwild_subepoch_{args.workload}.md")
+
+    # ---- end to end through the C ABI from pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        barrier(pg)
+        t0 = time.perf_counter()
+        ctx.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
+        ctx.set_matrix(P.TEST, host["trows"], host["tcols"], host["tvals"])
+        ctx.set_factors(host["W0"], host["H0"])
+        losses = []
+        for _ in range(args.steps):
+            ctx.epoch(eps)
+            losses.append((ctx.loss(), ctx.nzsl(P.TEST)))
+        W, H = ctx.get_factors()
+        t_e2e = time.perf_counter() - t0
+        t_e2e = allreduce_max(pg, t_e2e)
+        h2d = (16 * (len(host["vals"]) + len(host["tvals"])) + 8 * (wl["m"] + wl["n"]) * wl["rank"]
+               + args.steps * (2 * d * d * 4 + 24))
+        d2h = 8 * (wl["m"] + wl["n"]) * wl["rank"] + args.steps * 16
+        e2e = {"value": nnz * args.steps * world / t_e2e, "unit": "updates/s",
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+               "seconds": t_e2e, "final_test_rmse": float(np.sqrt(losses[-1][1] / len(host["tvals"])))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = time_cpu_reference(data, wl, steps=2, warmup=0)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": "SGD updates/s (DSGD++ epoch)", "value": value, "unit": "updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": wl["text"], "d": d, "blocks": f"{d} x {2 * d}",
+                       "nnz": nnz, "precision": args.precision, "exec": "hogwild",
+                       "launch": "graph", "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
+                       "grid": grid, "parallelism": f"replicas x{world}",
+                       "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "bytes_per_update": bpu, "kernel": "hogwild_subepoch_kernel",
+                         "avg_launch_us": avg_launch_s * 1e6},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * (2 * d + 1 + (1 if l2 else 0)),
+            "clocks": clk,
+            "wall_s_timed": wall, "setup_s": setup_s, "generate_s": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        barrier(pg)
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

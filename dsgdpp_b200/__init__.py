@@ -1,0 +1,379 @@
+"""Python binding of the B200 DSGD++ library (C ABI in include/dsgdpp.h).
+
+The compute path is the CUDA library ``dsgdpp_b200/lib/libdsgdpp_b200.so``;
+this module only marshals arguments through ctypes.  There is no CPU
+fallback: if the library is missing, importing the binding raises, and if no
+GPU is present, :class:`Context` creation fails with ``DsgdppError``.
+
+The classes mirror the reference's C++ entry points:
+
+* :class:`Context` -- a ``DsgdPpJob`` plus ``DsgdPpRunner`` bound to one GPU
+  (mf/sgd/dsgdpp.h:38-134): ``epoch`` is ``DsgdPpRunner::epoch``, ``run`` is
+  ``detail::defaultRunner`` (mf/sgd/sgd_impl.h:34-145), ``loss``/``nzsl``/
+  ``l2``/``nzl2`` are the losses of mf/loss.
+* :class:`Random32`, :func:`draw_schedule`, :func:`dsgd_schedule`,
+  :func:`point_orders`, :func:`block_offsets` -- host-side random draws and
+  blocking (mf/sgd/dsgdpp_impl.h:282-349, mf/sgd/dsgd_impl.h:246-325,
+  mf/sgd/sgd_impl.h:197-351, mf/matrix/distributed_matrix_impl.cc:24-40).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libdsgdpp_b200.so")
+
+# constants of include/dsgdpp.h
+OK = 0
+E_INVALID, E_CUDA, E_IO, E_UNSUPPORTED, E_STATE, E_NOMEM = -1, -2, -3, -4, -5, -6
+UPDATE = {"Nzsl": 0, "Nzsl_L2": 1, "Nzsl_Nzl2": 2}
+REGULARIZE = {"None": 0, "L2": 1}
+LOSS = {"Nzsl": 0, "Nzsl_L2": 1, "Nzsl_Nzl2": 2}
+SGD_ORDER = {"SEQ": 0, "WR": 1, "WOR": 2}
+STRATUM_ORDER = {"SEQ": 0, "RSEQ": 1, "WR": 2, "WOR": 3, "COWOR": 4}
+PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
+EXEC = {"replay": 0, "hogwild": 1}
+LAUNCH = {"stream": 0, "graph": 1}
+TRAIN, TEST = 0, 1
+DECAY = {"Const": 0, "BoldDriver": 1}
+
+
+class DsgdppError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class _Config(C.Structure):
+    _fields_ = [
+        ("m", C.c_uint64), ("n", C.c_uint64), ("rank", C.c_uint32), ("d", C.c_uint32),
+        ("precision", C.c_int32), ("exec", C.c_int32), ("launch", C.c_int32),
+        ("update", C.c_int32), ("update_lambda", C.c_double),
+        ("regularize", C.c_int32), ("regularize_lambda", C.c_double),
+        ("loss", C.c_int32), ("loss_lambda", C.c_double),
+        ("truncate", C.c_int32), ("truncate_min", C.c_double), ("truncate_max", C.c_double),
+        ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
+        ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
+        ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64),
+    ]
+
+
+class _TraceRow(C.Structure):
+    _fields_ = [
+        ("epoch", C.c_uint64), ("loss", C.c_double), ("test_loss", C.c_double),
+        ("eps", C.c_double), ("time_eps", C.c_double), ("time_epoch", C.c_double),
+        ("time_loss", C.c_double), ("time_test_loss", C.c_double),
+    ]
+
+
+_P = C.c_void_p
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_f64p = C.POINTER(C.c_double)
+
+# every symbol of include/dsgdpp.h with its ctypes signature
+SIGNATURES = {
+    "dsgdpp_config_init": (None, [C.POINTER(_Config)]),
+    "dsgdpp_create": (C.c_int, [C.POINTER(_Config), C.POINTER(_P)]),
+    "dsgdpp_create_error": (C.c_char_p, []),
+    "dsgdpp_destroy": (None, [_P]),
+    "dsgdpp_last_error": (C.c_char_p, [_P]),
+    "dsgdpp_status_string": (C.c_char_p, [C.c_int]),
+    "dsgdpp_abi_version": (C.c_int, []),
+    "dsgdpp_set_matrix": (C.c_int, [_P, C.c_int, C.c_uint64, _u32p, _u32p, _f64p]),
+    "dsgdpp_set_factors": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_get_factors": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_block_nnz": (C.c_int, [_P, C.c_int, _u64p]),
+    "dsgdpp_nnz12": (C.c_int, [_P, _u64p, _u64p, _u64p]),
+    "dsgdpp_seed": (C.c_int, [_P, C.c_uint32]),
+    "dsgdpp_epoch": (C.c_int, [_P, C.c_double]),
+    "dsgdpp_epoch_explicit": (C.c_int, [_P, C.c_double, _u32p, _u32p]),
+    "dsgdpp_last_epoch_ms": (C.c_int, [_P, _f64p]),
+    "dsgdpp_set_kernel_timing": (C.c_int, [_P, C.c_int]),
+    "dsgdpp_kernel_timing": (C.c_int, [_P, _f64p, _u64p]),
+    "dsgdpp_launch_shape": (C.c_int, [_P, _u32p, _u32p, _u32p]),
+    "dsgdpp_loss": (C.c_int, [_P, _f64p]),
+    "dsgdpp_nzsl": (C.c_int, [_P, C.c_int, _f64p]),
+    "dsgdpp_l2": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_nzl2": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_run": (C.c_int, [_P, C.c_uint32, C.c_int, C.c_double, C.c_double, C.c_double,
+                             C.POINTER(_TraceRow)]),
+    "dsgdpp_sync": (C.c_int, [_P]),
+    "dsgdpp_rng_create": (_P, [C.c_uint32]),
+    "dsgdpp_rng_destroy": (None, [_P]),
+    "dsgdpp_rng_next": (C.c_uint32, [_P]),
+    "dsgdpp_rng_next_int": (C.c_uint32, [_P, C.c_uint32]),
+    "dsgdpp_draw_schedule": (None, [_P, C.c_uint32, C.c_int, _u32p, _u32p]),
+    "dsgdpp_dsgd_schedule": (None, [_P, C.c_uint32, C.c_uint32, C.c_int, _u32p]),
+    "dsgdpp_point_orders": (C.c_uint64, [C.c_uint32, C.c_int, _u64p, _u32p, _u32p, _u32p]),
+    "dsgdpp_block_offsets": (None, [C.c_uint64, C.c_uint32, _u64p]),
+    "dsgdpp_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
+}
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; "
+            f"g.build()'` (make -C dsgdpp_b200/csrc)")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(a: Optional[np.ndarray], ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+@dataclass
+class Config:
+    """dsgdpp_config with the reference defaults (tools/mfdsgdpp.cc:429-441)."""
+    m: int
+    n: int
+    rank: int
+    d: int
+    precision: str = "fp32"
+    exec: str = "hogwild"
+    launch: str = "graph"
+    update: str = "Nzsl_L2"
+    update_lambda: float = 1.0
+    regularize: str = "None"
+    regularize_lambda: float = 0.0
+    loss: str = "Nzsl_L2"
+    loss_lambda: float = 1.0
+    truncate: Optional[tuple] = None
+    sgd_order: str = "WOR"
+    stratum_order: str = "COWOR"
+    device: int = 0
+    lanes_per_nnz: int = 0
+    vecs_per_lane: int = 0
+    ctas_per_sm: int = 0
+    layout_seed: int = 0x5EED5EED
+
+    def to_c(self) -> _Config:
+        c = _Config()
+        lib.dsgdpp_config_init(C.byref(c))
+        c.m, c.n, c.rank, c.d = self.m, self.n, self.rank, self.d
+        c.precision = PRECISION[self.precision]
+        c.exec = EXEC[self.exec]
+        c.launch = LAUNCH[self.launch]
+        c.update, c.update_lambda = UPDATE[self.update], self.update_lambda
+        c.regularize, c.regularize_lambda = REGULARIZE[self.regularize], self.regularize_lambda
+        c.loss, c.loss_lambda = LOSS[self.loss], self.loss_lambda
+        if self.truncate is not None:
+            c.truncate, c.truncate_min, c.truncate_max = 1, self.truncate[0], self.truncate[1]
+        c.sgd_order = SGD_ORDER[self.sgd_order]
+        c.stratum_order = STRATUM_ORDER[self.stratum_order]
+        c.device = self.device
+        c.lanes_per_nnz, c.vecs_per_lane = self.lanes_per_nnz, self.vecs_per_lane
+        c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
+        return c
+
+
+class Context:
+    """One DSGD++ job on one GPU (DsgdPpJob + DsgdPpRunner)."""
+
+    def __init__(self, config: Config):
+        self.config = config
+        self._cfg = config.to_c()
+        h = _P()
+        rc = lib.dsgdpp_create(C.byref(self._cfg), C.byref(h))
+        if rc != OK:
+            raise DsgdppError(rc, "dsgdpp_create: " + lib.dsgdpp_create_error().decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise DsgdppError(rc, f"{what}: {lib.dsgdpp_last_error(self._h).decode()}")
+
+    # data -------------------------------------------------------------------
+    def set_matrix(self, which: int, rows, cols, vals):
+        r, c, v = _u32(rows), _u32(cols), _f64(vals)
+        if not (len(r) == len(c) == len(v)):
+            raise ValueError("rows, cols and vals differ in length")
+        self._check(lib.dsgdpp_set_matrix(self._h, which, len(v), _ptr(r, C.c_uint32),
+                                          _ptr(c, C.c_uint32), _ptr(v, C.c_double)),
+                    "set_matrix")
+
+    def set_factors(self, W, H):
+        """W: m x r row-major; H: r x n column-major, passed as its n x r transpose."""
+        w, h = _f64(W), _f64(H)
+        self._check(lib.dsgdpp_set_factors(self._h, _ptr(w, C.c_double), _ptr(h, C.c_double)),
+                    "set_factors")
+
+    def get_factors(self):
+        w = np.empty((self.config.m, self.config.rank), np.float64)
+        h = np.empty((self.config.n, self.config.rank), np.float64)
+        self._check(lib.dsgdpp_get_factors(self._h, _ptr(w, C.c_double), _ptr(h, C.c_double)),
+                    "get_factors")
+        return w, h
+
+    def block_nnz(self, which: int = TRAIN) -> np.ndarray:
+        out = np.empty(2 * self.config.d * self.config.d, np.uint64)
+        self._check(lib.dsgdpp_block_nnz(self._h, which, _ptr(out, C.c_uint64)), "block_nnz")
+        return out.reshape(self.config.d, 2 * self.config.d)
+
+    def nnz12(self):
+        a = np.empty(self.config.m, np.uint64)
+        b = np.empty(self.config.n, np.uint64)
+        mx = C.c_uint64()
+        self._check(lib.dsgdpp_nnz12(self._h, _ptr(a, C.c_uint64), _ptr(b, C.c_uint64),
+                                     C.byref(mx)), "nnz12")
+        return a, b, mx.value
+
+    # epochs -----------------------------------------------------------------
+    def seed(self, seed: int):
+        self._check(lib.dsgdpp_seed(self._h, seed & 0xFFFFFFFF), "seed")
+
+    def epoch(self, eps: float):
+        self._check(lib.dsgdpp_epoch(self._h, eps), "epoch")
+
+    def epoch_explicit(self, eps: float, schedule, task_seeds):
+        s, t = _u32(schedule), _u32(task_seeds)
+        self._check(lib.dsgdpp_epoch_explicit(self._h, eps, _ptr(s, C.c_uint32),
+                                              _ptr(t, C.c_uint32)), "epoch_explicit")
+
+    def last_epoch_ms(self) -> float:
+        v = C.c_double()
+        self._check(lib.dsgdpp_last_epoch_ms(self._h, C.byref(v)), "last_epoch_ms")
+        return v.value
+
+    def set_kernel_timing(self, on: bool):
+        self._check(lib.dsgdpp_set_kernel_timing(self._h, int(on)), "set_kernel_timing")
+
+    def kernel_timing(self):
+        ms, n = C.c_double(), C.c_uint64()
+        self._check(lib.dsgdpp_kernel_timing(self._h, C.byref(ms), C.byref(n)), "kernel_timing")
+        return ms.value, n.value
+
+    def launch_shape(self):
+        a, b, g = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(lib.dsgdpp_launch_shape(self._h, C.byref(a), C.byref(b), C.byref(g)),
+                    "launch_shape")
+        return a.value, b.value, g.value
+
+    def sync(self):
+        self._check(lib.dsgdpp_sync(self._h), "sync")
+
+    # losses -----------------------------------------------------------------
+    def loss(self) -> float:
+        v = C.c_double()
+        self._check(lib.dsgdpp_loss(self._h, C.byref(v)), "loss")
+        return v.value
+
+    def nzsl(self, which: int = TRAIN) -> float:
+        v = C.c_double()
+        self._check(lib.dsgdpp_nzsl(self._h, which, C.byref(v)), "nzsl")
+        return v.value
+
+    def l2(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(lib.dsgdpp_l2(self._h, C.byref(a), C.byref(b)), "l2")
+        return a.value, b.value
+
+    def nzl2(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(lib.dsgdpp_nzl2(self._h, C.byref(a), C.byref(b)), "nzl2")
+        return a.value, b.value
+
+    def run(self, epochs: int, decay: str = "BoldDriver", eps0: float = 0.001,
+            decrease: float = 0.5, increase: float = 1.05):
+        rows = (_TraceRow * (epochs + 1))()
+        self._check(lib.dsgdpp_run(self._h, epochs, DECAY[decay], eps0, decrease, increase,
+                                   rows), "run")
+        return [dict(epoch=r.epoch, loss=r.loss, test_loss=r.test_loss, eps=r.eps,
+                     time_eps=r.time_eps, time_epoch=r.time_epoch, time_loss=r.time_loss,
+                     time_test_loss=r.time_test_loss) for r in rows]
+
+
+# ---- host utilities ---------------------------------------------------------
+class Random32:
+    """rg::Random32 as pinned by the library (MT19937, Boost bucket nextInt)."""
+
+    def __init__(self, seed: int):
+        self._h = lib.dsgdpp_rng_create(seed & 0xFFFFFFFF)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_rng_destroy(self._h)
+            self._h = None
+
+    def next(self) -> int:
+        return lib.dsgdpp_rng_next(self._h)
+
+    def next_int(self, n: int) -> int:
+        return lib.dsgdpp_rng_next_int(self._h, n)
+
+
+def draw_schedule(rng: Random32, d: int, stratum_order: str = "COWOR"):
+    """DsgdPpRunner::epoch draws: (2d x d schedule, d task seeds)."""
+    s = np.empty((2 * d, d), np.uint32)
+    t = np.empty(d, np.uint32)
+    lib.dsgdpp_draw_schedule(rng._h, d, STRATUM_ORDER[stratum_order], _ptr(s, C.c_uint32),
+                             _ptr(t, C.c_uint32))
+    return s, t
+
+
+def dsgd_schedule(rng: Random32, w: int, t: int, stratum_order: str) -> np.ndarray:
+    out = np.empty((w * t, w * t), np.uint32)
+    lib.dsgdpp_dsgd_schedule(rng._h, w, t, STRATUM_ORDER[stratum_order], _ptr(out, C.c_uint32))
+    return out
+
+
+def point_orders(d: int, sgd_order: str, block_nnz, schedule, task_seeds) -> np.ndarray:
+    bn = np.ascontiguousarray(block_nnz, dtype=np.uint64).ravel()
+    s, t = _u32(schedule), _u32(task_seeds)
+    total = lib.dsgdpp_point_orders(d, SGD_ORDER[sgd_order], _ptr(bn, C.c_uint64),
+                                    _ptr(s, C.c_uint32), _ptr(t, C.c_uint32), None)
+    out = np.empty(total, np.uint32)
+    lib.dsgdpp_point_orders(d, SGD_ORDER[sgd_order], _ptr(bn, C.c_uint64), _ptr(s, C.c_uint32),
+                            _ptr(t, C.c_uint32), _ptr(out, C.c_uint32))
+    return out
+
+
+def block_offsets(size: int, blocks: int) -> np.ndarray:
+    out = np.empty(blocks, np.uint64)
+    lib.dsgdpp_block_offsets(size, blocks, _ptr(out, C.c_uint64))
+    return out
+
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    c, k = _u32(ctr), _u32(key)
+    out = np.empty(4, np.uint32)
+    lib.dsgdpp_philox4x32_10(_ptr(c, C.c_uint32), _ptr(k, C.c_uint32), _ptr(out, C.c_uint32))
+    return out

@@ -1,0 +1,1089 @@
+// capi.cu -- the C ABI of include/dsgdpp.h: context, data upload, epochs,
+// losses and the defaultRunner loop.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/dsgdpp.h"
+#include "kernels.cuh"
+#include "schedule.h"
+
+using namespace dsgdpp;
+
+namespace {
+
+struct DevMatrix {
+  bool present = false;
+  uint64_t nnz = 0;
+  uint32_t* row = nullptr;
+  uint32_t* col = nullptr;
+  void* val = nullptr;
+  uint64_t* block_ptr = nullptr;
+  std::vector<uint64_t> h_block_ptr;
+};
+
+class Error {
+ public:
+  Error(int code, std::string msg) : code(code), msg(std::move(msg)) {}
+  int code;
+  std::string msg;
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw Error(e == cudaErrorMemoryAllocation ? DSGDPP_E_NOMEM : DSGDPP_E_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T* dalloc(size_t count, const char* what) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  check_cuda(cudaMalloc(&p, count * sizeof(T)), what);
+  return static_cast<T*>(p);
+}
+template <typename T>
+T* halloc(size_t count, const char* what) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  check_cuda(cudaMallocHost(&p, count * sizeof(T)), what);
+  return static_cast<T*>(p);
+}
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+template <typename T>
+void hfree(T*& p) {
+  if (p) cudaFreeHost((void*)p);
+  p = nullptr;
+}
+
+uint32_t vec_width(int precision) { return precision == kFp64 ? 2 : (precision == kFp32 ? 4 : 8); }
+size_t elem_size(int precision) { return precision == kFp64 ? 8 : (precision == kFp32 ? 4 : 2); }
+
+}  // namespace
+
+struct dsgdpp_ctx {
+  dsgdpp_config cfg{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  uint32_t d = 0, r = 0, rp = 0;
+  std::vector<uint64_t> off1, off2;  // with the end offset appended
+  uint64_t* d_off1 = nullptr;
+  uint64_t* d_off2 = nullptr;
+  DevMatrix mat[2];
+  void* W = nullptr;
+  void* H = nullptr;
+  bool factors_set = false;
+  uint32_t* cnt1 = nullptr;
+  uint32_t* cnt2 = nullptr;
+  void* inv1 = nullptr;
+  void* inv2 = nullptr;
+  double* staging = nullptr;  // (m + n) * r doubles, factor upload / download
+  // per-epoch inputs (pinned host copies feed the device copies)
+  uint32_t* h_schedule = nullptr;
+  uint32_t* d_schedule = nullptr;
+  EpochParams* h_params = nullptr;
+  EpochParams* d_params = nullptr;
+  float* h_sigma = nullptr;   // [2d][d][3]
+  float* d_sigma = nullptr;
+  float* h_scales = nullptr;  // [2d + 1]
+  float* d_scales = nullptr;
+  Segment* d_segs = nullptr;
+  uint32_t* d_counters = nullptr;
+  // replay
+  uint32_t* h_positions = nullptr;
+  uint32_t* d_positions = nullptr;
+  uint64_t positions_cap = 0;
+  uint64_t* h_pos_offset = nullptr;
+  uint64_t* d_pos_offset = nullptr;
+  uint8_t* h_mask = nullptr;  // [2d][2d]
+  uint8_t* d_mask = nullptr;
+  // losses
+  double* d_partials = nullptr;
+  double* d_out = nullptr;
+  double* h_out = nullptr;
+  uint32_t loss_grid = 0;
+  // Hogwild launch shape
+  uint32_t lanes = 0, vecs = 0, grid = 0;
+  // graph of one Hogwild epoch
+  cudaGraphExec_t graph_exec = nullptr;
+  // timing / ordering
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_inputs = nullptr;
+  bool epoch_timed = false;
+  // per-kernel timing of the Hogwild sub-epoch kernels (stream launch only)
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;  // 2d + 1 events around the sub-epoch kernels
+  double prof_ms = 0;                // summed sub-epoch kernel time of profiled epochs
+  uint64_t prof_launches = 0;
+  bool prof_pending = false;
+  Random32 master{0};
+  uint32_t epoch_counter = 0;
+};
+
+namespace {
+
+template <typename F>
+int guarded(dsgdpp_ctx* ctx, F&& f) {
+  if (!ctx) return DSGDPP_E_INVALID;
+  try {
+    ctx->err.clear();
+    return f();
+  } catch (const Error& e) {
+    ctx->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    ctx->err = "host allocation failed";
+    return DSGDPP_E_NOMEM;
+  }
+}
+
+void release_graph(dsgdpp_ctx* c) {
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  c->graph_exec = nullptr;
+}
+
+void choose_hogwild_shape(dsgdpp_ctx* c) {
+  const uint32_t nvec = c->rp / vec_width(c->cfg.precision);
+  uint32_t lanes = c->cfg.lanes_per_nnz, vecs = c->cfg.vecs_per_lane;
+  if (lanes == 0) {
+    lanes = 2;
+    while (lanes < nvec && lanes < 32) lanes <<= 1;
+  }
+  if (vecs == 0) vecs = (nvec + lanes - 1) / lanes;
+  if (vecs == 3) vecs = 4;
+  c->lanes = lanes;
+  c->vecs = vecs;
+  if ((uint64_t)lanes * vecs < nvec)
+    throw Error(DSGDPP_E_INVALID, "lanes_per_nnz x vecs_per_lane does not cover the rank");
+  int per_sm = hogwild_ctas_per_sm(c->cfg.precision, lanes, vecs, c->d);
+  if (per_sm <= 0)
+    throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
+                                      ", vecs_per_lane=" + std::to_string(vecs));
+  if (c->cfg.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm);
+  c->grid = (uint32_t)(per_sm * c->num_sms);
+}
+
+void validate_config(const dsgdpp_config* c) {
+  if (!c) throw Error(DSGDPP_E_INVALID, "config is null");
+  if (c->m == 0 || c->n == 0) throw Error(DSGDPP_E_INVALID, "m and n must be positive");
+  if (c->m > 0xFFFFFFFFull || c->n > 0xFFFFFFFFull)
+    throw Error(DSGDPP_E_INVALID, "m and n must fit in 32 bits");
+  if (c->d < 1 || c->d > 1024) throw Error(DSGDPP_E_INVALID, "d must be in [1, 1024]");
+  if ((uint64_t)2 * c->d > c->n || c->d > c->m)
+    throw Error(DSGDPP_E_INVALID, "the d x 2d blocking needs m >= d and n >= 2d");
+  if (c->rank < 1) throw Error(DSGDPP_E_INVALID, "rank must be positive");
+  if (c->precision < 0 || c->precision > 2) throw Error(DSGDPP_E_INVALID, "unknown precision");
+  if (c->exec != DSGDPP_EXEC_REPLAY && c->exec != DSGDPP_EXEC_HOGWILD)
+    throw Error(DSGDPP_E_INVALID, "unknown exec mode");
+  if (c->exec == DSGDPP_EXEC_REPLAY && c->precision != DSGDPP_FP64)
+    throw Error(DSGDPP_E_UNSUPPORTED, "replay mode runs FP64 factors only");
+  if (c->exec == DSGDPP_EXEC_REPLAY && c->rank > 256)
+    throw Error(DSGDPP_E_UNSUPPORTED, "replay mode supports rank <= 256");
+  if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
+    throw Error(DSGDPP_E_INVALID, "unknown launch form");
+  if (c->update < 0 || c->update > 2) throw Error(DSGDPP_E_INVALID, "unknown update");
+  if (c->regularize < 0 || c->regularize > 1) throw Error(DSGDPP_E_INVALID, "unknown regularize");
+  if (c->loss < 0 || c->loss > 2) throw Error(DSGDPP_E_INVALID, "unknown loss");
+  if (c->sgd_order < 0 || c->sgd_order > 2) throw Error(DSGDPP_E_INVALID, "unknown sgd order");
+  if (c->stratum_order < 0 || c->stratum_order > 4)
+    throw Error(DSGDPP_E_INVALID, "unknown stratum order");
+  if (c->truncate && c->regularize == DSGDPP_REGULARIZE_L2 && c->exec == DSGDPP_EXEC_HOGWILD)
+    throw Error(DSGDPP_E_UNSUPPORTED, "truncation with L2 regularization needs replay mode");
+  const uint64_t vw = vec_width(c->precision);
+  if ((c->rank + vw - 1) / vw > 128) throw Error(DSGDPP_E_UNSUPPORTED, "rank too large");
+}
+
+void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
+  validate_config(cfg);
+  c->cfg = *cfg;
+  int ndev = 0;
+  check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (cfg->device < 0 || cfg->device >= ndev) throw Error(DSGDPP_E_CUDA, "no such CUDA device");
+  check_cuda(cudaSetDevice(cfg->device), "cudaSetDevice");
+  check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg->device),
+             "cudaDeviceGetAttribute");
+  c->d = cfg->d;
+  c->r = cfg->rank;
+  const uint32_t vw = vec_width(cfg->precision);
+  c->rp = (c->r + vw - 1) / vw * vw;
+  const uint32_t d = c->d, d2 = 2 * d;
+  c->off1 = block_offsets(cfg->m, d);
+  c->off1.push_back(cfg->m);
+  c->off2 = block_offsets(cfg->n, d2);
+  c->off2.push_back(cfg->n);
+  c->d_off1 = dalloc<uint64_t>(d + 1, "off1");
+  c->d_off2 = dalloc<uint64_t>(d2 + 1, "off2");
+  check_cuda(cudaMemcpy(c->d_off1, c->off1.data(), (d + 1) * 8, cudaMemcpyHostToDevice), "off1");
+  check_cuda(cudaMemcpy(c->d_off2, c->off2.data(), (d2 + 1) * 8, cudaMemcpyHostToDevice), "off2");
+  const size_t es = elem_size(cfg->precision);
+  check_cuda(cudaMalloc(&c->W, cfg->m * c->rp * es), "W");
+  check_cuda(cudaMalloc(&c->H, cfg->n * c->rp * es), "H");
+  check_cuda(cudaMemset(c->W, 0, cfg->m * c->rp * es), "W");
+  check_cuda(cudaMemset(c->H, 0, cfg->n * c->rp * es), "H");
+  c->cnt1 = dalloc<uint32_t>(cfg->m, "cnt1");
+  c->cnt2 = dalloc<uint32_t>(cfg->n, "cnt2");
+  check_cuda(cudaMemset(c->cnt1, 0, cfg->m * 4), "cnt1");
+  check_cuda(cudaMemset(c->cnt2, 0, cfg->n * 4), "cnt2");
+  if (cfg->exec == DSGDPP_EXEC_HOGWILD) {
+    const size_t cs = cfg->precision == kFp64 ? 8 : 4;
+    check_cuda(cudaMalloc(&c->inv1, cfg->m * cs), "inv1");
+    check_cuda(cudaMalloc(&c->inv2, cfg->n * cs), "inv2");
+  }
+  c->h_schedule = halloc<uint32_t>((size_t)d2 * d, "schedule");
+  c->d_schedule = dalloc<uint32_t>((size_t)d2 * d, "schedule");
+  c->h_params = halloc<EpochParams>(1, "params");
+  c->d_params = dalloc<EpochParams>(1, "params");
+  c->h_sigma = halloc<float>((size_t)d2 * d * 3, "sigma");
+  c->d_sigma = dalloc<float>((size_t)d2 * d * 3, "sigma");
+  c->h_scales = halloc<float>(d2 + 1, "scales");
+  c->d_scales = dalloc<float>(d2 + 1, "scales");
+  c->d_segs = dalloc<Segment>((size_t)d2 * (d + 1), "segments");
+  c->d_counters = dalloc<uint32_t>(d2, "counters");
+  c->h_pos_offset = halloc<uint64_t>((size_t)d2 * d + 1, "pos_offset");
+  c->d_pos_offset = dalloc<uint64_t>((size_t)d2 * d + 1, "pos_offset");
+  c->h_mask = halloc<uint8_t>((size_t)d2 * d2, "mask");
+  c->d_mask = dalloc<uint8_t>((size_t)d2 * d2, "mask");
+  c->loss_grid = (uint32_t)c->num_sms * 4;
+  c->d_partials = dalloc<double>(c->loss_grid, "partials");
+  c->d_out = dalloc<double>(4, "loss out");
+  c->h_out = halloc<double>(4, "loss out");
+  check_cuda(cudaEventCreate(&c->ev_begin), "event");
+  check_cuda(cudaEventCreate(&c->ev_end), "event");
+  check_cuda(cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming), "event");
+  check_cuda(cudaEventRecord(c->ev_inputs, c->stream), "event");
+  if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
+}
+
+void destroy_impl(dsgdpp_ctx* c) {
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  release_graph(c);
+  for (auto& m : c->mat) {
+    dfree(m.row); dfree(m.col); dfree(m.val); dfree(m.block_ptr);
+  }
+  dfree(c->d_off1); dfree(c->d_off2);
+  dfree(c->W); dfree(c->H); dfree(c->cnt1); dfree(c->cnt2); dfree(c->inv1); dfree(c->inv2);
+  dfree(c->staging);
+  hfree(c->h_schedule); dfree(c->d_schedule); hfree(c->h_params); dfree(c->d_params);
+  hfree(c->h_sigma); dfree(c->d_sigma); hfree(c->h_scales); dfree(c->d_scales);
+  dfree(c->d_segs); dfree(c->d_counters);
+  hfree(c->h_positions); dfree(c->d_positions); hfree(c->h_pos_offset); dfree(c->d_pos_offset);
+  hfree(c->h_mask); dfree(c->d_mask);
+  dfree(c->d_partials); dfree(c->d_out); hfree(c->h_out);
+  for (auto e : c->prof_ev) cudaEventDestroy(e);
+  c->prof_ev.clear();
+  if (c->ev_begin) cudaEventDestroy(c->ev_begin);
+  if (c->ev_end) cudaEventDestroy(c->ev_end);
+  if (c->ev_inputs) cudaEventDestroy(c->ev_inputs);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+// ---- blocking on the GPU ----------------------------------------------------------
+int bit_length(uint64_t v) {
+  int b = 0;
+  while (v) { ++b; v >>= 1; }
+  return b;
+}
+
+void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* rows,
+                     const uint32_t* cols, const double* vals) {
+  if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
+  if (nnz > 0 && (!rows || !cols || !vals)) throw Error(DSGDPP_E_INVALID, "null input array");
+  if (nnz >= 0x7FFFFFFFull) throw Error(DSGDPP_E_UNSUPPORTED, "nnz must be below 2^31");
+  check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+  check_cuda(cudaStreamSynchronize(c->stream), "sync");
+  release_graph(c);
+  cudaStream_t st = c->stream;
+  const uint32_t d = c->d, d2 = 2 * d, nblocks = d * d2;
+  uint64_t mB = 0, nB = 0;
+  for (uint32_t b = 0; b < d; ++b) mB = std::max(mB, c->off1[b + 1] - c->off1[b]);
+  for (uint32_t b = 0; b < d2; ++b) nB = std::max(nB, c->off2[b + 1] - c->off2[b]);
+  const uint64_t span = mB * nB;
+  if (span == 0 || (double)nblocks * (double)span >= 1.8e19)
+    throw Error(DSGDPP_E_UNSUPPORTED, "m x n too large for the 64-bit block key");
+  const bool as_double = c->cfg.precision == kFp64;
+  const bool shuffled = which == DSGDPP_TRAIN && c->cfg.exec == DSGDPP_EXEC_HOGWILD;
+
+  DevMatrix& M = c->mat[which];
+  dfree(M.row); dfree(M.col); dfree(M.val); dfree(M.block_ptr);
+  M.present = false;
+  M.nnz = 0;
+  M.block_ptr = dalloc<uint64_t>(nblocks + 1, "block_ptr");
+  M.h_block_ptr.assign(nblocks + 1, 0);
+  if (nnz == 0) {
+    check_cuda(cudaMemset(M.block_ptr, 0, (nblocks + 1) * 8), "block_ptr");
+    M.row = dalloc<uint32_t>(1, "row");
+    M.col = dalloc<uint32_t>(1, "col");
+    check_cuda(cudaMalloc(&M.val, 8), "val");
+    M.present = true;
+    if (which == DSGDPP_TRAIN) {
+      check_cuda(cudaMemset(c->cnt1, 0, c->cfg.m * 4), "cnt1");
+      check_cuda(cudaMemset(c->cnt2, 0, c->cfg.n * 4), "cnt2");
+    }
+    return;
+  }
+
+  uint32_t* t_rows = dalloc<uint32_t>(nnz, "rows");
+  uint32_t* t_cols = dalloc<uint32_t>(nnz, "cols");
+  double* t_vals = dalloc<double>(nnz, "vals");
+  uint64_t* keys[2] = {dalloc<uint64_t>(nnz, "keys"), dalloc<uint64_t>(nnz, "keys")};
+  uint32_t* idx[2] = {dalloc<uint32_t>(nnz, "idx"), dalloc<uint32_t>(nnz, "idx")};
+  unsigned long long* d_bad = dalloc<unsigned long long>(1, "bad");
+  std::vector<void*> temps = {t_rows, t_cols, t_vals, keys[0], keys[1], idx[0], idx[1], d_bad};
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(st);
+    for (void* p : temps) cudaFree(p);
+  };
+  try {
+    check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
+    check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
+    check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+    check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
+    BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
+    check_cuda(launch_make_keys(g, t_rows, t_cols, nnz, keys[0], idx[0], d_bad, st), "make_keys");
+    unsigned long long bad = 0;
+    check_cuda(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st), "D2H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    if (bad) throw Error(DSGDPP_E_INVALID, std::to_string(bad) + " entries lie outside the matrix");
+
+    const int end_bit = bit_length((uint64_t)nblocks * span - 1);
+    cub::DoubleBuffer<uint64_t> kb(keys[0], keys[1]);
+    cub::DoubleBuffer<uint32_t> vb(idx[0], idx[1]);
+    size_t tb = 0;
+    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int)nnz, 0, end_bit, st), "sort");
+    void* tmp = nullptr;
+    check_cuda(cudaMalloc(&tmp, tb), "sort temp");
+    temps.push_back(tmp);
+    check_cuda(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)nnz, 0, end_bit, st), "sort");
+    uint64_t* skeys = kb.Current();
+    uint32_t* sidx = vb.Current();
+    uint64_t* okeys = kb.Alternate();
+    uint32_t* oidx = vb.Alternate();
+
+    // run heads -> output positions (reuse the alternate index buffer)
+    uint32_t* flags = oidx;
+    uint32_t* pos = dalloc<uint32_t>(nnz, "pos");
+    temps.push_back(pos);
+    check_cuda(launch_head_flags(skeys, nnz, flags, st), "head_flags");
+    size_t sb = 0;
+    check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, sb, flags, pos, (int)nnz, st), "scan");
+    void* stmp = nullptr;
+    check_cuda(cudaMalloc(&stmp, sb), "scan temp");
+    temps.push_back(stmp);
+    check_cuda(cub::DeviceScan::ExclusiveSum(stmp, sb, flags, pos, (int)nnz, st), "scan");
+    uint32_t last_pos = 0, last_flag = 0;
+    check_cuda(cudaMemcpyAsync(&last_pos, pos + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
+    check_cuda(cudaMemcpyAsync(&last_flag, flags + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    const uint64_t u = (uint64_t)last_pos + last_flag;
+
+    uint32_t* urow = dalloc<uint32_t>(u, "urow");
+    uint32_t* ucol = dalloc<uint32_t>(u, "ucol");
+    double* uval = dalloc<double>(u, "uval");
+    temps.push_back(urow); temps.push_back(ucol); temps.push_back(uval);
+    check_cuda(launch_merge_runs(g, skeys, sidx, pos, nnz, t_vals, t_rows, t_cols, okeys, urow,
+                                 ucol, uval, st), "merge_runs");
+    uint64_t* ukeys = okeys;
+    check_cuda(launch_block_ptr(ukeys, u, span, nblocks, M.block_ptr, st), "block_ptr");
+
+    M.row = dalloc<uint32_t>(u, "row");
+    M.col = dalloc<uint32_t>(u, "col");
+    check_cuda(cudaMalloc(&M.val, std::max<uint64_t>(u, 1) * (as_double ? 8 : 4)), "val");
+    if (shuffled) {
+      // in-block random layout: key = (block, hash(layout_seed, k))
+      uint64_t* k2 = skeys;   // free now
+      uint32_t* i2 = sidx;
+      check_cuda(launch_shuffle_keys(ukeys, u, span, c->cfg.layout_seed, k2, i2, st), "shuffle");
+      cub::DoubleBuffer<uint64_t> kb2(k2, ukeys);
+      cub::DoubleBuffer<uint32_t> vb2(i2, flags);
+      size_t tb2 = 0;
+      check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb2, kb2, vb2, (int)u, 0, 64, st), "sort");
+      void* tmp2 = nullptr;
+      check_cuda(cudaMalloc(&tmp2, tb2), "sort temp");
+      temps.push_back(tmp2);
+      check_cuda(cub::DeviceRadixSort::SortPairs(tmp2, tb2, kb2, vb2, (int)u, 0, 64, st), "sort");
+      check_cuda(launch_gather_records(vb2.Current(), u, urow, ucol, uval, M.row, M.col, M.val,
+                                       as_double, st), "gather");
+    } else {
+      check_cuda(launch_gather_records(nullptr, u, urow, ucol, uval, M.row, M.col, M.val,
+                                       as_double, st), "gather");
+    }
+    check_cuda(cudaMemcpyAsync(M.h_block_ptr.data(), M.block_ptr, (nblocks + 1) * 8,
+                               cudaMemcpyDeviceToHost, st), "D2H block_ptr");
+    if (which == DSGDPP_TRAIN) {
+      check_cuda(cudaMemsetAsync(c->cnt1, 0, c->cfg.m * 4, st), "cnt1");
+      check_cuda(cudaMemsetAsync(c->cnt2, 0, c->cfg.n * 4, st), "cnt2");
+      check_cuda(launch_count_nnz12(M.row, M.col, u, c->cnt1, c->cnt2, st), "nnz12");
+      if (c->inv1) {
+        check_cuda(launch_inverse_counts(c->cnt1, c->cfg.m, c->inv1, as_double, st), "inv1");
+        check_cuda(launch_inverse_counts(c->cnt2, c->cfg.n, c->inv2, as_double, st), "inv2");
+      }
+    }
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    M.nnz = u;
+    M.present = true;
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+}
+
+void ensure_staging(dsgdpp_ctx* c) {
+  if (!c->staging) c->staging = dalloc<double>((c->cfg.m + c->cfg.n) * c->r, "staging");
+}
+
+// ---- epochs --------------------------------------------------------------------------
+void wait_inputs_free(dsgdpp_ctx* c) {
+  check_cuda(cudaEventSynchronize(c->ev_inputs), "event sync");
+}
+
+void fill_epoch_params(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
+  EpochParams p{};
+  p.eps = eps;
+  p.key0 = seeds[0];
+  p.key1 = c->d > 1 ? seeds[1] : (seeds[0] ^ 0x5bd1e995u);
+  p.epoch = c->epoch_counter++;
+  *c->h_params = p;
+}
+
+// lazy L2 scales of the Hogwild path: sigma_W before sub-epoch s is f^s; the
+// scale of H block b2 is f^(earlier visits of b2); both are folded into the
+// update and applied to the factors once at the end of the epoch.
+void fill_sigma(dsgdpp_ctx* c, double eps) {
+  const uint32_t d = c->d, d2 = 2 * d;
+  const bool l2 = c->cfg.regularize == DSGDPP_REGULARIZE_L2 && c->cfg.regularize_lambda != 0;
+  double factor = 1.0;
+  if (l2) {
+    const double er = eps / d;
+    factor = 1 - er * 2 * c->cfg.regularize_lambda;
+    if (factor < 0.5) factor = 0.25 / (1 - factor);
+  }
+  std::vector<double> sh(d2, 1.0);
+  double sw = 1.0;
+  for (uint32_t s = 0; s < d2; ++s) {
+    for (uint32_t id = 0; id < d; ++id) {
+      const uint32_t b2 = c->h_schedule[(size_t)s * d + id];
+      float* o = c->h_sigma + ((size_t)s * d + id) * 3;
+      o[0] = (float)(sw * sh[b2]);
+      o[1] = (float)(sh[b2] / sw);
+      o[2] = (float)(sw / sh[b2]);
+    }
+    sw *= factor;
+    for (uint32_t id = 0; id < d; ++id) sh[c->h_schedule[(size_t)s * d + id]] *= factor;
+  }
+  for (uint32_t b = 0; b < d2; ++b) c->h_scales[b] = (float)sh[b];
+  c->h_scales[d2] = (float)sw;
+}
+
+bool lazy_l2(const dsgdpp_ctx* c) {
+  return c->cfg.regularize == DSGDPP_REGULARIZE_L2 && c->cfg.regularize_lambda != 0;
+}
+
+void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
+  cudaStream_t st = c->stream;
+  const uint32_t d = c->d, d2 = 2 * d;
+  const bool l2 = lazy_l2(c);
+  check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
+                             cudaMemcpyHostToDevice, st), "H2D schedule");
+  check_cuda(cudaMemcpyAsync(c->d_params, c->h_params, sizeof(EpochParams),
+                             cudaMemcpyHostToDevice, st), "H2D params");
+  if (l2) {
+    check_cuda(cudaMemcpyAsync(c->d_sigma, c->h_sigma, (size_t)d2 * d * 3 * 4,
+                               cudaMemcpyHostToDevice, st), "H2D sigma");
+    check_cuda(cudaMemcpyAsync(c->d_scales, c->h_scales, (d2 + 1) * 4, cudaMemcpyHostToDevice,
+                               st), "H2D scales");
+  }
+  SegBuildArgs sb{c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr, c->d_segs,
+                  c->d_counters, d};
+  check_cuda(launch_build_segments(sb, st), "build_segments");
+  HogwildArgs a{};
+  const DevMatrix& M = c->mat[0];
+  a.row = M.row; a.col = M.col; a.val = M.val;
+  a.inv1 = c->inv1; a.inv2 = c->inv2;
+  a.W = c->W; a.H = c->H;
+  a.segs = c->d_segs; a.counters = c->d_counters; a.params = c->d_params;
+  a.d = d; a.r = c->r; a.rp = c->rp;
+  a.update = c->cfg.update; a.truncate = c->cfg.truncate; a.sgd_order = c->cfg.sgd_order;
+  a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
+  const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
+  for (uint32_t s = 0; s < d2; ++s) {
+    if (prof) check_cuda(cudaEventRecord(c->prof_ev[s], st), "event");
+    check_cuda(launch_hogwild_subepoch(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
+               "hogwild_subepoch");
+  }
+  if (prof) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
+  if (l2)
+    check_cuda(launch_normalize(c->cfg.precision, c->W, c->H, c->cfg.m, c->cfg.n, c->rp,
+                                c->d_scales, c->d_off2, d2, st), "normalize");
+}
+
+void collect_profile(dsgdpp_ctx* c) {
+  if (!c->prof_pending) return;
+  c->prof_pending = false;
+  const uint32_t d2 = 2 * c->d;
+  check_cuda(cudaEventSynchronize(c->prof_ev[d2]), "event sync");
+  for (uint32_t s = 0; s < d2; ++s) {
+    float f = 0;
+    check_cuda(cudaEventElapsedTime(&f, c->prof_ev[s], c->prof_ev[s + 1]), "elapsed");
+    c->prof_ms += f;
+  }
+  c->prof_launches += d2;
+}
+
+void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
+  if (lazy_l2(c)) fill_sigma(c, eps);
+  cudaStream_t st = c->stream;
+  collect_profile(c);
+  check_cuda(cudaEventRecord(c->ev_begin, st), "event");
+  if (c->cfg.launch == DSGDPP_LAUNCH_GRAPH && !c->profiling) {
+    if (!c->graph_exec) {
+      cudaGraph_t g = nullptr;
+      check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+      try {
+        enqueue_hogwild_epoch(c);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      check_cuda(cudaStreamEndCapture(st, &g), "capture end");
+      cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+      cudaGraphDestroy(g);
+      check_cuda(e, "graph instantiate");
+    }
+    check_cuda(cudaGraphLaunch(c->graph_exec, st), "graph launch");
+  } else {
+    enqueue_hogwild_epoch(c);
+    c->prof_pending = c->profiling;
+  }
+  check_cuda(cudaEventRecord(c->ev_end, st), "event");
+  check_cuda(cudaEventRecord(c->ev_inputs, st), "event");
+  c->epoch_timed = true;
+}
+
+void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
+  const uint32_t d = c->d, d2 = 2 * d;
+  const DevMatrix& M = c->mat[0];
+  // point orders, one generator per task (mf/sgd/dsgdpp_impl.h:79,112)
+  uint64_t total = 0;
+  for (uint32_t s = 0; s < d2; ++s)
+    for (uint32_t id = 0; id < d; ++id) {
+      c->h_pos_offset[(size_t)s * d + id] = total;
+      const uint64_t blk = (uint64_t)id * d2 + c->h_schedule[(size_t)s * d + id];
+      total += M.h_block_ptr[blk + 1] - M.h_block_ptr[blk];
+    }
+  c->h_pos_offset[(size_t)d2 * d] = total;
+  if (total > c->positions_cap) {
+    hfree(c->h_positions);
+    dfree(c->d_positions);
+    c->positions_cap = std::max<uint64_t>(total, 1);
+    c->h_positions = halloc<uint32_t>(c->positions_cap, "positions");
+    c->d_positions = dalloc<uint32_t>(c->positions_cap, "positions");
+  }
+  const unsigned hw = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), d));
+  auto work = [&](unsigned t) {
+    for (uint32_t id = t; id < d; id += hw) {
+      TaskOrder order(seeds[id]);
+      for (uint32_t s = 0; s < d2; ++s) {
+        const uint64_t blk = (uint64_t)id * d2 + c->h_schedule[(size_t)s * d + id];
+        const uint64_t n = M.h_block_ptr[blk + 1] - M.h_block_ptr[blk];
+        order.next_block(c->cfg.sgd_order, n, c->h_positions + c->h_pos_offset[(size_t)s * d + id]);
+      }
+    }
+  };
+  if (hw > 1 && total > 100000) {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < hw; ++t) pool.emplace_back(work, t);
+    for (auto& th : pool) th.join();
+  } else {
+    for (unsigned t = 0; t < hw; ++t) work(t);
+  }
+  const bool l2 = c->cfg.regularize == DSGDPP_REGULARIZE_L2;
+  if (l2) {
+    std::memset(c->h_mask, 0, (size_t)d2 * d2);
+    for (uint32_t s = 0; s < d2; ++s)
+      for (uint32_t id = 0; id < d; ++id) c->h_mask[(size_t)s * d2 + c->h_schedule[(size_t)s * d + id]] = 1;
+  }
+  cudaStream_t st = c->stream;
+  check_cuda(cudaEventRecord(c->ev_begin, st), "event");
+  check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
+                             cudaMemcpyHostToDevice, st), "H2D schedule");
+  check_cuda(cudaMemcpyAsync(c->d_params, c->h_params, sizeof(EpochParams),
+                             cudaMemcpyHostToDevice, st), "H2D params");
+  check_cuda(cudaMemcpyAsync(c->d_pos_offset, c->h_pos_offset, ((size_t)d2 * d + 1) * 8,
+                             cudaMemcpyHostToDevice, st), "H2D pos_offset");
+  if (total)
+    check_cuda(cudaMemcpyAsync(c->d_positions, c->h_positions, total * 4, cudaMemcpyHostToDevice,
+                               st), "H2D positions");
+  if (l2)
+    check_cuda(cudaMemcpyAsync(c->d_mask, c->h_mask, (size_t)d2 * d2, cudaMemcpyHostToDevice, st),
+               "H2D mask");
+  ReplayArgs a{};
+  a.row = M.row; a.col = M.col; a.val = static_cast<const double*>(M.val);
+  a.cnt1 = c->cnt1; a.cnt2 = c->cnt2;
+  a.W = static_cast<double*>(c->W); a.H = static_cast<double*>(c->H);
+  a.block_ptr = M.block_ptr; a.schedule = c->d_schedule;
+  a.positions = c->d_positions; a.pos_offset = c->d_pos_offset; a.params = c->d_params;
+  a.d = d; a.r = c->r; a.rp = c->rp;
+  a.update = c->cfg.update; a.truncate = c->cfg.truncate;
+  a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
+  for (uint32_t s = 0; s < d2; ++s) {
+    check_cuda(launch_replay_subepoch(a, s, st), "replay_subepoch");
+    if (l2 && c->cfg.regularize_lambda != 0)
+      check_cuda(launch_regularize_exact(a.W, a.H, c->cfg.m, c->cfg.n, c->rp, c->r, c->d_off2,
+                                         c->d_mask + (size_t)s * d2, d, c->d_params,
+                                         c->cfg.regularize_lambda, c->cfg.truncate,
+                                         c->cfg.truncate_min, c->cfg.truncate_max, st),
+                 "regularize");
+  }
+  check_cuda(cudaEventRecord(c->ev_end, st), "event");
+  check_cuda(cudaEventRecord(c->ev_inputs, st), "event");
+  c->epoch_timed = true;
+}
+
+void epoch_explicit_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
+                         const uint32_t* seeds) {
+  if (!schedule || !seeds) throw Error(DSGDPP_E_INVALID, "schedule and task seeds are required");
+  if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
+  if (!c->factors_set) throw Error(DSGDPP_E_STATE, "factors not set");
+  if (!std::isfinite(eps)) throw Error(DSGDPP_E_INVALID, "step size is not finite");
+  const uint32_t d = c->d, d2 = 2 * d;
+  for (size_t k = 0; k < (size_t)d2 * d; ++k)
+    if (schedule[k] >= d2) throw Error(DSGDPP_E_INVALID, "schedule entry out of range");
+  check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+  wait_inputs_free(c);
+  std::memcpy(c->h_schedule, schedule, (size_t)d2 * d * 4);
+  fill_epoch_params(c, eps, seeds);
+  if (c->cfg.exec == DSGDPP_EXEC_REPLAY) run_replay_epoch(c, eps, seeds);
+  else run_hogwild_epoch(c, eps);
+}
+
+// ---- losses --------------------------------------------------------------------------
+double finish_sum(dsgdpp_ctx* c, uint32_t count) {
+  check_cuda(launch_sum_partials(c->d_partials, count, c->d_out, c->stream), "sum_partials");
+  check_cuda(cudaMemcpyAsync(c->h_out, c->d_out, 8, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  check_cuda(cudaStreamSynchronize(c->stream), "sync");
+  return c->h_out[0];
+}
+
+double nzsl_impl(dsgdpp_ctx* c, int which) {
+  if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
+  const DevMatrix& M = c->mat[which];
+  if (!M.present) throw Error(DSGDPP_E_STATE, which ? "no test matrix" : "no training matrix");
+  check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+  if (M.nnz == 0) return 0.0;
+  check_cuda(launch_nzsl_partials(c->cfg.precision, M.row, M.col, M.val, M.nnz, c->W, c->H, c->r,
+                                  c->rp, c->d_partials, c->loss_grid, c->stream), "nzsl");
+  return finish_sum(c, c->loss_grid);
+}
+
+double sumsq_impl(dsgdpp_ctx* c, const void* X, uint64_t count) {
+  check_cuda(launch_sumsq_partials(c->cfg.precision, X, count, c->d_partials, c->loss_grid,
+                                   c->stream), "l2");
+  return finish_sum(c, c->loss_grid);
+}
+
+double nzl2_impl(dsgdpp_ctx* c, const void* X, uint64_t rows, const uint32_t* cnt) {
+  check_cuda(launch_nzl2_partials(c->cfg.precision, X, rows, c->rp, cnt, c->d_partials,
+                                  c->loss_grid, c->stream), "nzl2");
+  return finish_sum(c, c->loss_grid);
+}
+
+double loss_impl(dsgdpp_ctx* c) {
+  double l = nzsl_impl(c, DSGDPP_TRAIN);
+  if (c->cfg.loss == DSGDPP_LOSS_NZSL_L2) {
+    const double w = sumsq_impl(c, c->W, c->cfg.m * c->rp);
+    const double h = sumsq_impl(c, c->H, c->cfg.n * c->rp);
+    l = l + c->cfg.loss_lambda * (w + h);
+  } else if (c->cfg.loss == DSGDPP_LOSS_NZSL_NZL2) {
+    const double w = nzl2_impl(c, c->W, c->cfg.m, c->cnt1);
+    const double h = nzl2_impl(c, c->H, c->cfg.n, c->cnt2);
+    l = l + c->cfg.loss_lambda * (w + h);
+  }
+  return l;
+}
+
+double elapsed_ns(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(b - a).count();
+}
+
+}  // namespace
+
+// ---- exported ------------------------------------------------------------------------
+namespace {
+thread_local std::string g_create_error;  // message of this thread's last failed dsgdpp_create
+}
+
+extern "C" {
+
+int dsgdpp_abi_version(void) { return DSGDPP_ABI_VERSION; }
+
+const char* dsgdpp_create_error(void) { return g_create_error.c_str(); }
+
+const char* dsgdpp_status_string(int s) {
+  switch (s) {
+    case DSGDPP_OK: return "ok";
+    case DSGDPP_E_INVALID: return "invalid argument";
+    case DSGDPP_E_CUDA: return "CUDA error";
+    case DSGDPP_E_IO: return "I/O error";
+    case DSGDPP_E_UNSUPPORTED: return "not supported";
+    case DSGDPP_E_STATE: return "call out of order";
+    case DSGDPP_E_NOMEM: return "out of memory";
+    default: return "unknown status";
+  }
+}
+
+void dsgdpp_config_init(dsgdpp_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->rank = 10;
+  c->d = 1;
+  c->precision = DSGDPP_FP32;
+  c->exec = DSGDPP_EXEC_HOGWILD;
+  c->launch = DSGDPP_LAUNCH_GRAPH;
+  c->update = DSGDPP_UPDATE_NZSL_L2;
+  c->update_lambda = 1.0;
+  c->regularize = DSGDPP_REGULARIZE_NONE;
+  c->loss = DSGDPP_LOSS_NZSL_L2;
+  c->loss_lambda = 1.0;
+  c->truncate = 0;
+  c->truncate_min = NAN;
+  c->truncate_max = NAN;
+  c->sgd_order = DSGDPP_SGD_WOR;
+  c->stratum_order = DSGDPP_STRATUM_COWOR;
+  c->device = 0;
+  c->layout_seed = 0x5eed5eedull;
+}
+
+int dsgdpp_create(const dsgdpp_config* cfg, dsgdpp_ctx** out) {
+  if (!out) return DSGDPP_E_INVALID;
+  *out = nullptr;
+  dsgdpp_ctx* c = new (std::nothrow) dsgdpp_ctx();
+  if (!c) return DSGDPP_E_NOMEM;
+  int rc = guarded(c, [&]() {
+    create_impl(c, cfg);
+    return DSGDPP_OK;
+  });
+  if (rc != DSGDPP_OK) {
+    g_create_error = c->err;
+    destroy_impl(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return DSGDPP_OK;
+}
+
+void dsgdpp_destroy(dsgdpp_ctx* c) {
+  if (!c) return;
+  destroy_impl(c);
+  delete c;
+}
+
+const char* dsgdpp_last_error(const dsgdpp_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int dsgdpp_set_matrix(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* rows,
+                      const uint32_t* cols, const double* vals) {
+  return guarded(c, [&]() {
+    set_matrix_impl(c, which, nnz, rows, cols, vals);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_factors(dsgdpp_ctx* c, const double* W, const double* H) {
+  return guarded(c, [&]() {
+    if (!W || !H) throw Error(DSGDPP_E_INVALID, "null factor array");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    ensure_staging(c);
+    const uint64_t m = c->cfg.m, n = c->cfg.n, r = c->r;
+    cudaStream_t st = c->stream;
+    check_cuda(cudaMemcpyAsync(c->staging, W, m * r * 8, cudaMemcpyHostToDevice, st), "H2D W");
+    check_cuda(cudaMemcpyAsync(c->staging + m * r, H, n * r * 8, cudaMemcpyHostToDevice, st), "H2D H");
+    check_cuda(launch_factor_to_device(c->cfg.precision, c->staging, m, c->r, c->rp, c->W, st), "W");
+    check_cuda(launch_factor_to_device(c->cfg.precision, c->staging + m * r, n, c->r, c->rp, c->H,
+                                       st), "H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    c->factors_set = true;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_get_factors(dsgdpp_ctx* c, double* W, double* H) {
+  return guarded(c, [&]() {
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    ensure_staging(c);
+    const uint64_t m = c->cfg.m, n = c->cfg.n, r = c->r;
+    cudaStream_t st = c->stream;
+    check_cuda(launch_factor_to_host(c->cfg.precision, c->W, m, c->r, c->rp, c->staging, st), "W");
+    check_cuda(launch_factor_to_host(c->cfg.precision, c->H, n, c->r, c->rp, c->staging + m * r,
+                                     st), "H");
+    if (W) check_cuda(cudaMemcpyAsync(W, c->staging, m * r * 8, cudaMemcpyDeviceToHost, st), "D2H W");
+    if (H)
+      check_cuda(cudaMemcpyAsync(H, c->staging + m * r, n * r * 8, cudaMemcpyDeviceToHost, st),
+                 "D2H H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_block_nnz(dsgdpp_ctx* c, int which, uint64_t* out) {
+  return guarded(c, [&]() {
+    if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
+    const DevMatrix& M = c->mat[which];
+    if (!M.present) throw Error(DSGDPP_E_STATE, "matrix not set");
+    const size_t nb = (size_t)c->d * 2 * c->d;
+    for (size_t b = 0; b < nb; ++b) out[b] = M.h_block_ptr[b + 1] - M.h_block_ptr[b];
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_nnz12(dsgdpp_ctx* c, uint64_t* nnz1, uint64_t* nnz2, uint64_t* nnz12max) {
+  return guarded(c, [&]() {
+    if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    std::vector<uint32_t> a(c->cfg.m), b(c->cfg.n);
+    check_cuda(cudaMemcpy(a.data(), c->cnt1, c->cfg.m * 4, cudaMemcpyDeviceToHost), "D2H");
+    check_cuda(cudaMemcpy(b.data(), c->cnt2, c->cfg.n * 4, cudaMemcpyDeviceToHost), "D2H");
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < c->cfg.m; ++i) {
+      if (nnz1) nnz1[i] = a[i];
+      mx = std::max<uint64_t>(mx, a[i]);
+    }
+    for (uint64_t j = 0; j < c->cfg.n; ++j) {
+      if (nnz2) nnz2[j] = b[j];
+      mx = std::max<uint64_t>(mx, b[j]);
+    }
+    if (nnz12max) *nnz12max = mx;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_seed(dsgdpp_ctx* c, uint32_t seed) {
+  return guarded(c, [&]() {
+    c->master.seed_with(seed);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_epoch(dsgdpp_ctx* c, double eps) {
+  return guarded(c, [&]() {
+    const uint32_t d = c->d;
+    std::vector<uint32_t> sched((size_t)2 * d * d), seeds(d);
+    dsgdpp_schedule(c->master, d, c->cfg.stratum_order, sched.data(), seeds.data());
+    epoch_explicit_impl(c, eps, sched.data(), seeds.data());
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_epoch_explicit(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
+                          const uint32_t* task_seeds) {
+  return guarded(c, [&]() {
+    epoch_explicit_impl(c, eps, schedule, task_seeds);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_last_epoch_ms(dsgdpp_ctx* c, double* ms) {
+  return guarded(c, [&]() {
+    if (!ms) throw Error(DSGDPP_E_INVALID, "null output");
+    if (!c->epoch_timed) throw Error(DSGDPP_E_STATE, "no epoch has run");
+    check_cuda(cudaEventSynchronize(c->ev_end), "event sync");
+    float f = 0;
+    check_cuda(cudaEventElapsedTime(&f, c->ev_begin, c->ev_end), "elapsed");
+    *ms = f;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_kernel_timing(dsgdpp_ctx* c, int on) {
+  return guarded(c, [&]() {
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    collect_profile(c);
+    if (on && c->prof_ev.empty()) {
+      c->prof_ev.resize(2 * c->d + 1);
+      for (auto& e : c->prof_ev) check_cuda(cudaEventCreate(&e), "event");
+    }
+    c->profiling = on != 0;
+    c->prof_ms = 0;
+    c->prof_launches = 0;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_kernel_timing(dsgdpp_ctx* c, double* total_ms, uint64_t* launches) {
+  return guarded(c, [&]() {
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    collect_profile(c);
+    if (total_ms) *total_ms = c->prof_ms;
+    if (launches) *launches = c->prof_launches;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_launch_shape(dsgdpp_ctx* c, uint32_t* lanes, uint32_t* vecs, uint32_t* grid) {
+  return guarded(c, [&]() {
+    if (lanes) *lanes = c->lanes;
+    if (vecs) *vecs = c->vecs;
+    if (grid) *grid = c->grid;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_loss(dsgdpp_ctx* c, double* out) {
+  return guarded(c, [&]() {
+    if (!out) throw Error(DSGDPP_E_INVALID, "null output");
+    *out = loss_impl(c);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_nzsl(dsgdpp_ctx* c, int which, double* out) {
+  return guarded(c, [&]() {
+    if (!out) throw Error(DSGDPP_E_INVALID, "null output");
+    *out = nzsl_impl(c, which);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_l2(dsgdpp_ctx* c, double* w2, double* h2) {
+  return guarded(c, [&]() {
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    if (w2) *w2 = sumsq_impl(c, c->W, c->cfg.m * c->rp);
+    if (h2) *h2 = sumsq_impl(c, c->H, c->cfg.n * c->rp);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_nzl2(dsgdpp_ctx* c, double* w, double* h) {
+  return guarded(c, [&]() {
+    if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    if (w) *w = nzl2_impl(c, c->W, c->cfg.m, c->cnt1);
+    if (h) *h = nzl2_impl(c, c->H, c->cfg.n, c->cnt2);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_run(dsgdpp_ctx* c, uint32_t epochs, int decay, double eps0, double decrease,
+               double increase, dsgdpp_trace_row* trace) {
+  return guarded(c, [&]() {
+    if (decay != DSGDPP_DECAY_CONST && decay != DSGDPP_DECAY_BOLDDRIVER)
+      throw Error(DSGDPP_E_INVALID, "unknown decay");
+    using clock = std::chrono::steady_clock;
+    const bool has_test = c->mat[1].present;
+    auto t0 = clock::now();
+    double cur = loss_impl(c);
+    auto t1 = clock::now();
+    double test = has_test ? nzsl_impl(c, DSGDPP_TEST) : NAN;
+    auto t2 = clock::now();
+    if (trace) {
+      trace[0] = dsgdpp_trace_row{0, cur, test, NAN, 0, 0, elapsed_ns(t0, t1),
+                                  has_test ? elapsed_ns(t1, t2) : 0.0};
+    }
+    double prev = 0, eps_state = eps0;
+    const uint32_t d = c->d;
+    std::vector<uint32_t> sched((size_t)2 * d * d), seeds(d);
+    for (uint32_t e = 0; e < epochs; ++e) {
+      auto a = clock::now();
+      double eps;
+      if (decay == DSGDPP_DECAY_CONST) {
+        eps = eps0;
+      } else if (e == 0) {
+        eps = eps_state;  // BoldDriver: the first call returns the initial step
+      } else {
+        eps_state *= (prev <= cur) ? decrease : increase;  // decay_bolddriver.h:59-67
+        eps = eps_state;
+      }
+      auto b = clock::now();
+      dsgdpp_schedule(c->master, d, c->cfg.stratum_order, sched.data(), seeds.data());
+      epoch_explicit_impl(c, eps, sched.data(), seeds.data());
+      check_cuda(cudaEventSynchronize(c->ev_end), "event sync");
+      auto e1 = clock::now();
+      prev = cur;
+      cur = loss_impl(c);
+      auto e2 = clock::now();
+      test = has_test ? nzsl_impl(c, DSGDPP_TEST) : NAN;
+      auto e3 = clock::now();
+      if (trace)
+        trace[e + 1] = dsgdpp_trace_row{e + 1u, cur, test, eps, elapsed_ns(a, b), elapsed_ns(b, e1),
+                                        elapsed_ns(e1, e2), has_test ? elapsed_ns(e2, e3) : 0.0};
+    }
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_sync(dsgdpp_ctx* c) {
+  return guarded(c, [&]() {
+    check_cuda(cudaStreamSynchronize(c->stream), "sync");
+    return DSGDPP_OK;
+  });
+}
+
+// ---- host utilities ------------------------------------------------------------------
+struct dsgdpp_rng {
+  Random32 r;
+};
+
+dsgdpp_rng* dsgdpp_rng_create(uint32_t seed) {
+  auto* g = new (std::nothrow) dsgdpp_rng();
+  if (g) g->r.seed_with(seed);
+  return g;
+}
+void dsgdpp_rng_destroy(dsgdpp_rng* g) { delete g; }
+uint32_t dsgdpp_rng_next(dsgdpp_rng* g) { return g->r.next(); }
+uint32_t dsgdpp_rng_next_int(dsgdpp_rng* g, uint32_t n) { return g->r.next_int(n); }
+
+void dsgdpp_draw_schedule(dsgdpp_rng* g, uint32_t d, int order, uint32_t* schedule,
+                          uint32_t* seeds) {
+  dsgdpp_schedule(g->r, d, order, schedule, seeds);
+}
+
+void dsgdpp_dsgd_schedule(dsgdpp_rng* g, uint32_t w, uint32_t t, int order, uint32_t* out) {
+  std::vector<uint32_t> s = dsgd_schedule(w, t, order, g->r);
+  std::copy(s.begin(), s.end(), out);
+}
+
+uint64_t dsgdpp_point_orders(uint32_t d, int sgd_order, const uint64_t* block_nnz,
+                             const uint32_t* schedule, const uint32_t* seeds, uint32_t* out) {
+  const uint32_t d2 = 2 * d;
+  std::vector<TaskOrder> tasks;
+  tasks.reserve(d);
+  for (uint32_t id = 0; id < d; ++id) tasks.emplace_back(seeds[id]);
+  uint64_t at = 0;
+  std::vector<uint32_t> tmp;
+  for (uint32_t s = 0; s < d2; ++s)
+    for (uint32_t id = 0; id < d; ++id) {
+      const uint64_t n = block_nnz[(size_t)id * d2 + schedule[(size_t)s * d + id]];
+      uint32_t* dst = out;
+      if (out) dst = out + at;
+      else { tmp.resize(n); dst = tmp.data(); }
+      tasks[id].next_block(sgd_order, n, dst);
+      at += n;
+    }
+  return at;
+}
+
+void dsgdpp_block_offsets(uint64_t size, uint32_t blocks, uint64_t* out) {
+  std::vector<uint64_t> o = block_offsets(size, blocks);
+  std::copy(o.begin(), o.end(), out);
+}
+
+void dsgdpp_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  Philox4 r = philox4x32_10(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1]);
+  for (int k = 0; k < 4; ++k) out[k] = r.v[k];
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// kernels.cuh -- argument blocks and host launchers of the DSGD++ kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace dsgdpp {
+
+enum Precision : int { kFp64 = 0, kFp32 = 1, kBf16 = 2 };
+enum UpdateKind : int { kUpdNzsl = 0, kUpdNzslL2 = 1, kUpdNzslNzl2 = 2 };
+
+// Parameters that change every epoch live in device memory so a captured
+// graph of the epoch stays valid.
+struct EpochParams {
+  double eps;
+  uint32_t key0, key1;  // Philox key: drawn from the task seeds of the epoch
+  uint32_t epoch;       // epoch counter (Philox counter word)
+  uint32_t pad;
+};
+
+// Hogwild sub-epoch: all records of the sub-epoch's d conflict-free blocks are
+// one work list of 32-record chunks; a warp takes a chunk, and 32/LPN groups
+// of LPN lanes update 32/LPN records at a time, lanes spanning the rank.
+struct HogwildArgs {
+  const uint32_t* row;
+  const uint32_t* col;
+  const void* val;       // float (fp32/bf16 factors) or double (fp64 factors)
+  const void* inv1;      // 1/nnz1 per row (float or double, as the compute type)
+  const void* inv2;      // 1/nnz2 per column
+  void* W;               // m x rp
+  void* H;               // n x rp (column j of H is contiguous)
+  const Segment* segs;   // [2d][d+1]
+  uint32_t* counters;    // [2d] work counters (zeroed by the segment builder)
+  const EpochParams* params;
+  uint32_t d, r, rp;
+  int update, truncate, sgd_order;
+  double lambda, tmin, tmax;
+};
+
+// Deterministic FP64 replay: one warp per task walks its block in the
+// host-generated point order; d blocks of a sub-epoch run side by side.
+struct ReplayArgs {
+  const uint32_t* row;
+  const uint32_t* col;
+  const double* val;
+  const uint32_t* cnt1;  // nnz1 per row
+  const uint32_t* cnt2;  // nnz2 per column
+  double* W;
+  double* H;
+  const uint64_t* block_ptr;  // d*2d+1
+  const uint32_t* schedule;   // [2d][d]
+  const uint32_t* positions;  // point order, concatenated per (sub-epoch, task)
+  const uint64_t* pos_offset; // [2d*d+1]
+  const EpochParams* params;
+  uint32_t d, r, rp;
+  int update, truncate;
+  double lambda, tmin, tmax;
+};
+
+struct SegBuildArgs {
+  const uint32_t* schedule;   // [2d][d]
+  const uint64_t* block_ptr;  // d*2d+1
+  const float* sigma;         // [2d][d][3] lazy L2 scales, or null (all ones)
+  Segment* segs;              // [2d][d+1]
+  uint32_t* counters;         // [2d]
+  uint32_t d;
+};
+
+// ---- launchers (return cudaError_t) -------------------------------------------
+cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);
+cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs,
+                                    const HogwildArgs& a, uint32_t s, uint32_t grid,
+                                    cudaStream_t st);
+// CTAs per SM that the Hogwild kernel sustains for this configuration
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d);
+cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
+// RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
+cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
+                                    uint32_t r, const uint64_t* off2, const uint8_t* mask,
+                                    uint32_t d, const EpochParams* params, double lambda,
+                                    int truncate, double tmin, double tmax, cudaStream_t st);
+// Lazy-L2 normalisation at the end of a Hogwild epoch: H column block b2 is
+// multiplied by scales[b2], all of W by scales[nb2] (device memory)
+cudaError_t launch_normalize(int precision, void* W, void* H, uint64_t m, uint64_t n,
+                             uint32_t rp, const float* scales, const uint64_t* off2,
+                             uint32_t nb2, cudaStream_t st);
+
+// Loss partial sums (FP64); `partials` holds `grid` doubles, then sum_partials
+// writes the total to out[0].
+cudaError_t launch_nzsl_partials(int precision, const uint32_t* row, const uint32_t* col,
+                                 const void* val, uint64_t nnz, const void* W, const void* H,
+                                 uint32_t r, uint32_t rp, double* partials, uint32_t grid,
+                                 cudaStream_t st);
+cudaError_t launch_sumsq_partials(int precision, const void* X, uint64_t count,
+                                  double* partials, uint32_t grid, cudaStream_t st);
+cudaError_t launch_nzl2_partials(int precision, const void* X, uint64_t rows, uint32_t rp,
+                                 const uint32_t* cnt, double* partials, uint32_t grid,
+                                 cudaStream_t st);
+cudaError_t launch_sum_partials(const double* partials, uint32_t count, double* out,
+                                cudaStream_t st);
+
+// ---- data preparation -----------------------------------------------------------
+struct BlockingGeom {
+  uint64_t m, n;
+  uint32_t nb1, nb2;      // d, 2d
+  uint64_t mB, nB;        // largest block extent in rows / columns
+  const uint64_t* off1;   // nb1+1 (last = m)
+  const uint64_t* off2;   // nb2+1 (last = n)
+};
+cudaError_t launch_make_keys(const BlockingGeom& g, const uint32_t* rows, const uint32_t* cols,
+                             uint64_t nnz, uint64_t* keys, uint32_t* idx,
+                             unsigned long long* bad, cudaStream_t st);
+cudaError_t launch_head_flags(const uint64_t* keys, uint64_t nnz, uint32_t* flags,
+                              cudaStream_t st);
+// merges runs of equal keys (values summed in input order) into compact arrays
+cudaError_t launch_merge_runs(const BlockingGeom& g, const uint64_t* keys, const uint32_t* idx,
+                              const uint32_t* pos, uint64_t nnz, const double* vals_in,
+                              const uint32_t* rows_in, const uint32_t* cols_in, uint64_t* ukeys,
+                              uint32_t* urow, uint32_t* ucol, double* uval, cudaStream_t st);
+cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
+                             uint32_t nblocks, uint64_t* block_ptr, cudaStream_t st);
+cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
+                                uint64_t seed, uint64_t* keys2, uint32_t* idx2,
+                                cudaStream_t st);
+cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
+                                  const uint32_t* ucol, const double* uval, uint32_t* row,
+                                  uint32_t* col, void* val, int val_is_double, cudaStream_t st);
+cudaError_t launch_count_nnz12(const uint32_t* row, const uint32_t* col, uint64_t nnz,
+                               uint32_t* cnt1, uint32_t* cnt2, cudaStream_t st);
+cudaError_t launch_inverse_counts(const uint32_t* cnt, uint64_t len, void* inv,
+                                  int as_double, cudaStream_t st);
+cudaError_t launch_factor_to_device(int precision, const double* src, uint64_t rows,
+                                    uint32_t r, uint32_t rp, void* dst, cudaStream_t st);
+cudaError_t launch_factor_to_host(int precision, const void* src, uint64_t rows, uint32_t r,
+                                  uint32_t rp, double* dst, cudaStream_t st);
+
+}  // namespace dsgdpp

@@ -1,0 +1,262 @@
+// kernels_data.cu -- blocking of the input matrices and factor conversion.
+//
+// Reference: ReadMatrixBlocksMm (mf/matrix/io/read_impl.h:364-486) routes
+// every entry to its block of the d x 2d grid and stores block-local
+// coordinates; coordinate_matrix::sort (read_impl.h:162-164) orders each block
+// by (i, j) and sums duplicate entries.  Here the entries arrive as one
+// global COO array and are blocked on the GPU: a 64-bit key
+// (block, local row, local column) is radix-sorted stably, runs of equal keys
+// are merged, and block boundaries are found by binary search.
+#include "kernels.cuh"
+
+namespace dsgdpp {
+namespace {
+
+__device__ __forceinline__ uint32_t find_block(const uint64_t* off, uint32_t nb, uint64_t x) {
+  uint32_t lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void make_keys_kernel(BlockingGeom g, const uint32_t* rows, const uint32_t* cols,
+                                 uint64_t nnz, uint64_t* keys, uint32_t* idx,
+                                 unsigned long long* bad) {
+  extern __shared__ uint64_t offs[];
+  uint64_t* o1 = offs;
+  uint64_t* o2 = offs + g.nb1 + 1;
+  for (uint32_t k = threadIdx.x; k <= g.nb1; k += blockDim.x) o1[k] = g.off1[k];
+  for (uint32_t k = threadIdx.x; k <= g.nb2; k += blockDim.x) o2[k] = g.off2[k];
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    const uint64_t i = rows[k], j = cols[k];
+    if (i >= g.m || j >= g.n) {
+      atomicAdd(bad, 1ull);
+      keys[k] = ~0ull;
+      idx[k] = (uint32_t)k;
+      continue;
+    }
+    const uint32_t b1 = find_block(o1, g.nb1, i), b2 = find_block(o2, g.nb2, j);
+    const uint64_t blk = (uint64_t)b1 * g.nb2 + b2;
+    keys[k] = (blk * g.mB + (i - o1[b1])) * g.nB + (j - o2[b2]);
+    idx[k] = (uint32_t)k;
+  }
+}
+
+__global__ void head_flags_kernel(const uint64_t* keys, uint64_t nnz, uint32_t* flags) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride)
+    flags[k] = (k == 0 || keys[k] != keys[k - 1]) ? 1u : 0u;
+}
+
+__global__ void merge_runs_kernel(BlockingGeom g, const uint64_t* keys, const uint32_t* idx,
+                                  const uint32_t* pos, uint64_t nnz, const double* vals_in,
+                                  const uint32_t* rows_in, const uint32_t* cols_in,
+                                  uint64_t* ukeys, uint32_t* urow, uint32_t* ucol,
+                                  double* uval) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    if (!(k == 0 || keys[k] != keys[k - 1])) continue;
+    const uint64_t o = pos[k];
+    double v = vals_in[idx[k]];
+    for (uint64_t q = k + 1; q < nnz && keys[q] == keys[k]; ++q) v += vals_in[idx[q]];
+    ukeys[o] = keys[k];
+    urow[o] = rows_in[idx[k]];
+    ucol[o] = cols_in[idx[k]];
+    uval[o] = v;
+  }
+}
+
+__global__ void block_ptr_kernel(const uint64_t* ukeys, uint64_t u, uint64_t span,
+                                 uint32_t nblocks, uint64_t* ptr) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > nblocks) return;
+  if (b == nblocks) { ptr[b] = u; return; }
+  const uint64_t target = (uint64_t)b * span;
+  uint64_t lo = 0, hi = u;  // first key >= target
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (ukeys[mid] < target) lo = mid + 1; else hi = mid;
+  }
+  ptr[b] = lo;
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void shuffle_keys_kernel(const uint64_t* ukeys, uint64_t u, uint64_t span,
+                                    uint64_t seed, uint64_t* keys2, uint32_t* idx2) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
+    const uint64_t blk = ukeys[k] / span;
+    keys2[k] = (blk << 40) | (mix64(seed ^ (k * 0xD6E8FEB86659FD93ull)) >> 24);
+    idx2[k] = (uint32_t)k;
+  }
+}
+
+__global__ void gather_records_kernel(const uint32_t* idx, uint64_t u, const uint32_t* urow,
+                                      const uint32_t* ucol, const double* uval, uint32_t* row,
+                                      uint32_t* col, void* val, int val_is_double) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
+    const uint32_t q = idx ? idx[k] : (uint32_t)k;
+    row[k] = urow[q];
+    col[k] = ucol[q];
+    if (val_is_double) reinterpret_cast<double*>(val)[k] = uval[q];
+    else reinterpret_cast<float*>(val)[k] = (float)uval[q];
+  }
+}
+
+__global__ void count_nnz12_kernel(const uint32_t* row, const uint32_t* col, uint64_t nnz,
+                                   uint32_t* cnt1, uint32_t* cnt2) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    atomicAdd(cnt1 + row[k], 1u);
+    atomicAdd(cnt2 + col[k], 1u);
+  }
+}
+
+__global__ void inverse_counts_kernel(const uint32_t* cnt, uint64_t len, void* inv, int as_double) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < len; k += stride) {
+    const uint32_t c = cnt[k];
+    if (as_double) reinterpret_cast<double*>(inv)[k] = c ? 1.0 / (double)c : 0.0;
+    else reinterpret_cast<float*>(inv)[k] = c ? 1.0f / (float)c : 0.0f;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T from_double(double x);
+template <> __device__ __forceinline__ double from_double<double>(double x) { return x; }
+template <> __device__ __forceinline__ float from_double<float>(double x) { return (float)x; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_double<__nv_bfloat16>(double x) {
+  return __double2bfloat16(x);
+}
+template <typename T>
+__device__ __forceinline__ double to_double(T x) { return (double)(float)x; }
+template <> __device__ __forceinline__ double to_double<double>(double x) { return x; }
+
+template <typename T>
+__global__ void factor_to_device_kernel(const double* src, uint64_t rows, uint32_t r,
+                                        uint32_t rp, T* dst) {
+  const uint64_t total = rows * rp, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
+    const uint64_t i = q / rp;
+    const uint32_t z = (uint32_t)(q % rp);
+    dst[q] = z < r ? from_double<T>(src[i * r + z]) : from_double<T>(0.0);
+  }
+}
+
+template <typename T>
+__global__ void factor_to_host_kernel(const T* src, uint64_t rows, uint32_t r, uint32_t rp,
+                                      double* dst) {
+  const uint64_t total = rows * r, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
+    const uint64_t i = q / r;
+    const uint32_t z = (uint32_t)(q % r);
+    dst[q] = to_double<T>(src[i * rp + z]);
+  }
+}
+
+constexpr uint32_t kGrid = 1184;  // 148 SMs x 8
+
+}  // namespace
+
+cudaError_t launch_make_keys(const BlockingGeom& g, const uint32_t* rows, const uint32_t* cols,
+                             uint64_t nnz, uint64_t* keys, uint32_t* idx,
+                             unsigned long long* bad, cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  const size_t sm = sizeof(uint64_t) * (g.nb1 + g.nb2 + 2);
+  make_keys_kernel<<<kGrid, 256, sm, st>>>(g, rows, cols, nnz, keys, idx, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_head_flags(const uint64_t* keys, uint64_t nnz, uint32_t* flags,
+                              cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  head_flags_kernel<<<kGrid, 256, 0, st>>>(keys, nnz, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge_runs(const BlockingGeom& g, const uint64_t* keys, const uint32_t* idx,
+                              const uint32_t* pos, uint64_t nnz, const double* vals_in,
+                              const uint32_t* rows_in, const uint32_t* cols_in, uint64_t* ukeys,
+                              uint32_t* urow, uint32_t* ucol, double* uval, cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  merge_runs_kernel<<<kGrid, 256, 0, st>>>(g, keys, idx, pos, nnz, vals_in, rows_in, cols_in,
+                                           ukeys, urow, ucol, uval);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
+                             uint32_t nblocks, uint64_t* block_ptr, cudaStream_t st) {
+  block_ptr_kernel<<<(nblocks + 1 + 255) / 256, 256, 0, st>>>(ukeys, u, block_span, nblocks,
+                                                               block_ptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
+                                uint64_t seed, uint64_t* keys2, uint32_t* idx2,
+                                cudaStream_t st) {
+  if (u == 0) return cudaSuccess;
+  shuffle_keys_kernel<<<kGrid, 256, 0, st>>>(ukeys, u, block_span, seed, keys2, idx2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
+                                  const uint32_t* ucol, const double* uval, uint32_t* row,
+                                  uint32_t* col, void* val, int val_is_double, cudaStream_t st) {
+  if (u == 0) return cudaSuccess;
+  gather_records_kernel<<<kGrid, 256, 0, st>>>(idx, u, urow, ucol, uval, row, col, val,
+                                               val_is_double);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nnz12(const uint32_t* row, const uint32_t* col, uint64_t nnz,
+                               uint32_t* cnt1, uint32_t* cnt2, cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  count_nnz12_kernel<<<kGrid, 256, 0, st>>>(row, col, nnz, cnt1, cnt2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inverse_counts(const uint32_t* cnt, uint64_t len, void* inv, int as_double,
+                                  cudaStream_t st) {
+  if (len == 0) return cudaSuccess;
+  inverse_counts_kernel<<<kGrid, 256, 0, st>>>(cnt, len, inv, as_double);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_factor_to_device(int precision, const double* src, uint64_t rows,
+                                    uint32_t r, uint32_t rp, void* dst, cudaStream_t st) {
+  if (rows == 0) return cudaSuccess;
+  if (precision == kFp64)
+    factor_to_device_kernel<double><<<kGrid, 256, 0, st>>>(src, rows, r, rp, (double*)dst);
+  else if (precision == kFp32)
+    factor_to_device_kernel<float><<<kGrid, 256, 0, st>>>(src, rows, r, rp, (float*)dst);
+  else
+    factor_to_device_kernel<__nv_bfloat16><<<kGrid, 256, 0, st>>>(src, rows, r, rp,
+                                                                  (__nv_bfloat16*)dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_factor_to_host(int precision, const void* src, uint64_t rows, uint32_t r,
+                                  uint32_t rp, double* dst, cudaStream_t st) {
+  if (rows == 0) return cudaSuccess;
+  if (precision == kFp64)
+    factor_to_host_kernel<double><<<kGrid, 256, 0, st>>>((const double*)src, rows, r, rp, dst);
+  else if (precision == kFp32)
+    factor_to_host_kernel<float><<<kGrid, 256, 0, st>>>((const float*)src, rows, r, rp, dst);
+  else
+    factor_to_host_kernel<__nv_bfloat16><<<kGrid, 256, 0, st>>>((const __nv_bfloat16*)src, rows,
+                                                                r, rp, dst);
+  return cudaGetLastError();
+}
+
+}  // namespace dsgdpp

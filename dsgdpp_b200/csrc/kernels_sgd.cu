@@ -1,0 +1,502 @@
+// kernels_sgd.cu -- the per-nonzero SGD step of DSGD++ on sm_100a.
+//
+// Reference hot loop: SgdRunner::updateWor (mf/sgd/sgd_impl.h:293-351) calling
+// UpdateNzslL2 / UpdateNzsl / UpdateNzslNzl2 (mf/sgd/functions/update-*.h),
+// one thread per block, d blocks per sub-epoch (mf/sgd/dsgdpp_impl.h:117-263).
+//
+// Two kernels:
+//  * hogwild_subepoch: the throughput path.  The sub-epoch's d blocks share no
+//    row of W and no column of H, so their records form one work list that
+//    every SM draws 32-record chunks from.  Inside a warp, groups of LPN lanes
+//    each own one record; a lane moves VPL 16-byte vectors of the W row and of
+//    the H column.  Within a block updates run concurrently (Hogwild).
+//  * replay_subepoch: the deterministic FP64 mode.  One warp per task walks its
+//    block in the exact point order of the reference and repeats every
+//    floating-point operation of the reference in the same order, without FMA
+//    contraction, so the result matches the CPU restatement bit for bit.
+#include "kernels.cuh"
+
+namespace dsgdpp {
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Eight primes just below 2^31; a prime above the chunk count is coprime to
+// it, so c -> (A c + B) mod C is a permutation of the chunks.
+__constant__ uint32_t kPrimes[8] = {2147483647u, 2147483629u, 2147483587u, 2147483579u,
+                                    2147483563u, 2147483549u, 2147483543u, 2147483497u};
+
+template <typename C>
+__device__ __forceinline__ C clampw(C v, C lo, C hi, C eps) {
+  // UpdateTruncate (mf/sgd/functions/update-truncate.h:50-72)
+  if (v <= lo) return lo + eps;
+  if (v >= hi) return hi - eps;
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_vec(T* p, const typename Elem<T>::C (&f)[Elem<T>::VW],
+                                          const Philox4*) {
+  *reinterpret_cast<uint4*>(p) = Elem<T>::pack(f);
+}
+template <>
+__device__ __forceinline__ void store_vec<__nv_bfloat16>(__nv_bfloat16* p, const float (&f)[8],
+                                                         const Philox4* rnd) {
+  uint32_t w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    uint32_t lo = bf16_sr_bits(f[2 * k], rnd->v[k]);
+    uint32_t hi = bf16_sr_bits(f[2 * k + 1], rnd->v[k] >> 16);
+    w[k] = (lo & 0xffffu) | (hi << 16);
+  }
+  *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+template <typename T, int LPN, int VPL>
+__global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t s) {
+  using E = Elem<T>;
+  using C = typename E::C;
+  constexpr int VW = E::VW;
+  constexpr int NG = 32 / LPN;
+  constexpr bool kSR = sizeof(T) == 2;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Segment* seg = reinterpret_cast<Segment*>(smem_raw);
+  const uint32_t d = a.d;
+  const Segment* gseg = a.segs + (size_t)s * (d + 1);
+  for (uint32_t k = threadIdx.x; k <= d; k += blockDim.x) seg[k] = gseg[k];
+  __syncthreads();
+  const uint32_t total = seg[d].chunk_begin;
+  if (total == 0) return;
+
+  const EpochParams ep = *a.params;
+  const C eps = (C)ep.eps;
+  const C f2 = (C)(ep.eps * 2.0 * a.lambda);
+  const C tmin = (C)a.tmin, tmax = (C)a.tmax;
+  const uint64_t h = mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)s << 17) ^ ep.epoch);
+  uint64_t mulA = 1, addB = 0;
+  if (a.sgd_order == 2) {  // WOR: affine permutation of the chunks
+    mulA = kPrimes[h & 7u] % total;
+    addB = (h >> 8) % total;
+  }
+  const C* inv1 = reinterpret_cast<const C*>(a.inv1);
+  const C* inv2 = reinterpret_cast<const C*>(a.inv2);
+  const C* vals = reinterpret_cast<const C*>(a.val);
+  T* W = reinterpret_cast<T*>(a.W);
+  T* H = reinterpret_cast<T*>(a.H);
+
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t grp = lane / LPN, gl = lane % LPN;
+
+  for (;;) {
+    uint32_t lc = 0;
+    if (lane == 0) lc = atomicAdd(a.counters + s, 1u);
+    lc = __shfl_sync(kFullMask, lc, 0);
+    if (lc >= total) break;
+    uint32_t pc;
+    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
+      pc = (uint32_t)(mix64(h ^ ((uint64_t)lc << 20)) % total);
+    else
+      pc = (uint32_t)((mulA * lc + addB) % total);
+
+    // segment holding chunk pc: the last k with chunk_begin <= pc
+    uint32_t lo = 0, hi = d - 1;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi + 1) >> 1;
+      if (seg[mid].chunk_begin <= pc) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t cin = pc - seg[lo].chunk_begin;
+    const uint64_t rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
+    const uint32_t nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
+    const C cwh = (C)seg[lo].cwh, rw = (C)seg[lo].rho_w, rh = (C)seg[lo].rho_h;
+
+    uint32_t my_row = 0, my_col = 0;
+    C my_x = 0, my_a = 0, my_b = 0;
+    if (lane < nrec) {
+      my_row = a.row[rb + lane];
+      my_col = a.col[rb + lane];
+      my_x = vals[rb + lane];
+      if (a.update == kUpdNzslL2) {
+        my_a = f2 * inv1[my_row];
+        my_b = f2 * inv2[my_col];
+      } else if (a.update == kUpdNzslNzl2) {
+        my_a = f2;
+        my_b = f2;
+      }
+    }
+
+    for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
+      const uint32_t ri = t0 + grp;
+      const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
+      const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
+      const C x = __shfl_sync(kFullMask, my_x, ri);
+      const C ca = __shfl_sync(kFullMask, my_a, ri);
+      const C cb = __shfl_sync(kFullMask, my_b, ri);
+      const bool valid = ri < nrec;
+      T* wp = W + (size_t)row * a.rp;
+      T* hp = H + (size_t)col * a.rp;
+
+      uint4 wv[VPL], hv[VPL];
+      bool live[VPL];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        live[v] = valid && e0 < a.rp;
+        if (live[v]) {
+          wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
+          hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
+        } else {
+          wv[v] = make_uint4(0, 0, 0, 0);
+          hv[v] = make_uint4(0, 0, 0, 0);
+        }
+      }
+      C dot = 0;
+      C wf[VPL][VW], hf[VPL][VW];
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        E::unpack(wv[v], wf[v]);
+        E::unpack(hv[v], hf[v]);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+      }
+#pragma unroll
+      for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+
+      const C f1 = (C)-2 * eps * (x - dot * cwh);
+      const C fw = f1 * rw, fh = f1 * rh;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        if (!live[v]) continue;
+        C nw[VW], nh[VW];
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+          nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+        }
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        if (a.truncate) {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            if (e0 + e < a.r) {
+              nw[e] = clampw(nw[e], tmin, tmax, eps);
+              nh[e] = clampw(nh[e], tmin, tmax, eps);
+            }
+        }
+        Philox4 rw4, rh4;
+        if (kSR) {
+          const uint64_t rec = rb + ri;
+          rw4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
+          rh4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
+                              ep.key0, ep.key1);
+        }
+        store_vec<T>(wp + e0, nw, &rw4);
+        store_vec<T>(hp + e0, nh, &rh4);
+      }
+    }
+  }
+}
+
+__global__ void build_segments_kernel(SegBuildArgs a) {
+  // one CTA per sub-epoch; thread id = task id (d <= 1024)
+  __shared__ uint32_t scan[1024];
+  const uint32_t s = blockIdx.x, d = a.d, id = threadIdx.x;
+  uint32_t chunks = 0;
+  uint64_t rb = 0;
+  uint32_t cnt = 0, b2 = 0;
+  if (id < d) {
+    b2 = a.schedule[(size_t)s * d + id];
+    const uint64_t blk = (uint64_t)id * 2 * d + b2;
+    rb = a.block_ptr[blk];
+    cnt = (uint32_t)(a.block_ptr[blk + 1] - rb);
+    chunks = (cnt + kChunk - 1) / kChunk;
+  }
+  scan[id] = chunks;
+  __syncthreads();
+  // Hillis-Steele inclusive scan over blockDim.x entries
+  for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+    uint32_t v = id >= off ? scan[id - off] : 0;
+    __syncthreads();
+    scan[id] += v;
+    __syncthreads();
+  }
+  Segment* out = a.segs + (size_t)s * (d + 1);
+  if (id < d) {
+    Segment g;
+    g.rec_begin = rb;
+    g.count = cnt;
+    g.chunk_begin = scan[id] - chunks;
+    if (a.sigma) {
+      const float* sg = a.sigma + ((size_t)s * d + id) * 3;
+      g.cwh = sg[0]; g.rho_w = sg[1]; g.rho_h = sg[2];
+    } else {
+      g.cwh = 1.f; g.rho_w = 1.f; g.rho_h = 1.f;
+    }
+    g.col_block = b2;
+    out[id] = g;
+  }
+  if (id == 0) {
+    Segment e;
+    e.rec_begin = 0; e.count = 0; e.chunk_begin = scan[d - 1];
+    e.cwh = e.rho_w = e.rho_h = 1.f; e.col_block = 0xffffffffu;
+    out[d] = e;
+    a.counters[s] = 0;
+  }
+}
+
+// ---- deterministic FP64 replay ---------------------------------------------
+constexpr int kReplayMaxK = 8;  // r <= 256
+
+__global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint32_t s) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t id = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (id >= a.d) return;
+  const uint32_t d = a.d, r = a.r;
+  const uint32_t b2 = a.schedule[(size_t)s * d + id];
+  const uint64_t blk = (uint64_t)id * 2 * d + b2;
+  const uint64_t rb = a.block_ptr[blk];
+  const uint64_t n = a.block_ptr[blk + 1] - rb;
+  const uint32_t* pos = a.positions + a.pos_offset[(size_t)s * d + id];
+  const double eps = a.params->eps;
+  const int kmax = (int)((r + 31) / 32);
+  // f1 = eps * -2. * (x - wh); f2 = eps * 2. * lambda
+  const double em2 = __dmul_rn(eps, -2.0);
+  const double f2 = __dmul_rn(__dmul_rn(eps, 2.0), a.lambda);
+
+  for (uint64_t q = 0; q < n; ++q) {
+    const uint64_t rec = rb + pos[q];
+    const uint32_t i = a.row[rec], j = a.col[rec];
+    const double x = a.val[rec];
+    double* w = a.W + (size_t)i * a.rp;
+    double* h = a.H + (size_t)j * a.rp;
+    double wz[kReplayMaxK], hz[kReplayMaxK], pz[kReplayMaxK];
+#pragma unroll
+    for (int k = 0; k < kReplayMaxK; ++k) {
+      const uint32_t z = (uint32_t)k * 32 + lane;
+      wz[k] = 0; hz[k] = 0; pz[k] = 0;
+      if (k < kmax && z < r) {
+        wz[k] = w[z];
+        hz[k] = h[z];
+        pz[k] = __dmul_rn(wz[k], hz[k]);
+      }
+    }
+    // wh = sum_z w[z] h[z] in z order (every lane computes the same sum)
+    double wh = 0;
+#pragma unroll
+    for (int k = 0; k < kReplayMaxK; ++k) {
+      if (k >= kmax) break;
+      for (uint32_t l = 0; l < 32; ++l) {
+        if ((uint32_t)k * 32 + l >= r) break;
+        wh = __dadd_rn(wh, __shfl_sync(kFullMask, pz[k], l));
+      }
+    }
+    const double f1 = __dmul_rn(em2, __dsub_rn(x, wh));
+    double f3 = 0, f4 = 0;
+    if (a.update == kUpdNzslL2) {
+      f3 = __ddiv_rn(1.0, (double)a.cnt1[i]);
+      f4 = __ddiv_rn(1.0, (double)a.cnt2[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < kReplayMaxK; ++k) {
+      const uint32_t z = (uint32_t)k * 32 + lane;
+      if (k >= kmax || z >= r) continue;
+      const double t = wz[k];
+      double nw, nh;
+      if (a.update == kUpdNzsl) {
+        nw = __dsub_rn(wz[k], __dmul_rn(f1, hz[k]));
+        nh = __dsub_rn(hz[k], __dmul_rn(f1, t));
+      } else if (a.update == kUpdNzslL2) {
+        nw = __dsub_rn(wz[k], __dadd_rn(__dmul_rn(f1, hz[k]), __dmul_rn(__dmul_rn(f2, wz[k]), f3)));
+        nh = __dsub_rn(hz[k], __dadd_rn(__dmul_rn(f1, t), __dmul_rn(__dmul_rn(f2, hz[k]), f4)));
+      } else {
+        nw = __dsub_rn(wz[k], __dadd_rn(__dmul_rn(f1, hz[k]), __dmul_rn(f2, wz[k])));
+        nh = __dsub_rn(hz[k], __dadd_rn(__dmul_rn(f1, t), __dmul_rn(f2, hz[k])));
+      }
+      if (a.truncate) {
+        if (nw <= a.tmin) nw = __dadd_rn(a.tmin, eps);
+        else if (nw >= a.tmax) nw = __dsub_rn(a.tmax, eps);
+        if (nh <= a.tmin) nh = __dadd_rn(a.tmin, eps);
+        else if (nh >= a.tmax) nh = __dsub_rn(a.tmax, eps);
+      }
+      w[z] = nw;
+      h[z] = nh;
+    }
+    __syncwarp();
+  }
+}
+
+// RegularizeL2 (mf/sgd/functions/regularize-l2.h:26-45) applied by every task
+// after sub-epoch s: each W block and the sub-epoch's H blocks are scaled.
+__global__ void regularize_exact_kernel(double* W, double* H, uint64_t m, uint64_t n,
+                                        uint32_t rp, uint32_t r, const uint64_t* off2,
+                                        const uint8_t* mask, uint32_t d,
+                                        const EpochParams* params, double lambda, int truncate,
+                                        double tmin, double tmax) {
+  const double eps = __ddiv_rn(params->eps, (double)d);  // eps/d: rescaleStratumStepsize()
+  double factor = __dsub_rn(1.0, __dmul_rn(__dmul_rn(eps, 2.0), lambda));
+  if (factor < 0.5) factor = __ddiv_rn(0.25, __dsub_rn(1.0, factor));
+  const uint64_t wtot = m * rp, htot = n * rp;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < wtot + htot; q += stride) {
+    double* p;
+    uint64_t z;
+    if (q < wtot) {
+      p = W + q;
+      z = q % rp;
+    } else {
+      const uint64_t hq = q - wtot, j = hq / rp;
+      // column block of j
+      uint32_t lo = 0, hi = 2 * d - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (off2[mid] <= j) lo = mid; else hi = mid - 1;
+      }
+      if (!mask[lo]) continue;
+      p = H + hq;
+      z = hq % rp;
+    }
+    if (z >= r) continue;
+    double v = __dmul_rn(*p, factor);
+    if (truncate) {
+      if (v <= tmin) v = __dadd_rn(tmin, eps);
+      else if (v >= tmax) v = __dsub_rn(tmax, eps);
+    }
+    *p = v;
+  }
+}
+
+// scales[b2] scales H column block b2, scales[nb2] scales all of W
+template <typename T>
+__global__ void normalize_kernel(T* W, T* H, uint64_t m, uint64_t n, uint32_t rp,
+                                 const float* scales, const uint64_t* off2, uint32_t nb2) {
+  const float sw = scales[nb2];
+  const float* sh = scales;
+  const uint64_t wtot = m * rp, htot = n * rp;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < wtot + htot; q += stride) {
+    if (q < wtot) {
+      W[q] = (T)((float)W[q] * sw);
+    } else {
+      const uint64_t hq = q - wtot, j = hq / rp;
+      uint32_t lo = 0, hi = nb2 - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (off2[mid] <= j) lo = mid; else hi = mid - 1;
+      }
+      H[hq] = (T)((float)H[hq] * sh[lo]);
+    }
+  }
+}
+template <>
+__global__ void normalize_kernel<double>(double* W, double* H, uint64_t m, uint64_t n,
+                                         uint32_t rp, const float* scales,
+                                         const uint64_t* off2, uint32_t nb2) {
+  const float sw = scales[nb2];
+  const float* sh = scales;
+  const uint64_t wtot = m * rp, htot = n * rp;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < wtot + htot; q += stride) {
+    if (q < wtot) {
+      W[q] *= (double)sw;
+    } else {
+      const uint64_t hq = q - wtot, j = hq / rp;
+      uint32_t lo = 0, hi = nb2 - 1;
+      while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (off2[mid] <= j) lo = mid; else hi = mid - 1;
+      }
+      H[hq] *= (double)sh[lo];
+    }
+  }
+}
+
+template <typename T, int LPN, int VPL>
+void* hogwild_fn() {
+  return reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL>);
+}
+
+template <typename T>
+void* pick_hogwild(uint32_t lanes, uint32_t vecs) {
+#define DSGDPP_CASE(L, V) \
+  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>();
+  DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
+  DSGDPP_CASE(2, 2) DSGDPP_CASE(4, 2) DSGDPP_CASE(8, 2) DSGDPP_CASE(16, 2) DSGDPP_CASE(32, 2)
+  DSGDPP_CASE(32, 4)
+#undef DSGDPP_CASE
+  return nullptr;
+}
+
+void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs) {
+  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs);
+  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs);
+  return pick_hogwild<__nv_bfloat16>(lanes, vecs);
+}
+
+}  // namespace
+
+cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st) {
+  uint32_t threads = 32;
+  while (threads < a.d) threads <<= 1;
+  if (threads > 1024) return cudaErrorInvalidValue;
+  build_segments_kernel<<<2 * a.d, threads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs);
+  if (!fn) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * (d + 1)) !=
+      cudaSuccess)
+    return 0;
+  return n;
+}
+
+cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs,
+                                    const HogwildArgs& a, uint32_t s, uint32_t grid,
+                                    cudaStream_t st) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs);
+  if (!fn) return cudaErrorInvalidValue;
+  HogwildArgs args = a;
+  uint32_t sub = s;
+  void* params[] = {&args, &sub};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(Segment) * (a.d + 1), st);
+}
+
+cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st) {
+  if (a.r > 32u * kReplayMaxK) return cudaErrorInvalidValue;
+  const uint32_t warps_per_cta = 4;
+  replay_subepoch_kernel<<<(a.d + warps_per_cta - 1) / warps_per_cta, 32 * warps_per_cta, 0, st>>>(
+      a, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
+                                    uint32_t r, const uint64_t* off2, const uint8_t* mask,
+                                    uint32_t d, const EpochParams* params, double lambda,
+                                    int truncate, double tmin, double tmax, cudaStream_t st) {
+  regularize_exact_kernel<<<1184, 256, 0, st>>>(W, H, m, n, rp, r, off2, mask, d, params, lambda,
+                                                truncate, tmin, tmax);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(int precision, void* W, void* H, uint64_t m, uint64_t n,
+                             uint32_t rp, const float* scales, const uint64_t* off2,
+                             uint32_t nb2, cudaStream_t st) {
+  if (precision == kFp64)
+    normalize_kernel<double><<<1184, 256, 0, st>>>((double*)W, (double*)H, m, n, rp, scales,
+                                                    off2, nb2);
+  else if (precision == kFp32)
+    normalize_kernel<float><<<1184, 256, 0, st>>>((float*)W, (float*)H, m, n, rp, scales, off2,
+                                                   nb2);
+  else
+    normalize_kernel<__nv_bfloat16><<<1184, 256, 0, st>>>(
+        (__nv_bfloat16*)W, (__nv_bfloat16*)H, m, n, rp, scales, off2, nb2);
+  return cudaGetLastError();
+}
+
+}  // namespace dsgdpp

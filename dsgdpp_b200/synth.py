@@ -1,0 +1,82 @@
+"""Seeded synthetic matrices of the DSGD++ benchmark shapes.
+
+The reference benchmarks on Netflix / KDD-Cup data (not available here) and on
+matrices from its own generator (mf/matrix/op/generate.h, tools/mfgenerate.cc).
+These generators produce stand-ins of the stated shapes and distributions:
+
+* uniform:  positions uniform over distinct (i, j) pairs;
+* zipf:     row and column degrees Zipf(s), positions drawn by degree weight
+            (ids randomly permuted so heavy rows spread over all blocks),
+            duplicates rejected;
+values are a rank-k ground truth W* H* (entries N(0,1)/sqrt(k)) plus
+N(0, noise^2); initial factors are U[-0.5, 0.5].
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Problem:
+    m: int
+    n: int
+    rows: np.ndarray      # uint32, 0-based
+    cols: np.ndarray
+    vals: np.ndarray      # float64
+    trows: np.ndarray
+    tcols: np.ndarray
+    tvals: np.ndarray
+    W0: np.ndarray        # m x r
+    H0: np.ndarray        # n x r (column j of H contiguous)
+
+
+def _distinct_uniform(rng, m, n, count):
+    keys = np.empty(0, np.uint64)
+    while len(keys) < count:
+        need = int((count - len(keys)) * 1.1) + 16
+        k = rng.integers(0, m * n, size=need, dtype=np.uint64)
+        keys = np.unique(np.concatenate([keys, k]))
+    keys = rng.permutation(keys)[:count]
+    return keys
+
+
+def _zipf_weights(rng, size, s):
+    w = 1.0 / np.arange(1, size + 1, dtype=np.float64) ** s
+    return rng.permutation(w / w.sum())
+
+
+def _distinct_weighted(rng, m, n, count, s_row, s_col, max_rounds=60):
+    pr = _zipf_weights(rng, m, s_row)
+    pc = _zipf_weights(rng, n, s_col)
+    cr, cc = np.cumsum(pr), np.cumsum(pc)
+    keys = np.empty(0, np.uint64)
+    for _ in range(max_rounds):
+        if len(keys) >= count:
+            break
+        need = int((count - len(keys)) * 1.3) + 16
+        i = np.minimum(np.searchsorted(cr, rng.random(need)), m - 1).astype(np.uint64)
+        j = np.minimum(np.searchsorted(cc, rng.random(need)), n - 1).astype(np.uint64)
+        keys = np.unique(np.concatenate([keys, i * np.uint64(n) + j]))
+    if len(keys) < count:
+        raise ValueError("degree distribution too skewed for this many distinct entries")
+    return rng.permutation(keys)[:count]
+
+
+def make(m, n, nnz, nnz_test, rank_true, r, noise, seed, kind="uniform", s_row=1.1,
+         s_col=1.1):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        keys = _distinct_uniform(rng, m, n, nnz + nnz_test)
+    else:
+        keys = _distinct_weighted(rng, m, n, nnz + nnz_test, s_row, s_col)
+    rows = (keys // np.uint64(n)).astype(np.uint32)
+    cols = (keys % np.uint64(n)).astype(np.uint32)
+    Ws = rng.standard_normal((m, rank_true)) / np.sqrt(rank_true)
+    Hs = rng.standard_normal((n, rank_true)) / np.sqrt(rank_true)
+    vals = np.einsum("ij,ij->i", Ws[rows], Hs[cols]) + noise * rng.standard_normal(len(keys))
+    W0 = rng.uniform(-0.5, 0.5, (m, r))
+    H0 = rng.uniform(-0.5, 0.5, (n, r))
+    return Problem(m, n, rows[:nnz], cols[:nnz], vals[:nnz], rows[nnz:], cols[nnz:],
+                   vals[nnz:], W0, H0)

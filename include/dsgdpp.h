@@ -1,0 +1,211 @@
+/*
+ * dsgdpp.h -- C ABI of the B200 DSGD++ epoch.
+ *
+ * The reference exposes this path as C++ templates, not as a runtime ABI:
+ *   - DsgdPpRunner::run / DsgdPpRunner::epoch      mf/sgd/dsgdpp.h:102-130
+ *   - the update functors (UpdateConcept)           mf/sgd/functions/functions.h:21-45
+ *   - the regularize functors (RegularizeConcept)   mf/sgd/functions/functions.h:47-63
+ *   - the losses (LossConcept)                      mf/loss/loss.h:30-57
+ *   - the adaptive decays (AdaptiveDecayConcept)    mf/sgd/decay/decay.h:35-67
+ * The entry points below replace those for one GPU: plain C types, every
+ * call returns an int status (0 = DSGDPP_OK, negative = error class) and
+ * dsgdpp_last_error(ctx) gives the message; no C++ exception crosses the ABI.
+ * One host thread drives a context; its work is ordered on one CUDA stream.
+ * The context owns all device memory; host buffers are caller-owned and
+ * copied.  There is no CPU fallback: without a usable GPU dsgdpp_create
+ * fails with DSGDPP_E_CUDA.
+ *
+ * Layouts follow the reference (mf/types.h:33-42): V is given as a global
+ * 0-based coordinate list; W is m x r row-major (DenseMatrix); H is r x n
+ * column-major (DenseMatrixCM), i.e. column j's r entries are contiguous.
+ */
+#ifndef DSGDPP_H
+#define DSGDPP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSGDPP_ABI_VERSION 1
+
+typedef struct dsgdpp_ctx dsgdpp_ctx;
+
+/* status codes */
+#define DSGDPP_OK 0
+#define DSGDPP_E_INVALID (-1)     /* rg::InvalidArgumentException */
+#define DSGDPP_E_CUDA (-2)        /* CUDA runtime error, no device */
+#define DSGDPP_E_IO (-3)          /* rg::IOException */
+#define DSGDPP_E_UNSUPPORTED (-4) /* rg::NotImplementedException */
+#define DSGDPP_E_STATE (-5)       /* call out of order (e.g. epoch before data) */
+#define DSGDPP_E_NOMEM (-6)       /* device allocation failed */
+
+/* --update / --loss / --regularize functors (tools/mfdsgdpp.cc:162-359) */
+#define DSGDPP_UPDATE_NZSL 0       /* UpdateNzsl        update-nzsl.h:33-50     */
+#define DSGDPP_UPDATE_NZSL_L2 1    /* UpdateNzslL2(l)   update-nzsl-l2.h:34-57  */
+#define DSGDPP_UPDATE_NZSL_NZL2 2  /* UpdateNzslNzl2(l) update-nzsl-nzl2.h:34-53 */
+#define DSGDPP_REGULARIZE_NONE 0   /* RegularizeNone    regularize-none.h:22-34 */
+#define DSGDPP_REGULARIZE_L2 1     /* RegularizeL2(l)   regularize-l2.h:26-50   */
+#define DSGDPP_LOSS_NZSL 0         /* NzslLoss                                  */
+#define DSGDPP_LOSS_NZSL_L2 1      /* SumLoss<NzslLoss, L2Loss(l)>              */
+#define DSGDPP_LOSS_NZSL_NZL2 2    /* SumLoss<NzslLoss, Nzl2Loss(l)>            */
+/* --sgd-order (mf/sgd/sgd.h:39) and --stratum-order (mf/sgd/dsgd.h:29) */
+#define DSGDPP_SGD_SEQ 0
+#define DSGDPP_SGD_WR 1
+#define DSGDPP_SGD_WOR 2
+#define DSGDPP_STRATUM_SEQ 0
+#define DSGDPP_STRATUM_RSEQ 1
+#define DSGDPP_STRATUM_WR 2
+#define DSGDPP_STRATUM_WOR 3
+#define DSGDPP_STRATUM_COWOR 4
+/* factor storage; arithmetic is FP64 for FP64 storage, FP32 otherwise */
+#define DSGDPP_FP64 0
+#define DSGDPP_FP32 1
+#define DSGDPP_BF16 2 /* stochastic rounding on every store */
+/* execution of a block's records */
+#define DSGDPP_EXEC_REPLAY 0  /* sequential per block, reference point order, FP64 only */
+#define DSGDPP_EXEC_HOGWILD 1 /* all SMs on the sub-epoch's records (Hogwild within a block) */
+/* launch form of an epoch */
+#define DSGDPP_LAUNCH_STREAM 0 /* 2d kernel launches per epoch */
+#define DSGDPP_LAUNCH_GRAPH 1  /* the epoch captured once as a CUDA graph and replayed */
+/* matrices */
+#define DSGDPP_TRAIN 0
+#define DSGDPP_TEST 1
+/* decays (mf/sgd/decay) */
+#define DSGDPP_DECAY_CONST 0      /* DecayConstant(eps)              decay_constant.h:31-63 */
+#define DSGDPP_DECAY_BOLDDRIVER 1 /* BoldDriver(eps, dec, inc)        decay_bolddriver.h:33-92 */
+
+typedef struct dsgdpp_config {
+  uint64_t m, n;          /* size of V: rows (of W) and columns (of H) */
+  uint32_t rank;          /* r */
+  uint32_t d;             /* tasks = row blocks; V is blocked d x 2d (1 <= d <= 1024) */
+  int32_t precision;      /* DSGDPP_FP64 / FP32 / BF16 */
+  int32_t exec;           /* DSGDPP_EXEC_* */
+  int32_t launch;         /* DSGDPP_LAUNCH_* */
+  int32_t update;         /* DSGDPP_UPDATE_* */
+  double update_lambda;
+  int32_t regularize;     /* DSGDPP_REGULARIZE_* */
+  double regularize_lambda;
+  int32_t loss;           /* DSGDPP_LOSS_* */
+  double loss_lambda;
+  int32_t truncate;       /* UpdateTruncate / RegularizeTruncate when nonzero */
+  double truncate_min, truncate_max;
+  int32_t sgd_order;      /* DSGDPP_SGD_* */
+  int32_t stratum_order;  /* DSGDPP_STRATUM_* */
+  int32_t device;         /* CUDA device ordinal */
+  uint32_t lanes_per_nnz; /* Hogwild lanes per record: 0 = auto, else 2..32 */
+  uint32_t vecs_per_lane; /* Hogwild 16-byte vectors per lane: 0 = auto */
+  uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
+  uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
+} dsgdpp_config;
+
+/* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */
+typedef struct dsgdpp_trace_row {
+  uint64_t epoch;
+  double loss, test_loss, eps;
+  double time_eps, time_epoch, time_loss, time_test_loss;
+} dsgdpp_trace_row;
+
+/* ---- context ------------------------------------------------------------ */
+/* Fills c with the reference defaults: WOR / COWOR, Nzsl_L2(1) update and
+ * loss, regularize None, FP32 Hogwild, graph launch, auto tuning. */
+void dsgdpp_config_init(dsgdpp_config* c);
+/* replaces: DsgdPpJob / DsgdPpFactorizationData construction
+ * (mf/sgd/dsgdpp.h:38-59, mf/sgd/dsgdpp-factorization.h:58-64) */
+int dsgdpp_create(const dsgdpp_config* c, dsgdpp_ctx** out);
+/* message of the calling thread's last failed dsgdpp_create */
+const char* dsgdpp_create_error(void);
+void dsgdpp_destroy(dsgdpp_ctx* ctx);
+const char* dsgdpp_last_error(const dsgdpp_ctx* ctx);
+const char* dsgdpp_status_string(int status);
+int dsgdpp_abi_version(void);
+
+/* ---- data --------------------------------------------------------------- */
+/* replaces: getDataMatrices / loadMatrix blocking (mf/matrix/io/
+ * generateDistributedMatrix_impl.h:692-744, read_impl.h:364-486).  Global
+ * 0-based coordinates from host memory; blocked d x 2d and sorted (i, j)
+ * inside each block on the GPU, duplicate entries summed.  For the training
+ * matrix this also counts nnz1 / nnz2 (mf/matrix/op/nnz.h:124-163). */
+int dsgdpp_set_matrix(dsgdpp_ctx* ctx, int which, uint64_t nnz, const uint32_t* rows,
+                      const uint32_t* cols, const double* vals);
+/* replaces: getFactors (generateDistributedMatrix_impl.h:655-690) */
+int dsgdpp_set_factors(dsgdpp_ctx* ctx, const double* W, const double* H);
+/* replaces: unblock + the factor arrays read by writeMatrix (tools/mfdsgdpp.cc:145-159) */
+int dsgdpp_get_factors(dsgdpp_ctx* ctx, double* W, double* H);
+/* nnz per block (d x 2d row-major) of the blocked matrix */
+int dsgdpp_block_nnz(dsgdpp_ctx* ctx, int which, uint64_t* out);
+/* per-row / per-column counts of the training matrix (nnz12) */
+int dsgdpp_nnz12(dsgdpp_ctx* ctx, uint64_t* nnz1, uint64_t* nnz2, uint64_t* nnz12max);
+
+/* ---- epoch -------------------------------------------------------------- */
+/* Seeds the master generator (the Random32 of DsgdPpRunner, tools/mfdsgdpp.cc:542). */
+int dsgdpp_seed(dsgdpp_ctx* ctx, uint32_t seed);
+/* replaces: DsgdPpRunner::epoch(job, eps) (mf/sgd/dsgdpp_impl.h:282-349):
+ * draws the red/blue split, the stratum schedule and the task seeds from the
+ * master generator, then runs the 2d sub-epochs on the GPU. */
+int dsgdpp_epoch(dsgdpp_ctx* ctx, double eps);
+/* The same with a caller-given schedule (2d x d, row = sub-epoch, column =
+ * task id, entry = column block) and task seeds (d). */
+int dsgdpp_epoch_explicit(dsgdpp_ctx* ctx, double eps, const uint32_t* schedule,
+                          const uint32_t* task_seeds);
+/* Device time of the last epoch's kernels in milliseconds. */
+int dsgdpp_last_epoch_ms(dsgdpp_ctx* ctx, double* ms);
+/* Per-kernel timing of the Hogwild sub-epoch kernels: when on, epochs launch
+ * on the stream (no graph) with an event around every sub-epoch kernel;
+ * dsgdpp_kernel_timing returns their summed time and launch count since the
+ * timing was switched on.  No reference counterpart (instrumentation). */
+int dsgdpp_set_kernel_timing(dsgdpp_ctx* ctx, int on);
+int dsgdpp_kernel_timing(dsgdpp_ctx* ctx, double* total_ms, uint64_t* launches);
+/* The Hogwild launch shape chosen: lanes per record, 16-byte vectors per lane,
+ * CTAs in the grid. */
+int dsgdpp_launch_shape(dsgdpp_ctx* ctx, uint32_t* lanes, uint32_t* vecs, uint32_t* grid);
+
+/* ---- losses (FP64 accumulation) ------------------------------------------- */
+/* replaces: the configured training loss, SumLoss<NzslLoss, L2Loss|Nzl2Loss>
+ * or NzslLoss (mf/loss/loss.h:88-112) */
+int dsgdpp_loss(dsgdpp_ctx* ctx, double* out);
+/* replaces: NzslLoss (mf/loss/nzsl.h:160-185); which = TRAIN or TEST */
+int dsgdpp_nzsl(dsgdpp_ctx* ctx, int which, double* out);
+/* replaces: l2 over W and over H (mf/loss/l2.h:134-145) */
+int dsgdpp_l2(dsgdpp_ctx* ctx, double* w2, double* h2);
+/* replaces: nzl2 over W and over H (mf/loss/nzl2.h:246-289) */
+int dsgdpp_nzl2(dsgdpp_ctx* ctx, double* w, double* h);
+
+/* ---- runner --------------------------------------------------------------- */
+/* replaces: DsgdPpRunner::run -> detail::defaultRunner (mf/sgd/sgd_impl.h:34-145):
+ * loss and test loss, then per epoch: decay, epoch, loss, test loss.  trace
+ * receives epochs+1 rows (row 0 = the initial losses, eps NaN).  The test loss
+ * is skipped (NaN) when no test matrix was set. */
+int dsgdpp_run(dsgdpp_ctx* ctx, uint32_t epochs, int decay, double eps0, double decrease,
+               double increase, dsgdpp_trace_row* trace);
+int dsgdpp_sync(dsgdpp_ctx* ctx);
+
+/* ---- host utilities (no GPU needed) --------------------------------------- */
+/* rg::Random32 as pinned by this library (MT19937, Boost bucket nextInt). */
+typedef struct dsgdpp_rng dsgdpp_rng;
+dsgdpp_rng* dsgdpp_rng_create(uint32_t seed);
+void dsgdpp_rng_destroy(dsgdpp_rng* rng);
+uint32_t dsgdpp_rng_next(dsgdpp_rng* rng);
+uint32_t dsgdpp_rng_next_int(dsgdpp_rng* rng, uint32_t n);
+/* DsgdPpRunner::epoch's master-generator draws (mf/sgd/dsgdpp_impl.h:289-344) */
+void dsgdpp_draw_schedule(dsgdpp_rng* master, uint32_t d, int stratum_order,
+                          uint32_t* schedule, uint32_t* task_seeds);
+/* detail::computeDsgdSchedule (mf/sgd/dsgd_impl.h:246-325): (w t) x (w t) */
+void dsgdpp_dsgd_schedule(dsgdpp_rng* rng, uint32_t w, uint32_t t, int stratum_order,
+                          uint32_t* out);
+/* SgdRunner point orders of one epoch for an explicit schedule: for
+ * s = 0..2d-1, task id = 0..d-1, the positions inside block (id, schedule[s][id])
+ * given the block sizes block_nnz (d x 2d).  Returns the count written. */
+uint64_t dsgdpp_point_orders(uint32_t d, int sgd_order, const uint64_t* block_nnz,
+                             const uint32_t* schedule, const uint32_t* task_seeds,
+                             uint32_t* out);
+/* computeDefaultBlockOffsets (mf/matrix/distributed_matrix_impl.cc:24-40) */
+void dsgdpp_block_offsets(uint64_t size, uint32_t blocks, uint64_t* out);
+/* Philox4x32-10 of the BF16 stochastic rounding, for known-answer checks */
+void dsgdpp_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,266 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerances:
+* FP64 replay factors: bit-identical to the oracle (the bar is 1e-10 relative
+  per entry; the replay repeats every operation in the reference order);
+* FP64 losses: 1e-12 relative (the terms are identical, only the summation
+  order differs);
+* blocking, counts, schedules: exact;
+* FP32 / BF16 Hogwild runs: final test RMSE within a stated tolerance of the
+  FP64 oracle's, since updates inside a block run concurrently.
+"""
+import numpy as np
+import pytest
+
+import dsgdpp_b200 as P
+from dsgdpp_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+LOSS_RTOL = 1e-12
+
+
+def _problem(m=500, n=400, nnz=6000, ntest=600, r=10, seed=5, kind="uniform"):
+    return synth.make(m, n, nnz, ntest, rank_true=min(r, 8), r=r, noise=0.1, seed=seed,
+                      kind=kind)
+
+
+def _pair(p, r, d, precision="fp64", exec="replay", launch="stream", **kw):
+    okw = {k: v for k, v in kw.items() if k in ("update", "update_lambda", "regularize",
+                                                 "regularize_lambda", "loss", "loss_lambda",
+                                                 "truncate", "sgd_order", "stratum_order")}
+    ref = O.Problem(p.m, p.n, r, d, p.rows, p.cols, p.vals, p.trows, p.tcols, p.tvals)
+    ref.configure(**okw)
+    ref.set_factors(p.W0, p.H0)
+    cfg = P.Config(m=p.m, n=p.n, rank=r, d=d, precision=precision, exec=exec, launch=launch,
+                   **{k: v for k, v in kw.items()})
+    ctx = P.Context(cfg)
+    ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+    ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+    ctx.set_factors(p.W0, p.H0)
+    return ref, ctx
+
+
+@pytest.mark.parametrize("update", ["Nzsl", "Nzsl_L2", "Nzsl_Nzl2"])
+@pytest.mark.parametrize("sgd_order", ["SEQ", "WR", "WOR"])
+@pytest.mark.parametrize("truncate", [None, (-0.3, 0.3)])
+def test_replay_bit_exact(update, sgd_order, truncate):
+    p = _problem()
+    d = 3
+    ref, ctx = _pair(p, 10, d, update=update, update_lambda=0.5, sgd_order=sgd_order,
+                     truncate=truncate, loss="Nzsl")
+    with ctx:
+        R = P.Random32(77)
+        for _ in range(2):
+            sched, seeds = P.draw_schedule(R, d, "COWOR")
+            ctx.epoch_explicit(0.02, sched, seeds)
+            ref.epoch_explicit(0.02, sched, seeds)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+
+
+@pytest.mark.parametrize("r", [1, 3, 32, 33, 64, 128])
+def test_replay_ranks(r):
+    p = _problem(m=300, n=200, nnz=3000, r=r)
+    d = 2
+    ref, ctx = _pair(p, r, d)
+    with ctx:
+        sched, seeds = P.draw_schedule(P.Random32(r), d, "WOR")
+        ctx.epoch_explicit(0.01, sched, seeds)
+        ref.epoch_explicit(0.01, sched, seeds)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+
+
+def test_replay_l2_regularize_exact():
+    p = _problem()
+    d = 4
+    ref, ctx = _pair(p, 10, d, update="Nzsl", regularize="L2", regularize_lambda=0.05,
+                     loss="Nzsl_L2", loss_lambda=0.05)
+    with ctx:
+        R = P.Random32(3)
+        for _ in range(2):
+            sched, seeds = P.draw_schedule(R, d, "COWOR")
+            ctx.epoch_explicit(0.05, sched, seeds)
+            ref.epoch_explicit(0.05, sched, seeds)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+
+
+@pytest.mark.parametrize("stratum_order", ["SEQ", "RSEQ", "WR", "WOR", "COWOR"])
+def test_replay_master_rng_epochs(stratum_order):
+    # dsgdpp_epoch draws the schedule itself, like DsgdPpRunner::epoch
+    p = _problem()
+    d = 2
+    ref, ctx = _pair(p, 10, d, stratum_order=stratum_order)
+    with ctx:
+        ctx.seed(1499881717)
+        ref.seed(1499881717)
+        for _ in range(3):
+            ctx.epoch(0.01)
+            ref.epoch(0.01)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+
+
+@pytest.mark.parametrize("loss", ["Nzsl", "Nzsl_L2", "Nzsl_Nzl2"])
+def test_loss_parity(loss):
+    p = _problem(m=2000, n=1500, nnz=60000, ntest=5000, r=16)
+    ref, ctx = _pair(p, 16, 4, loss=loss, loss_lambda=0.3)
+    with ctx:
+        assert ctx.loss() == pytest.approx(ref.loss(), rel=LOSS_RTOL)
+        assert ctx.nzsl(P.TEST) == pytest.approx(ref.nzsl(1), rel=LOSS_RTOL)
+        assert ctx.nzsl(P.TRAIN) == pytest.approx(ref.nzsl(0), rel=LOSS_RTOL)
+        for a, b in zip(ctx.l2(), ref.l2()):
+            assert a == pytest.approx(b, rel=LOSS_RTOL)
+        for a, b in zip(ctx.nzl2(), ref.nzl2()):
+            assert a == pytest.approx(b, rel=LOSS_RTOL)
+
+
+def test_loss_parity_fp32_and_bf16_factors():
+    # the FP64 loss of stored low-precision factors equals the oracle's loss of
+    # the same factors read back as doubles
+    p = _problem(m=2000, n=1500, nnz=40000, r=32)
+    for prec in ("fp32", "bf16"):
+        ref, ctx = _pair(p, 32, 4, precision=prec, exec="hogwild")
+        with ctx:
+            W, H = ctx.get_factors()
+            ref.set_factors(W, H)
+            assert ctx.nzsl(P.TRAIN) == pytest.approx(ref.nzsl(0), rel=LOSS_RTOL)
+            assert ctx.loss() == pytest.approx(ref.loss(), rel=LOSS_RTOL)
+
+
+def test_blocking_and_counts():
+    p = _problem(m=1001, n=997, nnz=20000, kind="zipf")
+    for d in (1, 3, 8):
+        ref, ctx = _pair(p, 8, d)
+        with ctx:
+            np.testing.assert_array_equal(ctx.block_nnz(P.TRAIN), ref.block_nnz(0))
+            np.testing.assert_array_equal(ctx.block_nnz(P.TEST), ref.block_nnz(1))
+            a, b, mx = ctx.nnz12()
+            ra, rb, rmx = ref.nnz12()
+            np.testing.assert_array_equal(a, ra)
+            np.testing.assert_array_equal(b, rb)
+            assert mx == rmx
+
+
+def test_duplicates_are_summed():
+    rows = np.array([5, 0, 5, 3, 0, 5], np.uint32)
+    cols = np.array([1, 7, 1, 2, 0, 1], np.uint32)
+    vals = np.array([1.0, 2.0, 0.5, 3.0, 4.0, 0.25])
+    W0 = np.random.default_rng(0).uniform(-0.5, 0.5, (6, 2))
+    H0 = np.random.default_rng(1).uniform(-0.5, 0.5, (8, 2))
+    ref = O.Problem(6, 8, 2, 2, rows, cols, vals).configure()
+    ref.set_factors(W0, H0)
+    with P.Context(P.Config(m=6, n=8, rank=2, d=2, precision="fp64", exec="replay")) as ctx:
+        ctx.set_matrix(P.TRAIN, rows, cols, vals)
+        ctx.set_factors(W0, H0)
+        np.testing.assert_array_equal(ctx.block_nnz(), ref.block_nnz())
+        assert ctx.nzsl() == pytest.approx(ref.nzsl(), rel=LOSS_RTOL)
+
+
+def test_run_trace_matches_oracle():
+    p = _problem(m=800, n=600, nnz=10000, ntest=1000)
+    ref, ctx = _pair(p, 10, 2)
+    with ctx:
+        ctx.seed(42)
+        ref.seed(42)
+        tr = ctx.run(6, "BoldDriver", 0.01)
+        rt = ref.run(6, "BoldDriver", 0.01)
+        for k, row in enumerate(tr):
+            assert row["loss"] == pytest.approx(rt[k, 0], rel=LOSS_RTOL)
+            assert row["test_loss"] == pytest.approx(rt[k, 1], rel=LOSS_RTOL)
+            if k:
+                assert row["eps"] == rt[k, 2]
+
+
+def test_empty_matrix_and_empty_blocks():
+    p = _problem(m=50, n=40, nnz=30, ntest=0)
+    ref, ctx = _pair(p, 4, 4)  # 4 x 8 blocks, most of them empty
+    with ctx:
+        sched, seeds = P.draw_schedule(P.Random32(1), 4, "COWOR")
+        ctx.epoch_explicit(0.1, sched, seeds)
+        ref.epoch_explicit(0.1, sched, seeds)
+        np.testing.assert_array_equal(ctx.get_factors()[0], ref.get_factors()[0])
+        assert ctx.nzsl(P.TEST) == 0.0
+    with P.Context(P.Config(m=10, n=10, rank=2, d=1, precision="fp32")) as ctx:
+        ctx.set_matrix(P.TRAIN, [], [], [])
+        ctx.set_factors(np.ones((10, 2)), np.ones((10, 2)))
+        ctx.epoch(0.1)
+        assert ctx.nzsl() == 0.0
+        np.testing.assert_array_equal(ctx.get_factors()[0], np.ones((10, 2)))
+
+
+def test_errors_are_reported_not_crashed():
+    with P.Context(P.Config(m=10, n=10, rank=2, d=2)) as ctx:
+        with pytest.raises(P.DsgdppError) as e:
+            ctx.epoch(0.1)
+        assert e.value.status == P.E_STATE
+        with pytest.raises(P.DsgdppError) as e:
+            ctx.set_matrix(P.TRAIN, [1, 10], [0, 0], [1.0, 2.0])
+        assert e.value.status == P.E_INVALID
+        with pytest.raises(P.DsgdppError):
+            ctx.epoch_explicit(0.1, np.full((4, 2), 9, np.uint32), np.zeros(2, np.uint32))
+
+
+def _rmse(ctx, ntest):
+    return float(np.sqrt(ctx.nzsl(P.TEST) / ntest))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.01), ("fp32", 0.01), ("bf16", 0.02)])
+@pytest.mark.parametrize("launch", ["stream", "graph"])
+def test_hogwild_tracks_fp64_oracle(precision, tol, launch):
+    p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
+    d = 4
+    ref, ctx = _pair(p, 10, d, precision=precision, exec="hogwild", launch=launch)
+    with ctx:
+        ctx.seed(9)
+        ref.seed(9)
+        eps = 0.01
+        for _ in range(8):
+            ctx.epoch(eps)
+            ref.epoch(eps)
+        got = _rmse(ctx, len(p.tvals))
+        want = float(np.sqrt(ref.nzsl(1) / len(p.tvals)))
+        start = float(np.sqrt(np.sum((p.tvals - np.einsum("ij,ij->i", p.W0[p.trows],
+                                                          p.H0[p.tcols])) ** 2) / len(p.tvals)))
+        assert want < 0.9 * start  # the run made progress
+        assert abs(got - want) <= tol * want, (got, want)
+
+
+def test_hogwild_lazy_l2_scaling_matches_exact():
+    # with no training entries the epoch is pure RegularizeL2 scaling: W is
+    # scaled 2d times, each H column block d times
+    m, n, r, d = 64, 64, 8, 4
+    rng = np.random.default_rng(0)
+    W0, H0 = rng.uniform(-1, 1, (m, r)), rng.uniform(-1, 1, (n, r))
+    outs = []
+    for prec, ex in (("fp64", "replay"), ("fp32", "hogwild"), ("fp64", "hogwild")):
+        cfg = P.Config(m=m, n=n, rank=r, d=d, precision=prec, exec=ex, update="Nzsl",
+                       regularize="L2", regularize_lambda=0.5, loss="Nzsl")
+        with P.Context(cfg) as ctx:
+            ctx.set_matrix(P.TRAIN, [], [], [])
+            ctx.set_factors(W0, H0)
+            sched, seeds = P.draw_schedule(P.Random32(4), d, "COWOR")
+            ctx.epoch_explicit(0.3, sched, seeds)
+            outs.append(ctx.get_factors())
+    for W, H in outs[1:]:
+        np.testing.assert_allclose(W, outs[0][0], rtol=2e-6)
+        np.testing.assert_allclose(H, outs[0][1], rtol=2e-6)
+
+
+def test_epoch_time_is_reported():
+    p = _problem()
+    _, ctx = _pair(p, 10, 2, precision="fp32", exec="hogwild")
+    with ctx:
+        ctx.epoch(0.01)
+        assert ctx.last_epoch_ms() > 0
