@@ -30,7 +30,6 @@ import re
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -44,6 +43,11 @@ WORKLOADS = {
                s=1.1, d=64, noise=0.2,
                text="2,000,000 x 500,000, 100M entries (+1M test), Zipf(1.1) rows and columns, "
                     "rank 32, Nzsl_L2(1) update, L2(0.05) regularize, BoldDriver(0.001) first step"),
+    # a smaller case of the same shape for profiler captures (a few GB on the device)
+    "c2s": dict(m=400_000, n=100_000, nnz=20_000_000, nnz_test=200_000, rank=32, s=1.1, d=64,
+                noise=0.2,
+                text="400,000 x 100,000, 20M entries (+200k test), Zipf(1.1) rows and columns, "
+                     "rank 32, Nzsl_L2(1) update, L2(0.05) regularize"),
     "c1": dict(m=100_000, n=100_000, nnz=1_000_000, nnz_test=100_000, rank=10, s=None, d=4,
                noise=0.1,
                text="100,000 x 100,000, 1M uniform entries (+100k test), rank 10, "
@@ -62,45 +66,50 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples nvidia-smi clocks and throttle reasons (every 100 ms) while the
+    timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index=0):
         self.index = index
-        self.rows = []
-        self._stop = threading.Event()
-        self._t = None
+        self.proc = None
 
     def start(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
-
-    def _run(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index),
-                                      f"--query-gpu={q}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
 
     def stop(self):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        rows = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            rows = [[x.strip() for x in line.split(",")] for line in out.splitlines() if line.strip()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[0]) for r in rows if r) if v is not None]
+        mx = [v for v in (num(r[1]) for r in rows if len(r) > 1) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4)
+        reasons = sorted({names[k] for r in rows for k in range(4)
                           if len(r) > 3 + k and r[3 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+                "samples": len(rows)}
 
 
 def algorithmic_bytes_per_update(r, precision, update):
@@ -133,7 +142,7 @@ def time_cpu_reference(data, wl, steps, warmup, threads=None):
     rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
     prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals)
     prob.configure(update="Nzsl_L2", update_lambda=1.0,
-                   regularize="L2" if wl is WORKLOADS["c2"] else "None",
+                   regularize="L2" if wl["s"] is not None else "None",
                    regularize_lambda=0.05, loss="Nzsl_L2", loss_lambda=1.0)
     prob.set_factors(data["W0"], data["H0"])
     prob.seed(1)
@@ -245,7 +254,7 @@ def main():
     wl = WORKLOADS[args.workload]
     d = args.d or wl["d"]
     data, gen_s = generate(wl, args.seed + rank)
-    l2 = args.workload == "c2"
+    l2 = args.workload in ("c2", "c2s")
     cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=args.precision,
                    exec="hogwild", launch="graph", update="Nzsl_L2", update_lambda=1.0,
                    regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,

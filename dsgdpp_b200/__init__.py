@@ -113,6 +113,17 @@ SIGNATURES = {
     "dsgdpp_point_orders": (C.c_uint64, [C.c_uint32, C.c_int, _u64p, _u32p, _u32p, _u32p]),
     "dsgdpp_block_offsets": (None, [C.c_uint64, C.c_uint32, _u64p]),
     "dsgdpp_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
+    "dsgdpp_io_error": (C.c_char_p, []),
+    "dsgdpp_free": (None, [_P]),
+    "dsgdpp_read_sparse": (C.c_int, [C.c_char_p, _u64p, _u64p, _u64p, C.POINTER(_u32p),
+                                     C.POINTER(_u32p), C.POINTER(_f64p)]),
+    "dsgdpp_write_mm_coord": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint64, C.c_uint64, _u32p,
+                                        _u32p, _f64p]),
+    "dsgdpp_read_mm_array": (C.c_int, [C.c_char_p, _u64p, _u64p, C.POINTER(_f64p)]),
+    "dsgdpp_write_mm_array": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint64, _f64p]),
+    "dsgdpp_write_blocked": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64,
+                                       C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _u32p,
+                                       _u32p, _f64p]),
 }
 
 
@@ -370,6 +381,67 @@ def block_offsets(size: int, blocks: int) -> np.ndarray:
     out = np.empty(blocks, np.uint64)
     lib.dsgdpp_block_offsets(size, blocks, _ptr(out, C.c_uint64))
     return out
+
+
+class IOError_(DsgdppError):
+    pass
+
+
+def _io(rc, what):
+    if rc != OK:
+        raise IOError_(rc, f"{what}: {lib.dsgdpp_io_error().decode()}")
+
+
+def read_sparse(path: str):
+    """.mmc or .xml-blocked sparse file -> (m, n, rows, cols, vals), 0-based."""
+    m, n, nnz = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    r, c, v = _u32p(), _u32p(), _f64p()
+    _io(lib.dsgdpp_read_sparse(path.encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(r),
+                               C.byref(c), C.byref(v)), "read_sparse")
+    k = nnz.value
+    try:
+        rows = np.ctypeslib.as_array(r, shape=(max(k, 1),))[:k].copy()
+        cols = np.ctypeslib.as_array(c, shape=(max(k, 1),))[:k].copy()
+        vals = np.ctypeslib.as_array(v, shape=(max(k, 1),))[:k].copy()
+    finally:
+        for p in (r, c, v):
+            lib.dsgdpp_free(C.cast(p, _P))
+    return m.value, n.value, rows, cols, vals
+
+
+def write_mm_coord(path: str, m: int, n: int, rows, cols, vals):
+    r, c, v = _u32(rows), _u32(cols), _f64(vals)
+    _io(lib.dsgdpp_write_mm_coord(path.encode(), m, n, len(v), _ptr(r, C.c_uint32),
+                                  _ptr(c, C.c_uint32), _ptr(v, C.c_double)), "write_mm_coord")
+
+
+def read_mm_array(path: str) -> np.ndarray:
+    """.mma -> a size1 x size2 array (the file lists it column by column)."""
+    m, n = C.c_uint64(), C.c_uint64()
+    p = _f64p()
+    _io(lib.dsgdpp_read_mm_array(path.encode(), C.byref(m), C.byref(n), C.byref(p)),
+        "read_mm_array")
+    try:
+        k = m.value * n.value
+        flat = np.ctypeslib.as_array(p, shape=(max(k, 1),))[:k].copy()
+    finally:
+        lib.dsgdpp_free(C.cast(p, _P))
+    return flat.reshape(n.value, m.value).T.copy()
+
+
+def write_mm_array(path: str, a):
+    a = np.asarray(a, np.float64)
+    flat = np.ascontiguousarray(a.T).ravel()
+    _io(lib.dsgdpp_write_mm_array(path.encode(), a.shape[0], a.shape[1], _ptr(flat, C.c_double)),
+        "write_mm_array")
+
+
+def write_blocked(xml_path: str, directory: str, base: str, m: int, n: int, blocks1: int,
+                  blocks2: int, rows, cols, vals):
+    r, c, v = _u32(rows), _u32(cols), _f64(vals)
+    _io(lib.dsgdpp_write_blocked(xml_path.encode(), directory.encode(), base.encode(), m, n,
+                                 blocks1, blocks2, len(v), _ptr(r, C.c_uint32),
+                                 _ptr(c, C.c_uint32), _ptr(v, C.c_double)), "write_blocked")
 
 
 def philox4x32_10(ctr, key) -> np.ndarray:

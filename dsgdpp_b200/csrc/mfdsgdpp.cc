@@ -1,0 +1,597 @@
+// mfdsgdpp.cc -- drop-in for the reference tool tools/mfdsgdpp.cc on one B200.
+//
+// Same options, defaults, spec strings, messages, log lines, R trace and
+// .mmc/.mma/.xml files as the reference (tools/mfdsgdpp.cc:361-567,
+// tools/parse.h, tools/detail/mfdsgd-args.h).  One MPI rank: the number of
+// tasks d is --tasks-per-rank, and V is blocked d x 2d.  Added options:
+//   --device N                   CUDA device (default 0)
+//   --precision fp64|fp32|bf16   factor storage (default fp32)
+//   --exec hogwild|replay        replay = the reference's sequential point
+//                                order per block, FP64 only (default hogwild)
+//   --launch graph|stream        epoch as one CUDA graph or 2d launches
+// Extension: --regularize L2(l) is accepted (the reference rejects every
+// regularizer other than None, tools/mfdsgdpp.cc:165-258).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <regex>
+#include <string>
+#include <vector>
+
+#include "../../include/dsgdpp.h"
+#include "mmio.h"
+#include "runner.h"
+
+using namespace dsgdpp;
+
+namespace {
+
+struct Args {
+  std::string inputMatrixFile, inputTestMatrixFile, inputRowFacFile, inputColFacFile,
+      outputRowFacFile, outputColFacFile, traceFile, traceVar, sgdOrderString,
+      stratumOrderString, updateString, regularizeString, lossString, decayString,
+      truncateString, balanceString;
+  std::string updateName, regularizeName, lossName, decayName;
+  std::vector<double> updateArgs, regularizeArgs, lossArgs, truncateArgs;
+  std::vector<std::string> decayArgs;
+  unsigned long long epochs = 10, rank = 0;
+  unsigned seed = 0;
+  int tasksPerRank = 1;
+  bool abs = false;
+  double epsilon = NAN, epsDecrease = NAN, epsIncrease = NAN;
+  int sgdOrder = DSGDPP_SGD_WOR, stratumOrder = DSGDPP_STRATUM_COWOR;
+  // added options
+  int device = 0;
+  std::string precision = "fp32", exec = "hogwild", launch = "graph";
+};
+
+const char* kOptions[] = {
+    "help", "input-file", "input-test-file", "input-row-file", "input-col-file",
+    "output-row-file", "output-col-file", "trace", "trace-var", "epochs", "tasks-per-rank",
+    "sgd-order", "stratum-order", "seed", "rank", "update", "regularize", "loss", "abs",
+    "truncate", "decay", "balance", "device", "precision", "exec", "launch"};
+
+void usage() {
+  std::cout << "mfsgdpp [options]\n\nOptions:\n"
+            << "  --help                 produce help message\n"
+            << "  --input-file arg       filename of data matrix\n"
+            << "  --input-test-file arg  filename of test matrix\n"
+            << "  --input-row-file arg   filename of initial row factors\n"
+            << "  --input-col-file arg   filename of initial column factors\n"
+            << "  --output-row-file arg  filename of final row factors\n"
+            << "  --output-col-file arg  filename of final column factors\n"
+            << "  --trace arg            filename of trace [trace.R]\n"
+            << "  --trace-var arg        variable name for trace [traceVar]\n"
+            << "  --epochs arg           number of epochs to run [10]\n"
+            << "  --tasks-per-rank arg   number of concurrent tasks per rank [1]\n"
+            << "  --sgd-order arg        order of SGD steps [WOR] (e.g., \"SEQ\", \"WR\", \"WOR\")\n"
+            << "  --stratum-order arg    order of strata [COWOR] (e.g., \"SEQ\", \"RSEQ\", \"WR\", "
+               "\"WOR\", \"COWOR\")\n"
+            << "  --seed arg             seed for random number generator (system time if not "
+               "set)\n"
+            << "  --rank arg             rank of factorization\n"
+            << "  --update arg           SGD update function (e.g., \"Sl\", \"Nzsl\", \"GklData\")\n"
+            << "  --regularize arg       SGD regularization function (e.g., \"None\", "
+               "\"L2(0.05)\", \"Nzl2(0.05)\")\n"
+            << "  --loss arg             loss function (e.g., \"Nzsl\", \"Nzsl_L2(0.5)\"))\n"
+            << "  --abs                  if present, absolute values are taken after every SGD "
+               "step\n"
+            << "  --truncate arg         if present, truncatation is enabled (e.g., --truncate "
+               "\"(-1000, 1000)\"\n"
+            << "  --decay arg            decay function (constant, bold driver, or auto)\n"
+            << "  --balance arg          Type of balancing (None, L2, Nzl2)\n"
+            << "  --device arg           CUDA device [0]\n"
+            << "  --precision arg        factor storage fp64|fp32|bf16 [fp32]\n"
+            << "  --exec arg             hogwild|replay [hogwild]\n"
+            << "  --launch arg           graph|stream [graph]\n";
+}
+
+// parse::parseArg (tools/parse.h:38-61): "Name(a,b,...)" -> name + doubles
+bool parse_arg(const std::string& arg, std::string& name, std::vector<std::string>& args) {
+  static const std::regex re("^(.*)\\((.*)\\)$");
+  std::smatch what;
+  args.clear();
+  if (!std::regex_match(arg, what, re)) {
+    name = arg;
+    return true;
+  }
+  name = what.str(1);
+  std::string s = what.str(2);
+  size_t a = 0;
+  for (;;) {
+    size_t c = s.find(',', a);
+    args.push_back(s.substr(a, c == std::string::npos ? std::string::npos : c - a));
+    if (c == std::string::npos) break;
+    a = c + 1;
+  }
+  return true;
+}
+
+bool to_double(const std::string& t, double& v) {  // boost::lexical_cast<double>
+  if (t.empty()) return false;
+  char* q = nullptr;
+  v = std::strtod(t.c_str(), &q);
+  return q && *q == 0 && q != t.c_str();
+}
+
+void parse_doubles(const std::string& arg, std::string& name, std::vector<double>& out) {
+  std::vector<std::string> a;
+  parse_arg(arg, name, a);
+  out.clear();
+  for (size_t k = 0; k < a.size(); ++k) {
+    double v;
+    if (!to_double(a[k], v)) {
+      std::cerr << "Invalid argument " << (k + 1) << " in " << arg << std::endl;
+      std::exit(1);
+    }
+    out.push_back(v);
+  }
+}
+
+std::string print_arg(const std::string& name, const std::vector<std::string>& a) {
+  std::string s = name + "(";
+  for (size_t k = 0; k < a.size(); ++k) s += (k ? "," : "") + a[k];
+  return s + ")";
+}
+
+// parse::parseTruncate (tools/parse.h:114-139)
+void parse_truncate(const std::string& arg, Args& args) {
+  std::string name;
+  std::vector<std::string> a;
+  parse_arg(arg, name, a);
+  double lo, hi;
+  if (name.empty() && a.size() == 2 && to_double(a[0], lo) && to_double(a[1], hi)) {
+    args.truncateArgs = {lo, hi};
+    return;
+  }
+  std::cerr << "Error in argument truncate with options " << print_arg(name, a) << std::endl;
+  std::cerr << "Valid options are:" << std::endl << "    (<min>,<max>)" << std::endl;
+  std::exit(1);
+}
+
+// parse::parseDecay (tools/parse.h:141-235)
+void parse_decay(const std::string& arg, Args& args) {
+  std::string name;
+  std::vector<std::string> a;
+  parse_arg(arg, name, a);
+  double e, x, y;
+  if (name == "Const" && a.size() == 1 && to_double(a[0], e)) {
+    args.decayName = "Const";
+    args.epsilon = e;
+    args.decayArgs = a;
+    return;
+  }
+  if (name == "Auto" && a.size() == 3 && to_double(a[0], e)) {
+    args.decayName = "Auto";
+    args.decayArgs = a;
+    return;
+  }
+  if (name == "BoldDriver" && a.size() == 1 && to_double(a[0], e)) {
+    args.decayName = "BoldDriver";
+    args.epsilon = e;
+    args.epsDecrease = NAN;
+    args.epsIncrease = NAN;
+    args.decayArgs = a;
+    return;
+  }
+  if (name == "BoldDriver" && a.size() == 3 && to_double(a[0], e) && to_double(a[1], x) &&
+      to_double(a[2], y)) {
+    args.decayName = "BoldDriver";
+    args.epsilon = e;
+    args.epsDecrease = x;
+    args.epsIncrease = y;
+    args.decayArgs = a;
+    return;
+  }
+  if (name == "Sequential" && (a.size() == 1 || a.size() == 3) && to_double(a[0], e)) {
+    args.decayName = "Sequential";
+    args.decayArgs = a;
+    return;
+  }
+  std::cerr << "Error in argument 'decay': Unknown or invalid loss '" << print_arg(name, a) << "'"
+            << std::endl;
+  std::cerr << "Valid choices are: " << std::endl
+            << "    Const(<epsilon>)" << std::endl
+            << "    Auto(<epsilon>,<tries>,<input-sample-matrix>)" << std::endl
+            << "    BoldDriver(<epsilon>)" << std::endl
+            << "    BoldDriver(<epsilon>,<epsDecrease>,<epsIncrease>)" << std::endl
+            << "    Sequential(<epsilon>)" << std::endl
+            << "    Sequential(<epsilon>,<alpha>,<A>)" << std::endl;
+  std::exit(1);
+}
+
+struct Job {
+  int update, regularize, loss;
+  double update_lambda = 0, regularize_lambda = 0, loss_lambda = 0;
+};
+
+// runArgs (tools/mfdsgdpp.cc:162-359): the valid (update, regularize, loss)
+// combinations and their argument counts.
+bool resolve(const Args& a, Job& job) {
+  auto arity = [&](const std::vector<double>& v, size_t n, const std::string& s) {
+    if (v.size() != n) {
+      std::cout << "Invalid number of arguments in " << s << std::endl;
+      return false;
+    }
+    return true;
+  };
+  if (!a.abs) {
+    const bool reg_none = a.regularizeName == "None";
+    const bool reg_l2 = a.regularizeName == "L2";  // extension
+    if (reg_none || reg_l2) {
+      if (reg_l2 && !arity(a.regularizeArgs, 1, a.regularizeString)) return false;
+      if (reg_none && !arity(a.regularizeArgs, 0, a.regularizeString)) return false;
+      job.regularize = reg_l2 ? DSGDPP_REGULARIZE_L2 : DSGDPP_REGULARIZE_NONE;
+      job.regularize_lambda = reg_l2 ? a.regularizeArgs[0] : 0;
+      if (a.updateName == "Nzsl" && a.lossName == "Nzsl") {
+        if (!arity(a.updateArgs, 0, a.updateString) || !arity(a.lossArgs, 0, a.lossString))
+          return false;
+        job.update = DSGDPP_UPDATE_NZSL;
+        job.loss = DSGDPP_LOSS_NZSL;
+        return true;
+      }
+      if (a.updateName == "Nzsl_L2" && a.lossName == "Nzsl_L2") {
+        if (!arity(a.updateArgs, 1, a.updateString) || !arity(a.lossArgs, 1, a.lossString))
+          return false;
+        job.update = DSGDPP_UPDATE_NZSL_L2;
+        job.update_lambda = a.updateArgs[0];
+        job.loss = DSGDPP_LOSS_NZSL_L2;
+        job.loss_lambda = a.lossArgs[0];
+        return true;
+      }
+      if (a.updateName == "Nzsl_Nzl2" && a.lossName == "Nzsl_Nzl2") {
+        if (!arity(a.updateArgs, 1, a.updateString) || !arity(a.lossArgs, 1, a.lossString))
+          return false;
+        job.update = DSGDPP_UPDATE_NZSL_NZL2;
+        job.update_lambda = a.updateArgs[0];
+        job.loss = DSGDPP_LOSS_NZSL_NZL2;
+        job.loss_lambda = a.lossArgs[0];
+        return true;
+      }
+    }
+  }
+  std::cerr << "Invalid combination of update, regularize, and loss arguments" << std::endl;
+  std::cout << "Valid combinations are:" << std::endl;
+  std::cout << "\tNzsl / None / Nzsl" << std::endl;
+  std::cout << "\tNzsl / L2 / Nzsl_L2" << std::endl;
+  std::cout << "\tNzsl_Nzl2 / None / Nzsl_Nzl2" << std::endl;
+  return false;
+}
+
+std::string blocks_list(uint64_t b1, uint64_t b2) {
+  std::string s;
+  for (uint64_t i = 0; i < b1; ++i)
+    for (uint64_t j = 0; j < b2; ++j) s += "(" + std::to_string(i) + "," + std::to_string(j) + ") ";
+  return s;
+}
+
+int run(Args& args, const Job& job) {
+  const uint32_t d = (uint32_t)args.tasksPerRank;
+  if (args.decayName != "BoldDriver" && args.decayName != "Const") {
+    std::cerr << "not implemented: decay" << std::endl;  // rg::NotImplementedException
+    return 1;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  auto load_sparse = [&](const std::string& f) {
+    BlockedDescriptor desc;
+    if (!ends_with(f, ".xml")) {
+      Log::info("mf", "File '" + f + "' is not blocked; it will be blocked automatically");
+      Log::info("mf", "Constructing blocks " + blocks_list(d, 2 * d) + " of '" + f + "'");
+    }
+    Coo m = read_sparse(f, &desc);
+    if (ends_with(f, ".xml")) {
+      // the descriptor's blocking must be the job's d x 2d default blocking
+      // (checkBlockingDsgdPp, mf/sgd/dsgdpp-factorization.h:21-33)
+      std::vector<uint64_t> o1(d), o2(2 * d);
+      dsgdpp_block_offsets(desc.size1, d, o1.data());
+      dsgdpp_block_offsets(desc.size2, 2 * d, o2.data());
+      if (desc.blocks1 != d || desc.blocks2 != 2 * d || desc.offsets1 != o1 || desc.offsets2 != o2)
+        throw std::invalid_argument("blocking of " + f + " does not match the d x 2d job blocking");
+    }
+    return m;
+  };
+  Coo V = load_sparse(args.inputMatrixFile);
+  Coo T;
+  const bool has_test = !args.inputTestMatrixFile.empty();
+  if (has_test) {
+    T = load_sparse(args.inputTestMatrixFile);
+    Log::info("mf", "Test matrix: " + std::to_string(T.size1) + " x " + std::to_string(T.size2) +
+                        ", " + std::to_string(T.vals.size()) + " nonzeros, " + std::to_string(d) +
+                        " x " + std::to_string(2 * d) + " blocks");
+  }
+  Log::info("mf", "Data matrix: " + std::to_string(V.size1) + " x " + std::to_string(V.size2) +
+                      ", " + std::to_string(V.vals.size()) + " nonzeros, " + std::to_string(d) +
+                      " x " + std::to_string(2 * d) + " blocks");
+  Log::info("mf", "File '" + args.inputRowFacFile + "' is not blocked; it will be blocked automatically");
+  Dense Wf = read_mm_array(args.inputRowFacFile);
+  Log::info("mf", "Row factor matrix: " + std::to_string(Wf.size1) + " x " +
+                      std::to_string(Wf.size2) + ", " + std::to_string(d) + " x 1 blocks");
+  Log::info("mf", "File '" + args.inputColFacFile + "' is not blocked; it will be blocked automatically");
+  Dense Hf = read_mm_array(args.inputColFacFile);
+  Log::info("mf", "Column factor matrix: " + std::to_string(Hf.size1) + " x " +
+                      std::to_string(Hf.size2) + ", 1 x " + std::to_string(2 * d) + " blocks");
+  // conformity (mf/factorization.h:27-33)
+  if (Wf.size1 != V.size1 || Hf.size2 != V.size2 || Wf.size2 != Hf.size1 ||
+      (has_test && (T.size1 != V.size1 || T.size2 != V.size2)))
+    throw std::invalid_argument("factor and data matrices do not conform");
+  if (Wf.size2 != args.rank)
+    Log::info("main", "Warning: --rank differs from the factor files; using " +
+                          std::to_string(Wf.size2));
+  const uint64_t m = V.size1, n = V.size2, r = Wf.size2;
+  // W: m x r column-major in the file -> row-major; H: r x n column-major = n x r rows
+  std::vector<double> W(m * r), H(n * r);
+  for (uint64_t i = 0; i < m; ++i)
+    for (uint64_t z = 0; z < r; ++z) W[i * r + z] = Wf.colmajor[z * m + i];
+  for (uint64_t j = 0; j < n; ++j)
+    for (uint64_t z = 0; z < r; ++z) H[j * r + z] = Hf.colmajor[j * r + z];
+  auto t1 = std::chrono::steady_clock::now();
+  Log::info("main", "Total time for loading matrices: " +
+                        fmt_secs((double)std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count()));
+
+  dsgdpp_config cfg;
+  dsgdpp_config_init(&cfg);
+  cfg.m = m;
+  cfg.n = n;
+  cfg.rank = (uint32_t)r;
+  cfg.d = d;
+  cfg.precision = args.precision == "fp64" ? DSGDPP_FP64 : args.precision == "bf16" ? DSGDPP_BF16 : DSGDPP_FP32;
+  cfg.exec = args.exec == "replay" ? DSGDPP_EXEC_REPLAY : DSGDPP_EXEC_HOGWILD;
+  cfg.launch = args.launch == "stream" ? DSGDPP_LAUNCH_STREAM : DSGDPP_LAUNCH_GRAPH;
+  cfg.update = job.update;
+  cfg.update_lambda = job.update_lambda;
+  cfg.regularize = job.regularize;
+  cfg.regularize_lambda = job.regularize_lambda;
+  cfg.loss = job.loss;
+  cfg.loss_lambda = job.loss_lambda;
+  if (!std::isnan(args.truncateArgs[0]) && !std::isnan(args.truncateArgs[1])) {
+    cfg.truncate = 1;
+    cfg.truncate_min = args.truncateArgs[0];
+    cfg.truncate_max = args.truncateArgs[1];
+  }
+  cfg.sgd_order = args.sgdOrder;
+  cfg.stratum_order = args.stratumOrder;
+  cfg.device = args.device;
+  dsgdpp_ctx* ctx = nullptr;
+  int rc = dsgdpp_create(&cfg, &ctx);
+  if (rc != DSGDPP_OK) throw CallError(rc, std::string("dsgdpp_create: ") + dsgdpp_create_error());
+  struct Guard {
+    dsgdpp_ctx* c;
+    ~Guard() { dsgdpp_destroy(c); }
+  } guard{ctx};
+  check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TRAIN, V.vals.size(), V.rows.data(), V.cols.data(),
+                               V.vals.data()), "set_matrix");
+  if (has_test)
+    check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TEST, T.vals.size(), T.rows.data(), T.cols.data(),
+                                 T.vals.data()), "set_matrix");
+  check(ctx, dsgdpp_set_factors(ctx, W.data(), H.data()), "set_factors");
+  check(ctx, dsgdpp_seed(ctx, args.seed), "seed");
+
+  Trace trace;  // Args::createTraceFields (tools/detail/mfdsgd-args.h:53-63)
+  trace.add_field("update", args.updateString);
+  trace.add_field("regularize", args.regularizeString);
+  trace.add_field("rank", (double)args.rank);
+  trace.add_field("input_file", args.inputMatrixFile);
+  trace.add_field("sample_matrix", "");
+  trace.add_field("nodes", 1.0);
+  trace.add_field("threads", (double)args.tasksPerRank);
+  trace.add_field("barrier", "false");
+
+  Decay decay;
+  decay.kind = args.decayName == "Const" ? DSGDPP_DECAY_CONST : DSGDPP_DECAY_BOLDDRIVER;
+  decay.eps = args.epsilon;
+  if (!std::isnan(args.epsDecrease) || !std::isnan(args.epsIncrease)) {
+    decay.decrease = args.epsDecrease;
+    decay.increase = args.epsIncrease;
+  }
+  if (has_test) Log::info("main", "Using NzslLoss for test data");
+  Log::info("mf", "Starting DSGD++ on " + std::string(args.exec) + " " + args.precision +
+                      " (B200, one GPU)");
+  static const char* kStrata[] = {"SEQ", "RSEQ", "WR", "WOR", "COWOR"};
+  static const char* kPoints[] = {"SEQ", "WR", "WOR"};
+  Log::info("mf", std::string("Using ") + kStrata[args.stratumOrder] + " order for selecting strata");
+  Log::info("mf", std::string("Using ") + kPoints[args.sgdOrder] +
+                      " order for selecting training points");
+  auto r0 = std::chrono::steady_clock::now();
+  default_runner(ctx, args.epochs, decay, trace, has_test);
+  auto r1 = std::chrono::steady_clock::now();
+  Log::info("mf", "Finished DSGD++");
+  Log::info("main", "Total time: " +
+                        fmt_secs((double)std::chrono::duration_cast<std::chrono::nanoseconds>(r1 - r0).count()));
+
+  if (!args.traceFile.empty()) {
+    Log::info("main", "Writing trace to " + args.traceFile);
+    std::ofstream f(args.traceFile);
+    f << trace.to_r(args.traceVar);
+  }
+  if (!args.outputRowFacFile.empty() || !args.outputColFacFile.empty()) {
+    check(ctx, dsgdpp_get_factors(ctx, W.data(), H.data()), "get_factors");
+  }
+  if (!args.outputRowFacFile.empty()) {
+    Log::info("main", "Writing row factors to " + args.outputRowFacFile);
+    Dense o;
+    o.size1 = m;
+    o.size2 = r;
+    o.colmajor.resize(m * r);
+    for (uint64_t i = 0; i < m; ++i)
+      for (uint64_t z = 0; z < r; ++z) o.colmajor[z * m + i] = W[i * r + z];
+    write_mm_array(args.outputRowFacFile, o);
+  }
+  if (!args.outputColFacFile.empty()) {
+    Log::info("main", "Writing column factors to " + args.outputColFacFile);
+    Dense o;
+    o.size1 = r;
+    o.size2 = n;
+    o.colmajor = H;  // column j of H is contiguous
+    write_mm_array(args.outputColFacFile, o);
+  }
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Args args;
+  std::map<std::string, std::string> vm;
+  std::vector<std::string> positional;
+  const std::vector<std::string> flags(std::begin(kOptions), std::end(kOptions));
+  for (int k = 1; k < argc; ++k) {
+    std::string a = argv[k];
+    if (a.rfind("--", 0) == 0) {
+      std::string key = a.substr(2), val;
+      size_t eq = key.find('=');
+      if (eq != std::string::npos) {
+        val = key.substr(eq + 1);
+        key = key.substr(0, eq);
+      } else if (key != "help" && key != "abs") {
+        if (k + 1 >= argc) {
+          std::cerr << "the required argument for option '--" << key << "' is missing" << std::endl;
+          return 1;
+        }
+        val = argv[++k];
+      }
+      if (std::find(flags.begin(), flags.end(), key) == flags.end()) {
+        std::cerr << "unrecognised option '--" << key << "'" << std::endl;
+        return 1;
+      }
+      vm[key] = val;
+    } else {
+      positional.push_back(a);
+    }
+  }
+  const char* pos_names[] = {"input-file", "input-test-file", "input-row-file", "input-col-file",
+                             "output-row-file", "output-col-file"};
+  for (size_t k = 0; k < positional.size() && k < 6; ++k)
+    if (!vm.count(pos_names[k])) vm[pos_names[k]] = positional[k];
+
+  const char* required[] = {"input-file", "input-row-file", "input-col-file", "update",
+                            "regularize", "loss", "rank", "decay"};
+  bool missing = vm.count("help") > 0;
+  for (auto r : required) missing = missing || !vm.count(r);
+  if (missing) {
+    std::cerr << "Error: Options input-file, input-row-file, input-col-file, update, regularize, "
+                 "loss, rank, and decay have to be present"
+              << std::endl;
+    usage();
+    return 1;
+  }
+  auto get = [&](const char* k, const std::string& dflt) { return vm.count(k) ? vm[k] : dflt; };
+  args.inputMatrixFile = vm["input-file"];
+  args.inputTestMatrixFile = get("input-test-file", "");
+  args.inputRowFacFile = vm["input-row-file"];
+  args.inputColFacFile = vm["input-col-file"];
+  args.outputRowFacFile = get("output-row-file", "");
+  args.outputColFacFile = get("output-col-file", "");
+  args.traceFile = get("trace", "");
+  args.traceVar = get("trace-var", "trace");
+  try {
+    args.seed = vm.count("seed") ? (unsigned)std::stoul(vm["seed"]) : (unsigned)std::time(nullptr);
+    args.epochs = vm.count("epochs") ? std::stoull(vm["epochs"]) : 10;
+    args.tasksPerRank = vm.count("tasks-per-rank") ? std::stoi(vm["tasks-per-rank"]) : 1;
+    args.rank = std::stoull(vm["rank"]);
+    args.device = vm.count("device") ? std::stoi(vm["device"]) : 0;
+  } catch (const std::exception&) {
+    std::cerr << "invalid numeric option value" << std::endl;
+    return 1;
+  }
+  args.sgdOrderString = get("sgd-order", "WOR");
+  args.stratumOrderString = get("stratum-order", "COWOR");
+  args.updateString = vm["update"];
+  args.regularizeString = vm["regularize"];
+  args.lossString = vm["loss"];
+  args.decayString = vm["decay"];
+  args.balanceString = get("balance", "None");
+  args.precision = get("precision", "fp32");
+  args.exec = get("exec", "hogwild");
+  args.launch = get("launch", "graph");
+
+  Log::info("main", "Input");
+  Log::info("main", "    Input file: " + args.inputMatrixFile);
+  Log::info("main", "    Input test file: " +
+                        (args.inputTestMatrixFile.empty() ? std::string("Disabled") : args.inputTestMatrixFile));
+  Log::info("main", "    Input row factors: " + args.inputRowFacFile);
+  Log::info("main", "    Input column factors: " + args.inputColFacFile);
+  Log::info("main", "Output");
+  Log::info("main", "    Output row factors: " +
+                        (args.outputRowFacFile.empty() ? std::string("Disabled") : args.outputRowFacFile));
+  Log::info("main", "    Output column factors: " +
+                        (args.outputColFacFile.empty() ? std::string("Disabled") : args.outputColFacFile));
+  Log::info("main", args.traceFile.empty() ? std::string("    Trace: Disabled")
+                                           : "    Trace: " + args.traceFile + " (" + args.traceVar + ")");
+  Log::info("main", "Parallelization");
+  Log::info("main", "    MPI ranks: 1");
+  Log::info("main", "    Tasks per rank: " + std::to_string(args.tasksPerRank));
+  Log::info("main", "DSGD++ options");
+  Log::info("main", "    Seed: " + std::to_string(args.seed));
+  Log::info("main", "    Epochs: " + std::to_string(args.epochs));
+  Log::info("main", "    Factorization rank: " + std::to_string(args.rank));
+  Log::info("main", "    Update function: " + args.updateString);
+  Log::info("main", "    Regularize function: " + args.regularizeString);
+  Log::info("main", "    Loss function: " + args.lossString);
+  Log::info("main", "    Decay: " + args.decayString);
+
+  if (args.balanceString == "None") {
+    Log::info("main", "    Balancing: Disabled");
+  } else if (args.balanceString == "L2" || args.balanceString == "NZL2") {
+    std::cerr << "Balancing " << args.balanceString << " is not supported on the GPU path" << std::endl;
+    return 1;
+  } else {
+    std::cerr << "Invalid arguments for balance; expected \"None\", \"L2\" or \"Nzl2\"" << std::endl;
+    return 1;
+  }
+  args.abs = vm.count("abs") > 0;
+  Log::info("main", args.abs ? "    Absolute function: Enabled" : "    Absolute function: Disabled");
+  if (!vm.count("truncate")) {
+    args.truncateArgs = {NAN, NAN};
+    Log::info("main", "    Truncation: Disabled");
+  } else {
+    parse_truncate(vm["truncate"], args);
+    Log::info("main", "    Truncation: (" + fmt_g(args.truncateArgs[0]) + "," +
+                          fmt_g(args.truncateArgs[1]) + ")");
+  }
+  if (args.sgdOrderString == "SEQ") args.sgdOrder = DSGDPP_SGD_SEQ;
+  else if (args.sgdOrderString == "WR") args.sgdOrder = DSGDPP_SGD_WR;
+  else if (args.sgdOrderString == "WOR") args.sgdOrder = DSGDPP_SGD_WOR;
+  else {
+    std::cerr << "Invalid arguments for sgdOrder; expected \"SEQ\", \"WR\" or \"WOR\"" << std::endl;
+    return 1;
+  }
+  Log::info("main", "    SGD step sequence: " + args.sgdOrderString);
+  const char* strata[] = {"SEQ", "RSEQ", "WR", "WOR", "COWOR"};
+  int so = -1;
+  for (int k = 0; k < 5; ++k)
+    if (args.stratumOrderString == strata[k]) so = k;
+  if (so < 0) {
+    std::cerr << "Invalid arguments for stratumOrder; expected \"SEQ\", \"RSEQ\", \"WR\", \"WOR\" "
+                 "or \"COWOR\""
+              << std::endl;
+    return 1;
+  }
+  args.stratumOrder = so;
+  Log::info("main", "    DSGD stratum sequence: " + args.stratumOrderString);
+
+  parse_doubles(args.updateString, args.updateName, args.updateArgs);
+  parse_doubles(args.regularizeString, args.regularizeName, args.regularizeArgs);
+  parse_doubles(args.lossString, args.lossName, args.lossArgs);
+  parse_decay(args.decayString, args);
+
+  Job job{};
+  if (!resolve(args, job)) return 1;
+  if (args.tasksPerRank < 1) {
+    std::cerr << "tasks-per-rank must be positive" << std::endl;
+    return 1;
+  }
+  try {
+    return run(args, job);
+  } catch (const MmError& e) {
+    std::cerr << "I/O error: " << e.what() << std::endl;
+  } catch (const CallError& e) {
+    std::cerr << "error: " << e.what() << std::endl;
+  } catch (const std::exception& e) {
+    std::cerr << "error: " << e.what() << std::endl;
+  }
+  return 1;
+}

@@ -202,6 +202,25 @@ uint64_t dsgdpp_point_orders(uint32_t d, int sgd_order, const uint64_t* block_nn
                              uint32_t* out);
 /* computeDefaultBlockOffsets (mf/matrix/distributed_matrix_impl.cc:24-40) */
 void dsgdpp_block_offsets(uint64_t size, uint32_t blocks, uint64_t* out);
+/* ---- file I/O (replaces mf/matrix/io: read_impl.h:45-256, write_impl.h:42-118,
+ * descriptor_impl.cc:25-75); failures return DSGDPP_E_IO, message in
+ * dsgdpp_io_error().  Arrays returned through pointers are malloc'ed; release
+ * them with dsgdpp_free. */
+const char* dsgdpp_io_error(void);
+void dsgdpp_free(void* p);
+/* .mmc, or an .xml descriptor of .mmc blocks: global 0-based coordinates */
+int dsgdpp_read_sparse(const char* path, uint64_t* m, uint64_t* n, uint64_t* nnz,
+                       uint32_t** rows, uint32_t** cols, double** vals);
+int dsgdpp_write_mm_coord(const char* path, uint64_t m, uint64_t n, uint64_t nnz,
+                          const uint32_t* rows, const uint32_t* cols, const double* vals);
+/* .mma: entries column by column */
+int dsgdpp_read_mm_array(const char* path, uint64_t* m, uint64_t* n, double** colmajor);
+int dsgdpp_write_mm_array(const char* path, uint64_t m, uint64_t n, const double* colmajor);
+/* the blocked form written by tools/mfdblock.cc: per-block .mmc files with
+ * block-local coordinates named <base>-<b1>-<b2>.mmc in dir, plus the .xml */
+int dsgdpp_write_blocked(const char* xml_path, const char* dir, const char* base, uint64_t m,
+                         uint64_t n, uint32_t blocks1, uint32_t blocks2, uint64_t nnz,
+                         const uint32_t* rows, const uint32_t* cols, const double* vals);
 /* Philox4x32-10 of the BF16 stochastic rounding, for known-answer checks */
 void dsgdpp_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

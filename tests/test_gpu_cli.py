@@ -1,0 +1,61 @@
+"""The mfdsgdpp drop-in tool end to end on the GPU against the oracle."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import dsgdpp_b200 as P
+from dsgdpp_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "dsgdpp_b200", "bin", "mfdsgdpp")
+
+
+def _write(tmp_path, p):
+    P.write_mm_coord(str(tmp_path / "train.mmc"), p.m, p.n, p.rows, p.cols, p.vals)
+    P.write_mm_coord(str(tmp_path / "test.mmc"), p.m, p.n, p.trows, p.tcols, p.tvals)
+    P.write_mm_array(str(tmp_path / "W.mma"), p.W0)
+    P.write_mm_array(str(tmp_path / "H.mma"), p.H0.T)
+
+
+@pytest.mark.parametrize("blocked", [False, True])
+def test_cli_replay_matches_oracle(tmp_path, blocked):
+    p = synth.make(400, 300, 6000, 600, rank_true=4, r=5, noise=0.1, seed=4)
+    _write(tmp_path, p)
+    d = 3
+    train = str(tmp_path / "train.mmc")
+    if blocked:
+        train = str(tmp_path / "V.xml")
+        P.write_blocked(train, str(tmp_path), "V", p.m, p.n, d, 2 * d, p.rows, p.cols, p.vals)
+    r = subprocess.run([CLI, f"--input-file={train}", f"--input-test-file={tmp_path}/test.mmc",
+                        f"--input-row-file={tmp_path}/W.mma", f"--input-col-file={tmp_path}/H.mma",
+                        "--rank=5", f"--tasks-per-rank={d}", "--update=Nzsl_L2(1)",
+                        "--regularize=None", "--loss=Nzsl_L2(1)", "--decay=BoldDriver(0.01)",
+                        "--epochs=4", "--seed=1499881717", "--precision=fp64", "--exec=replay",
+                        f"--trace={tmp_path}/trace.R", f"--output-row-file={tmp_path}/Wout.mma",
+                        f"--output-col-file={tmp_path}/Hout.mma"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    # the same job on the oracle; the files hold 16 significant digits
+    W0 = P.read_mm_array(str(tmp_path / "W.mma"))
+    H0 = P.read_mm_array(str(tmp_path / "H.mma")).T
+    _, _, tr, tc, tv = P.read_sparse(str(tmp_path / "train.mmc"))
+    _, _, sr, sc, sv = P.read_sparse(str(tmp_path / "test.mmc"))
+    ref = O.Problem(p.m, p.n, 5, d, tr, tc, tv, sr, sc, sv).configure()
+    ref.set_factors(W0, H0)
+    ref.seed(1499881717)
+    trace = ref.run(4, "BoldDriver", 0.01)
+    W, H = ref.get_factors()
+    np.testing.assert_allclose(P.read_mm_array(str(tmp_path / "Wout.mma")), W, rtol=1e-14, atol=1e-15)
+    np.testing.assert_allclose(P.read_mm_array(str(tmp_path / "Hout.mma")).T, H, rtol=1e-14, atol=1e-15)
+    losses = [float(x) for x in re.findall(r"\| Loss: ([0-9.e+-]+)", r.stdout)]
+    assert len(losses) == 5
+    np.testing.assert_allclose(losses, trace[:, 0], rtol=1e-5)
+    text = open(tmp_path / "trace.R").read()
+    assert text.startswith("trace <- list(trace=list(")
+    assert "eps=NA" in text and 'update = "Nzsl_L2(1)"' in text and "rank = 5" in text
+    assert "Step size: 0.01 " in r.stdout and "Finished epoch 4" in r.stdout

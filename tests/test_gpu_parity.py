@@ -130,6 +130,9 @@ def test_loss_parity_fp32_and_bf16_factors():
     # the FP64 loss of stored low-precision factors equals the oracle's loss of
     # the same factors read back as doubles
     p = _problem(m=2000, n=1500, nnz=40000, r=32)
+    # FP32 / BF16 factor storage keeps the entry values in FP32 (12-byte records)
+    p.vals = p.vals.astype(np.float32).astype(np.float64)
+    p.tvals = p.tvals.astype(np.float32).astype(np.float64)
     for prec in ("fp32", "bf16"):
         ref, ctx = _pair(p, 32, 4, precision=prec, exec="hogwild")
         with ctx:
