@@ -238,6 +238,7 @@ def main():
     ap.add_argument("--vecs", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--write-mode", default="auto", choices=["auto", "store", "atomic"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -259,7 +260,8 @@ def main():
                    exec="hogwild", launch="graph", update="Nzsl_L2", update_lambda=1.0,
                    regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,
                    loss="Nzsl_L2", loss_lambda=1.0, lanes_per_nnz=args.lanes,
-                   vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local)
+                   vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local,
+                   write_mode=args.write_mode)
     host = {k: pinned(np.ascontiguousarray(v)) for k, v in data.items()}
     ctx = P.Context(cfg)
     t0 = time.time()
@@ -342,6 +344,7 @@ def main():
             "config": {"workload": wl["text"], "d": d, "blocks": f"{d} x {2 * d}",
                        "nnz": nnz, "precision": args.precision, "exec": "hogwild",
                        "launch": "graph", "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
+                       "write_mode": args.write_mode,
                        "grid": grid, "parallelism": f"replicas x{world}",
                        "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -39,6 +39,7 @@ STRATUM_ORDER = {"SEQ": 0, "RSEQ": 1, "WR": 2, "WOR": 3, "COWOR": 4}
 PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
 EXEC = {"replay": 0, "hogwild": 1}
 LAUNCH = {"stream": 0, "graph": 1}
+WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
 TRAIN, TEST = 0, 1
 DECAY = {"Const": 0, "BoldDriver": 1}
 
@@ -59,7 +60,7 @@ class _Config(C.Structure):
         ("truncate", C.c_int32), ("truncate_min", C.c_double), ("truncate_max", C.c_double),
         ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
         ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
-        ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64),
+        ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64), ("write_mode", C.c_int32),
     ]
 
 
@@ -181,6 +182,7 @@ class Config:
     vecs_per_lane: int = 0
     ctas_per_sm: int = 0
     layout_seed: int = 0x5EED5EED
+    write_mode: str = "auto"
 
     def to_c(self) -> _Config:
         c = _Config()
@@ -199,6 +201,7 @@ class Config:
         c.device = self.device
         c.lanes_per_nnz, c.vecs_per_lane = self.lanes_per_nnz, self.vecs_per_lane
         c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
+        c.write_mode = WRITE_MODE[self.write_mode]
         return c
 
 

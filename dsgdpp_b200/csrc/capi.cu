@@ -117,6 +117,7 @@ struct dsgdpp_ctx {
   uint32_t loss_grid = 0;
   // Hogwild launch shape
   uint32_t lanes = 0, vecs = 0, grid = 0;
+  int atomic_writes = 0;
   // graph of one Hogwild epoch
   cudaGraphExec_t graph_exec = nullptr;
   // timing / ordering
@@ -193,6 +194,7 @@ void validate_config(const dsgdpp_config* c) {
     throw Error(DSGDPP_E_UNSUPPORTED, "replay mode supports rank <= 256");
   if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
     throw Error(DSGDPP_E_INVALID, "unknown launch form");
+  if (c->write_mode < 0 || c->write_mode > 2) throw Error(DSGDPP_E_INVALID, "unknown write mode");
   if (c->update < 0 || c->update > 2) throw Error(DSGDPP_E_INVALID, "unknown update");
   if (c->regularize < 0 || c->regularize > 1) throw Error(DSGDPP_E_INVALID, "unknown regularize");
   if (c->loss < 0 || c->loss > 2) throw Error(DSGDPP_E_INVALID, "unknown loss");
@@ -265,6 +267,11 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   check_cuda(cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming), "event");
   check_cuda(cudaEventRecord(c->ev_inputs, c->stream), "event");
   if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
+  if (cfg->write_mode == DSGDPP_WRITE_ATOMIC && (cfg->precision == DSGDPP_BF16 || cfg->truncate))
+    throw Error(DSGDPP_E_UNSUPPORTED, "atomic writes need FP32/FP64 factors and no truncation");
+  c->atomic_writes = cfg->write_mode == DSGDPP_WRITE_ATOMIC ||
+                     (cfg->write_mode == DSGDPP_WRITE_AUTO && cfg->precision != DSGDPP_BF16 &&
+                      !cfg->truncate);
 }
 
 void destroy_impl(dsgdpp_ctx* c) {
@@ -517,6 +524,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.segs = c->d_segs; a.counters = c->d_counters; a.params = c->d_params;
   a.d = d; a.r = c->r; a.rp = c->rp;
   a.update = c->cfg.update; a.truncate = c->cfg.truncate; a.sgd_order = c->cfg.sgd_order;
+  a.atomic = c->atomic_writes;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
   for (uint32_t s = 0; s < d2; ++s) {

@@ -36,6 +36,7 @@ struct HogwildArgs {
   const EpochParams* params;
   uint32_t d, r, rp;
   int update, truncate, sgd_order;
+  int atomic;            // 1: add the update with vector atomics (FP32/FP64 only)
   double lambda, tmin, tmax;
 };
 

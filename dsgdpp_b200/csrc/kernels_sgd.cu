@@ -187,6 +187,29 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
               nh[e] = clampw(nh[e], tmin, tmax, eps);
             }
         }
+        if constexpr (!kSR) {
+          if (a.atomic) {
+            // classical Hogwild: add the update to the current row/column so
+            // concurrent updates of the same row are not lost
+            C dw[VW], dh[VW];
+#pragma unroll
+            for (int e = 0; e < VW; ++e) {
+              dw[e] = nw[e] - wf[v][e];
+              dh[e] = nh[e] - hf[v][e];
+            }
+            if constexpr (sizeof(T) == 4) {
+              atomicAdd(reinterpret_cast<float4*>(wp + e0), make_float4(dw[0], dw[1], dw[2], dw[3]));
+              atomicAdd(reinterpret_cast<float4*>(hp + e0), make_float4(dh[0], dh[1], dh[2], dh[3]));
+            } else {
+#pragma unroll
+              for (int e = 0; e < VW; ++e) {
+                atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)dw[e]);
+                atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)dh[e]);
+              }
+            }
+            continue;
+          }
+        }
         Philox4 rw4, rh4;
         if (kSR) {
           const uint64_t rec = rb + ri;

@@ -69,6 +69,10 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 /* launch form of an epoch */
 #define DSGDPP_LAUNCH_STREAM 0 /* 2d kernel launches per epoch */
 #define DSGDPP_LAUNCH_GRAPH 1  /* the epoch captured once as a CUDA graph and replayed */
+/* how a Hogwild update is written back */
+#define DSGDPP_WRITE_AUTO 0   /* ATOMIC for FP32/FP64 without truncation, else STORE */
+#define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */
+#define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically (no update is lost) */
 /* matrices */
 #define DSGDPP_TRAIN 0
 #define DSGDPP_TEST 1
@@ -98,6 +102,7 @@ typedef struct dsgdpp_config {
   uint32_t vecs_per_lane; /* Hogwild 16-byte vectors per lane: 0 = auto */
   uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
+  int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
 } dsgdpp_config;
 
 /* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */

@@ -219,12 +219,19 @@ def _rmse(ctx, ntest):
     return float(np.sqrt(ctx.nzsl(P.TEST) / ntest))
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 0.01), ("fp32", 0.01), ("bf16", 0.02)])
+# Test RMSE after 8 constant-step epochs against the sequential FP64 oracle.
+# Atomic writes lose no concurrent update and track the oracle to 0.5%; plain
+# stores lose some updates of rows updated at the same time (3%); BF16 adds
+# stochastic rounding of every factor write (7%).
+@pytest.mark.parametrize("precision,write_mode,tol", [
+    ("fp64", "atomic", 0.005), ("fp32", "atomic", 0.005), ("fp64", "store", 0.03),
+    ("fp32", "store", 0.03), ("bf16", "store", 0.07)])
 @pytest.mark.parametrize("launch", ["stream", "graph"])
-def test_hogwild_tracks_fp64_oracle(precision, tol, launch):
+def test_hogwild_tracks_fp64_oracle(precision, write_mode, tol, launch):
     p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
     d = 4
-    ref, ctx = _pair(p, 10, d, precision=precision, exec="hogwild", launch=launch)
+    ref, ctx = _pair(p, 10, d, precision=precision, exec="hogwild", launch=launch,
+                     write_mode=write_mode)
     with ctx:
         ctx.seed(9)
         ref.seed(9)
