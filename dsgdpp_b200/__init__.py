@@ -102,6 +102,8 @@ SIGNATURES = {
     "dsgdpp_nzsl": (C.c_int, [_P, C.c_int, _f64p]),
     "dsgdpp_l2": (C.c_int, [_P, _f64p, _f64p]),
     "dsgdpp_nzl2": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_nzsl_fp32_noalloc": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, _P, _P]),
     "dsgdpp_run": (C.c_int, [_P, C.c_uint32, C.c_int, C.c_double, C.c_double, C.c_double,
                              C.POINTER(_TraceRow)]),
     "dsgdpp_sync": (C.c_int, [_P]),

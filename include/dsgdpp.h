@@ -177,6 +177,29 @@ int dsgdpp_l2(dsgdpp_ctx* ctx, double* w2, double* h2);
 /* replaces: nzl2 over W and over H (mf/loss/nzl2.h:246-289) */
 int dsgdpp_nzl2(dsgdpp_ctx* ctx, double* w, double* h);
 
+/* Capacity of the fixed scratch of dsgdpp_nzsl_fp32_noalloc, in partial sums
+ * (4096 doubles = 32 KiB of device memory per GPU that loads this library). */
+#define DSGDPP_NOALLOC_MAX_PARTIALS 4096
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running inside another framework's memory pool, or under an
+ * allocator it does not own -- this computes the same sum of squared errors
+ * as dsgdpp_nzsl, sum over k < nnz of (vals[k] - W[rows[k]] . H[cols[k]])^2
+ * accumulated in FP64, from caller-owned device buffers: FP32 values, W and H
+ * as FP32 rows of `ld` floats (ld a multiple of 4 and >= rank rounded up to
+ * 4; W and H 16-byte aligned; only the first `rank` entries of a row count).
+ * The result is written to the device double *out, ordered on `stream` (a
+ * cudaStream_t; NULL is the default stream).  The call allocates and frees
+ * nothing: its scratch is a fixed device array of DSGDPP_NOALLOC_MAX_PARTIALS
+ * doubles, one per CTA; `partials` sets the CTA count (0 = 4 per SM) and a
+ * count above the capacity returns DSGDPP_E_INVALID with a message on stderr.
+ * The first call on a device looks up the scratch address (device set-up);
+ * make that first call before any stream capture.  All calls on a device share
+ * the scratch, which keeps the last call's contents; calls that overlap on the
+ * GPU race on it. */
+int dsgdpp_nzsl_fp32_noalloc(const uint32_t* rows, const uint32_t* cols, const float* vals,
+                             uint64_t nnz, const float* W, const float* H, uint32_t rank,
+                             uint32_t ld, uint32_t partials, double* out, void* stream);
+
 /* ---- runner --------------------------------------------------------------- */
 /* replaces: DsgdPpRunner::run -> detail::defaultRunner (mf/sgd/sgd_impl.h:34-145):
  * loss and test loss, then per epoch: decay, epoch, loss, test loss.  trace
