@@ -30,6 +30,7 @@ import re
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -66,50 +67,62 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons (every 100 ms) while the
-    timed region runs."""
+    """Reads SM clocks, power and clock-event (throttle) reasons through NVML
+    every 10 ms while the timed region runs (read-only queries)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    def __init__(self, cuda_index=0):
+        self.cuda_index = cuda_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+        self._h = None
 
-    def __init__(self, index=0):
-        self.index = index
-        self.proc = None
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.cuda_index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            self._h = self._handle()
+        except Exception:
+            self._h = None
+            return
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        import pynvml
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.rows.append((pynvml.nvmlDeviceGetClockInfo(self._h, pynvml.NVML_CLOCK_SM),
+                                  pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM),
+                                  pynvml.nvmlDeviceGetPowerUsage(self._h) / 1000.0,
+                                  get_reasons(self._h)))
+            except Exception:
+                pass
+            self._stop.wait(0.01)
 
     def stop(self):
-        rows = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=10)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            rows = [[x.strip() for x in line.split(",")] for line in out.splitlines() if line.strip()]
-
-        def num(x):
-            try:
-                return float(x)
-            except ValueError:
-                return None
-        sm = [v for v in (num(r[0]) for r in rows if r) if v is not None]
-        mx = [v for v in (num(r[1]) for r in rows if len(r) > 1) if v is not None]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4)
-                          if len(r) > 3 + k and r[3 + k].lower() == "active"})
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        bits = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+        reasons = sorted({k for r in self.rows for k, b in bits.items() if r[3] & b})
+        sm = [r[0] for r in self.rows]
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                "power_w_max": max(r[2] for r in self.rows) if self.rows else None,
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml"}
 
 
 def algorithmic_bytes_per_update(r, precision, update):
@@ -310,23 +323,31 @@ def main():
     e2e = None
     if not args.no_e2e:
         barrier(pg)
+        W = np.empty((wl["m"], wl["rank"]), np.float64)
+        H = np.empty((wl["n"], wl["rank"]), np.float64)
+        W[:] = 0.0  # fault the result pages in before the timed region
+        H[:] = 0.0
         t0 = time.perf_counter()
         ctx.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
         ctx.set_matrix(P.TEST, host["trows"], host["tcols"], host["tvals"])
         ctx.set_factors(host["W0"], host["H0"])
+        t1 = time.perf_counter()
         losses = []
         for _ in range(args.steps):
             ctx.epoch(eps)
             losses.append((ctx.loss(), ctx.nzsl(P.TEST)))
-        W, H = ctx.get_factors()
+        t2 = time.perf_counter()
+        ctx.get_factors_into(W, H)
         t_e2e = time.perf_counter() - t0
+        parts = {"upload_s": t1 - t0, "steps_s": t2 - t1, "download_s": t_e2e - (t2 - t0)}
         t_e2e = allreduce_max(pg, t_e2e)
         h2d = (16 * (len(host["vals"]) + len(host["tvals"])) + 8 * (wl["m"] + wl["n"]) * wl["rank"]
                + args.steps * (2 * d * d * 4 + 24))
         d2h = 8 * (wl["m"] + wl["n"]) * wl["rank"] + args.steps * 16
         e2e = {"value": nnz * args.steps * world / t_e2e, "unit": "updates/s",
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
-               "seconds": t_e2e, "final_test_rmse": float(np.sqrt(losses[-1][1] / len(host["tvals"])))}
+               "seconds": t_e2e, **parts,
+               "final_test_rmse": float(np.sqrt(losses[-1][1] / len(host["tvals"])))}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

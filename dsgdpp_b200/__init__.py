@@ -40,6 +40,7 @@ PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
 EXEC = {"replay": 0, "hogwild": 1}
 LAUNCH = {"stream": 0, "graph": 1}
 WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
+PIPELINE = {"auto": 0, "off": 1, "on": 2}
 TRAIN, TEST = 0, 1
 DECAY = {"Const": 0, "BoldDriver": 1}
 
@@ -61,6 +62,7 @@ class _Config(C.Structure):
         ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
         ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
         ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64), ("write_mode", C.c_int32),
+        ("pipeline", C.c_int32),
     ]
 
 
@@ -76,6 +78,7 @@ _P = C.c_void_p
 _u32p = C.POINTER(C.c_uint32)
 _u64p = C.POINTER(C.c_uint64)
 _f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
 
 # every symbol of include/dsgdpp.h with its ctypes signature
 SIGNATURES = {
@@ -107,6 +110,21 @@ SIGNATURES = {
     "dsgdpp_run": (C.c_int, [_P, C.c_uint32, C.c_int, C.c_double, C.c_double, C.c_double,
                              C.POINTER(_TraceRow)]),
     "dsgdpp_sync": (C.c_int, [_P]),
+    "dsgdpp_save_factors": (C.c_int, [_P]),
+    "dsgdpp_restore_factors": (C.c_int, [_P]),
+    "dsgdpp_update_norms": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "dsgdpp_mlp_destroy": (None, [_P]),
+    "dsgdpp_mlp_param_count": (C.c_int, []),
+    "dsgdpp_mlp_get_params": (C.c_int, [_P, _f32p]),
+    "dsgdpp_mlp_set_params": (C.c_int, [_P, _f32p]),
+    "dsgdpp_mlp_forward": (C.c_int, [_P, _f32p, C.c_int, _f32p]),
+    "dsgdpp_mlp_gradient": (C.c_int, [_P, _f32p, _f32p, C.c_int, _f32p, _f32p]),
+    "dsgdpp_mlp_train_step": (C.c_int, [_P, _f32p, _f32p, C.c_int, C.c_float, _f32p]),
+    "dsgdpp_run_controlled": (C.c_int, [_P, _P, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.POINTER(_TraceRow), _u32p, _u32p]),
+    "dsgdpp_controller_features": (None, [_f64p, _f64p, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, _f32p]),
     "dsgdpp_rng_create": (_P, [C.c_uint32]),
     "dsgdpp_rng_destroy": (None, [_P]),
     "dsgdpp_rng_next": (C.c_uint32, [_P]),
@@ -185,6 +203,7 @@ class Config:
     ctas_per_sm: int = 0
     layout_seed: int = 0x5EED5EED
     write_mode: str = "auto"
+    pipeline: str = "auto"
 
     def to_c(self) -> _Config:
         c = _Config()
@@ -204,6 +223,7 @@ class Config:
         c.lanes_per_nnz, c.vecs_per_lane = self.lanes_per_nnz, self.vecs_per_lane
         c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
         c.write_mode = WRITE_MODE[self.write_mode]
+        c.pipeline = PIPELINE[self.pipeline]
         return c
 
 
@@ -259,6 +279,14 @@ class Context:
                     "get_factors")
         return w, h
 
+    def get_factors_into(self, W: np.ndarray, H: np.ndarray):
+        """Reads the factors into caller-provided C-contiguous float64 arrays."""
+        for a, rows in ((W, self.config.m), (H, self.config.n)):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != (rows, self.config.rank):
+                raise ValueError("factor buffers must be C-contiguous float64 of the factor shape")
+        self._check(lib.dsgdpp_get_factors(self._h, _ptr(W, C.c_double), _ptr(H, C.c_double)),
+                    "get_factors")
+
     def block_nnz(self, which: int = TRAIN) -> np.ndarray:
         out = np.empty(2 * self.config.d * self.config.d, np.uint64)
         self._check(lib.dsgdpp_block_nnz(self._h, which, _ptr(out, C.c_uint64)), "block_nnz")
@@ -302,6 +330,29 @@ class Context:
         self._check(lib.dsgdpp_launch_shape(self._h, C.byref(a), C.byref(b), C.byref(g)),
                     "launch_shape")
         return a.value, b.value, g.value
+
+    def run_controlled(self, mlp: "Mlp", epochs: int, eps0: float = 0.001, decrease: float = 0.5,
+                       increase: float = 1.05, target_test_loss: float = 0.0):
+        rows = (_TraceRow * (epochs + 1))()
+        done, fb = C.c_uint32(), C.c_uint32()
+        self._check(lib.dsgdpp_run_controlled(self._h, mlp._h, epochs, eps0, decrease, increase,
+                                              target_test_loss, rows, C.byref(done), C.byref(fb)),
+                    "run_controlled")
+        trace = [dict(epoch=r.epoch, loss=r.loss, test_loss=r.test_loss, eps=r.eps,
+                      time_eps=r.time_eps, time_epoch=r.time_epoch, time_loss=r.time_loss,
+                      time_test_loss=r.time_test_loss) for r in rows[:done.value + 1]]
+        return trace, fb.value
+
+    def save_factors(self):
+        self._check(lib.dsgdpp_save_factors(self._h), "save_factors")
+
+    def restore_factors(self):
+        self._check(lib.dsgdpp_restore_factors(self._h), "restore_factors")
+
+    def update_norms(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(lib.dsgdpp_update_norms(self._h, C.byref(a), C.byref(b)), "update_norms")
+        return a.value, b.value
 
     def sync(self):
         self._check(lib.dsgdpp_sync(self._h), "sync")
@@ -385,6 +436,83 @@ def point_orders(d: int, sgd_order: str, block_nnz, schedule, task_seeds) -> np.
 def block_offsets(size: int, blocks: int) -> np.ndarray:
     out = np.empty(blocks, np.uint64)
     lib.dsgdpp_block_offsets(size, blocks, _ptr(out, C.c_uint64))
+    return out
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Mlp:
+    """The step-size controller network (16 -> 64 -> 64 -> 1, GELU) on the GPU."""
+
+    INPUTS = 16
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        h = _P()
+        rc = lib.dsgdpp_mlp_create(device, seed, C.byref(h))
+        if rc != OK:
+            raise DsgdppError(rc, "dsgdpp_mlp_create")
+        self._h = h
+        self.n_params = lib.dsgdpp_mlp_param_count()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _chk(self, rc, what):
+        if rc != OK:
+            raise DsgdppError(rc, what)
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(self.n_params, np.float32)
+        self._chk(lib.dsgdpp_mlp_get_params(self._h, _ptr(p, C.c_float)), "mlp_get_params")
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p)
+        self._chk(lib.dsgdpp_mlp_set_params(self._h, _ptr(p, C.c_float)), "mlp_set_params")
+
+    def forward(self, x) -> np.ndarray:
+        x = _f32(x).reshape(-1, self.INPUTS)
+        out = np.empty(len(x), np.float32)
+        self._chk(lib.dsgdpp_mlp_forward(self._h, _ptr(x, C.c_float), len(x), _ptr(out, C.c_float)),
+                  "mlp_forward")
+        return out
+
+    def gradient(self, x, y):
+        x = _f32(x).reshape(-1, self.INPUTS)
+        y = _f32(y)
+        g = np.empty(self.n_params, np.float32)
+        loss = C.c_float()
+        self._chk(lib.dsgdpp_mlp_gradient(self._h, _ptr(x, C.c_float), _ptr(y, C.c_float), len(x),
+                                          C.byref(loss), _ptr(g, C.c_float)), "mlp_gradient")
+        return loss.value, g
+
+    def train_step(self, x, y, lr=1e-3) -> float:
+        x = _f32(x).reshape(-1, self.INPUTS)
+        y = _f32(y)
+        loss = C.c_float()
+        self._chk(lib.dsgdpp_mlp_train_step(self._h, _ptr(x, C.c_float), _ptr(y, C.c_float),
+                                            len(x), lr, C.byref(loss)), "mlp_train_step")
+        return loss.value
+
+
+def controller_features(train_hist, test_hist, eps, upd_mean, upd_max, epoch_frac,
+                        last_log_mult) -> np.ndarray:
+    tr = np.full(5, np.nan)
+    te = np.full(5, np.nan)
+    tr[:min(5, len(train_hist))] = list(train_hist)[:5]
+    te[:min(5, len(test_hist))] = list(test_hist)[:5]
+    out = np.empty(16, np.float32)
+    lib.dsgdpp_controller_features(_ptr(tr, C.c_double), _ptr(te, C.c_double), eps, upd_mean,
+                                   upd_max, epoch_frac, last_log_mult, _ptr(out, C.c_float))
     return out
 
 

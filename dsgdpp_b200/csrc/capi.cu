@@ -91,6 +91,8 @@ struct dsgdpp_ctx {
   void* inv1 = nullptr;
   void* inv2 = nullptr;
   double* staging = nullptr;  // (m + n) * r doubles, factor upload / download
+  void* W_saved = nullptr;    // factor snapshot (dsgdpp_save_factors)
+  void* H_saved = nullptr;
   // per-epoch inputs (pinned host copies feed the device copies)
   uint32_t* h_schedule = nullptr;
   uint32_t* d_schedule = nullptr;
@@ -118,6 +120,7 @@ struct dsgdpp_ctx {
   // Hogwild launch shape
   uint32_t lanes = 0, vecs = 0, grid = 0;
   int atomic_writes = 0;
+  int pipeline = 1;
   // graph of one Hogwild epoch
   cudaGraphExec_t graph_exec = nullptr;
   // timing / ordering
@@ -168,7 +171,8 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
   c->vecs = vecs;
   if ((uint64_t)lanes * vecs < nvec)
     throw Error(DSGDPP_E_INVALID, "lanes_per_nnz x vecs_per_lane does not cover the rank");
-  int per_sm = hogwild_ctas_per_sm(c->cfg.precision, lanes, vecs, c->d);
+  int per_sm = hogwild_ctas_per_sm(c->cfg.precision, lanes, vecs, c->atomic_writes != 0,
+                                   c->pipeline != 0, c->d);
   if (per_sm <= 0)
     throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
                                       ", vecs_per_lane=" + std::to_string(vecs));
@@ -195,6 +199,7 @@ void validate_config(const dsgdpp_config* c) {
   if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
     throw Error(DSGDPP_E_INVALID, "unknown launch form");
   if (c->write_mode < 0 || c->write_mode > 2) throw Error(DSGDPP_E_INVALID, "unknown write mode");
+  if (c->pipeline < 0 || c->pipeline > 2) throw Error(DSGDPP_E_INVALID, "unknown pipeline mode");
   if (c->update < 0 || c->update > 2) throw Error(DSGDPP_E_INVALID, "unknown update");
   if (c->regularize < 0 || c->regularize > 1) throw Error(DSGDPP_E_INVALID, "unknown regularize");
   if (c->loss < 0 || c->loss > 2) throw Error(DSGDPP_E_INVALID, "unknown loss");
@@ -259,19 +264,19 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   c->h_mask = halloc<uint8_t>((size_t)d2 * d2, "mask");
   c->d_mask = dalloc<uint8_t>((size_t)d2 * d2, "mask");
   c->loss_grid = (uint32_t)c->num_sms * 4;
-  c->d_partials = dalloc<double>(c->loss_grid, "partials");
+  c->d_partials = dalloc<double>(2 * (size_t)c->loss_grid, "partials");
   c->d_out = dalloc<double>(4, "loss out");
   c->h_out = halloc<double>(4, "loss out");
   check_cuda(cudaEventCreate(&c->ev_begin), "event");
   check_cuda(cudaEventCreate(&c->ev_end), "event");
   check_cuda(cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming), "event");
   check_cuda(cudaEventRecord(c->ev_inputs, c->stream), "event");
-  if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
-  if (cfg->write_mode == DSGDPP_WRITE_ATOMIC && (cfg->precision == DSGDPP_BF16 || cfg->truncate))
-    throw Error(DSGDPP_E_UNSUPPORTED, "atomic writes need FP32/FP64 factors and no truncation");
+  if (cfg->write_mode == DSGDPP_WRITE_ATOMIC && cfg->truncate)
+    throw Error(DSGDPP_E_UNSUPPORTED, "atomic writes cannot truncate");
   c->atomic_writes = cfg->write_mode == DSGDPP_WRITE_ATOMIC ||
-                     (cfg->write_mode == DSGDPP_WRITE_AUTO && cfg->precision != DSGDPP_BF16 &&
-                      !cfg->truncate);
+                     (cfg->write_mode == DSGDPP_WRITE_AUTO && !cfg->truncate);
+  c->pipeline = cfg->pipeline != DSGDPP_PIPELINE_OFF;
+  if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
 }
 
 void destroy_impl(dsgdpp_ctx* c) {
@@ -283,6 +288,7 @@ void destroy_impl(dsgdpp_ctx* c) {
   dfree(c->d_off1); dfree(c->d_off2);
   dfree(c->W); dfree(c->H); dfree(c->cnt1); dfree(c->cnt2); dfree(c->inv1); dfree(c->inv2);
   dfree(c->staging);
+  dfree(c->W_saved); dfree(c->H_saved);
   hfree(c->h_schedule); dfree(c->d_schedule); hfree(c->h_params); dfree(c->d_params);
   hfree(c->h_sigma); dfree(c->d_sigma); hfree(c->h_scales); dfree(c->d_scales);
   dfree(c->d_segs); dfree(c->d_counters);
@@ -525,6 +531,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.d = d; a.r = c->r; a.rp = c->rp;
   a.update = c->cfg.update; a.truncate = c->cfg.truncate; a.sgd_order = c->cfg.sgd_order;
   a.atomic = c->atomic_writes;
+  a.pipe = c->pipeline;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
   for (uint32_t s = 0; s < d2; ++s) {
@@ -1029,6 +1036,56 @@ int dsgdpp_run(dsgdpp_ctx* c, uint32_t epochs, int decay, double eps0, double de
         trace[e + 1] = dsgdpp_trace_row{e + 1u, cur, test, eps, elapsed_ns(a, b), elapsed_ns(b, e1),
                                         elapsed_ns(e1, e2), has_test ? elapsed_ns(e2, e3) : 0.0};
     }
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_save_factors(dsgdpp_ctx* c) {
+  return guarded(c, [&]() {
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    const size_t es = elem_size(c->cfg.precision);
+    if (!c->W_saved) {
+      check_cuda(cudaMalloc(&c->W_saved, c->cfg.m * c->rp * es), "W snapshot");
+      check_cuda(cudaMalloc(&c->H_saved, c->cfg.n * c->rp * es), "H snapshot");
+    }
+    check_cuda(cudaMemcpyAsync(c->W_saved, c->W, c->cfg.m * c->rp * es, cudaMemcpyDeviceToDevice,
+                               c->stream), "save W");
+    check_cuda(cudaMemcpyAsync(c->H_saved, c->H, c->cfg.n * c->rp * es, cudaMemcpyDeviceToDevice,
+                               c->stream), "save H");
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_restore_factors(dsgdpp_ctx* c) {
+  return guarded(c, [&]() {
+    if (!c->W_saved) throw Error(DSGDPP_E_STATE, "no saved factors");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    const size_t es = elem_size(c->cfg.precision);
+    check_cuda(cudaMemcpyAsync(c->W, c->W_saved, c->cfg.m * c->rp * es, cudaMemcpyDeviceToDevice,
+                               c->stream), "restore W");
+    check_cuda(cudaMemcpyAsync(c->H, c->H_saved, c->cfg.n * c->rp * es, cudaMemcpyDeviceToDevice,
+                               c->stream), "restore H");
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_update_norms(dsgdpp_ctx* c, double* mean, double* max) {
+  return guarded(c, [&]() {
+    if (!c->W_saved) throw Error(DSGDPP_E_STATE, "no saved factors");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    double sum = 0, mx = 0;
+    const struct { const void* x; const void* old; uint64_t rows; } parts[2] = {
+        {c->W, c->W_saved, c->cfg.m}, {c->H, c->H_saved, c->cfg.n}};
+    for (const auto& p : parts) {
+      check_cuda(launch_update_norms(c->cfg.precision, p.x, p.old, p.rows, c->rp, c->d_partials,
+                                     c->loss_grid, c->d_out, c->stream), "update norms");
+      check_cuda(cudaMemcpyAsync(c->h_out, c->d_out, 16, cudaMemcpyDeviceToHost, c->stream), "D2H");
+      check_cuda(cudaStreamSynchronize(c->stream), "sync");
+      sum += c->h_out[0];
+      mx = std::max(mx, c->h_out[1]);
+    }
+    if (mean) *mean = sum / (double)(c->cfg.m + c->cfg.n);
+    if (max) *max = mx;
     return DSGDPP_OK;
   });
 }

@@ -1,0 +1,94 @@
+// controller.cc -- the learned step-size controller's epoch loop over the C ABI.
+//
+// defaultRunner (mf/sgd/sgd_impl.h:34-145) with the step chosen by the
+// controller network instead of BoldDriver's multiplier.  Each epoch:
+//   1. the network maps the 16 history features to a log multiplier m in
+//      [-1, 1]; the proposed step is eps * exp(m);
+//   2. the factors are saved on the device and the epoch runs with the
+//      proposed step;
+//   3. if the training loss rose, the proposal is rejected: the factors are
+//      restored and the epoch runs again with BoldDriver's step (eps halved,
+//      decay_bolddriver.h:59-67) -- a fallback event;
+//   4. the run stops early once the test loss reaches the target.
+// No reference counterpart (the reference's BoldDriver never rolls back).
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "../../include/dsgdpp.h"
+
+namespace {
+
+double since(std::chrono::steady_clock::time_point a) {
+  return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now() - a).count();
+}
+
+}  // namespace
+
+extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs,
+                                     double eps0, double decrease, double increase,
+                                     double target_test_loss, dsgdpp_trace_row* trace,
+                                     uint32_t* epochs_done, uint32_t* fallbacks) {
+  if (!ctx || !mlp || epochs == 0) return DSGDPP_E_INVALID;
+  int rc;
+  std::vector<double> tr(5, NAN), te(5, NAN);  // index 0 = newest
+  auto push = [](std::vector<double>& h, double v) {
+    for (int k = 4; k > 0; --k) h[k] = h[k - 1];
+    h[0] = v;
+  };
+  auto t0 = std::chrono::steady_clock::now();
+  double loss = 0, test = NAN;
+  if ((rc = dsgdpp_loss(ctx, &loss)) != DSGDPP_OK) return rc;
+  const double tl = since(t0);
+  auto t1 = std::chrono::steady_clock::now();
+  const bool has_test = dsgdpp_nzsl(ctx, DSGDPP_TEST, &test) == DSGDPP_OK;
+  if (!has_test) test = NAN;
+  if (trace) trace[0] = dsgdpp_trace_row{0, loss, test, NAN, 0, 0, tl, has_test ? since(t1) : 0.0};
+  push(tr, loss);
+  push(te, test);
+  double eps = eps0, upd_mean = 0, upd_max = 0, last_m = 0;
+  uint32_t fb = 0, e = 0;
+  for (; e < epochs; ++e) {
+    auto a = std::chrono::steady_clock::now();
+    float f[16], m = 0;
+    dsgdpp_controller_features(tr.data(), te.data(), eps, upd_mean, upd_max,
+                               (double)e / (double)epochs, last_m, f);
+    if ((rc = dsgdpp_mlp_forward(mlp, f, 1, &m)) != DSGDPP_OK) return rc;
+    const double proposed = eps * std::exp((double)m);
+    const double t_eps = since(a);
+    auto b = std::chrono::steady_clock::now();
+    if ((rc = dsgdpp_save_factors(ctx)) != DSGDPP_OK) return rc;
+    if ((rc = dsgdpp_epoch(ctx, proposed)) != DSGDPP_OK) return rc;
+    double cur = 0;
+    if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
+    double used = proposed;
+    if (!(cur <= tr[0])) {  // the proposed step raised the training loss
+      ++fb;
+      used = eps * decrease;
+      if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
+      if ((rc = dsgdpp_epoch(ctx, used)) != DSGDPP_OK) return rc;
+      if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
+      last_m = std::log(decrease);
+    } else {
+      last_m = m;
+      (void)increase;
+    }
+    if ((rc = dsgdpp_update_norms(ctx, &upd_mean, &upd_max)) != DSGDPP_OK) return rc;
+    const double t_epoch = since(b);
+    eps = used;
+    auto c = std::chrono::steady_clock::now();
+    if (has_test && (rc = dsgdpp_nzsl(ctx, DSGDPP_TEST, &test)) != DSGDPP_OK) return rc;
+    const double t_test = has_test ? since(c) : 0.0;
+    push(tr, cur);
+    push(te, test);
+    if (trace) trace[e + 1] = dsgdpp_trace_row{e + 1u, cur, test, used, t_eps, t_epoch, 0.0, t_test};
+    if (target_test_loss > 0 && has_test && test <= target_test_loss) {
+      ++e;
+      break;
+    }
+  }
+  if (epochs_done) *epochs_done = e;
+  if (fallbacks) *fallbacks = fb;
+  return DSGDPP_OK;
+}

@@ -36,7 +36,8 @@ struct HogwildArgs {
   const EpochParams* params;
   uint32_t d, r, rp;
   int update, truncate, sgd_order;
-  int atomic;            // 1: add the update with vector atomics (FP32/FP64 only)
+  int atomic;            // 1: write the update atomically (vector atomic add; CAS for BF16)
+  int pipe;              // 1: prefetch the next chunk's entries and the next step's vectors
   double lambda, tmin, tmax;
 };
 
@@ -75,7 +76,8 @@ cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs
                                     const HogwildArgs& a, uint32_t s, uint32_t grid,
                                     cudaStream_t st);
 // CTAs per SM that the Hogwild kernel sustains for this configuration
-int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d);
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe,
+                        uint32_t d);
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
 // RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
@@ -101,6 +103,21 @@ cudaError_t launch_nzl2_partials(int precision, const void* X, uint64_t rows, ui
                                  cudaStream_t st);
 cudaError_t launch_sum_partials(const double* partials, uint32_t count, double* out,
                                 cudaStream_t st);
+
+// Sum (out2[0]) and maximum (out2[1]) over rows of |X_i - Xold_i|; partials
+// holds 2 * grid doubles.
+cudaError_t launch_update_norms(int precision, const void* X, const void* Xold, uint64_t rows,
+                                uint32_t rp, double* partials, uint32_t grid, double* out2,
+                                cudaStream_t st);
+
+// ---- step-size controller network (16 -> 64 -> 64 -> 1, GELU) -----------------------
+int mlp_param_count();
+int mlp_input_count();
+cudaError_t launch_mlp(const float* P, const float* X, const float* Y, int batch, float* out,
+                       float* grads, float* losses, cudaStream_t st);
+cudaError_t launch_mlp_reduce(const float* grads, int batch, float* grad, cudaStream_t st);
+cudaError_t launch_adam(float* P, const float* g, float* m, float* v, float lr, float b1,
+                        float b2, float eps, int step, cudaStream_t st);
 
 // ---- data preparation -----------------------------------------------------------
 struct BlockingGeom {

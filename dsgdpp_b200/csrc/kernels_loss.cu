@@ -165,3 +165,81 @@ cudaError_t launch_sum_partials(const double* partials, uint32_t count, double* 
 }
 
 }  // namespace dsgdpp
+
+// ---- factor-update norms (controller features) -------------------------------------
+namespace dsgdpp {
+namespace {
+
+// Per row: the Euclidean norm of (X - Xold) over the rp entries; per CTA the sum
+// and the maximum of those norms go to partials[blockIdx.x] and
+// partials[gridDim.x + blockIdx.x].
+template <typename T>
+__global__ void __launch_bounds__(256) update_norm_partials_kernel(const T* X, const T* Xold,
+                                                                   uint64_t rows, uint32_t rp,
+                                                                   double* partials) {
+  __shared__ double sh[32];
+  __shared__ double shm[32];
+  double sum = 0, mx = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < rows; i += stride) {
+    double s = 0;
+    for (uint32_t z = 0; z < rp; ++z) {
+      const double dlt = as_double(X[i * rp + z]) - as_double(Xold[i * rp + z]);
+      s += dlt * dlt;
+    }
+    const double nrm = sqrt(s);
+    sum += nrm;
+    mx = fmax(mx, nrm);
+  }
+  const double t = block_reduce(sum, sh);
+  // block max
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(kFullMask, mx, off));
+  if ((threadIdx.x & 31) == 0) shm[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m2 = 0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) m2 = fmax(m2, shm[w]);
+    partials[blockIdx.x] = t;
+    partials[gridDim.x + blockIdx.x] = m2;
+  }
+}
+
+__global__ void max_partials_kernel(const double* partials, uint32_t count, double* out) {
+  __shared__ double sh[32];
+  double mx = 0;
+  for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) mx = fmax(mx, partials[k]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(kFullMask, mx, off));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m2 = 0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) m2 = fmax(m2, sh[w]);
+    out[0] = m2;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_update_norms(int precision, const void* X, const void* Xold, uint64_t rows,
+                                uint32_t rp, double* partials, uint32_t grid, double* out2,
+                                cudaStream_t st) {
+  if (precision == kFp64)
+    update_norm_partials_kernel<double><<<grid, 256, 0, st>>>((const double*)X, (const double*)Xold,
+                                                              rows, rp, partials);
+  else if (precision == kFp32)
+    update_norm_partials_kernel<float><<<grid, 256, 0, st>>>((const float*)X, (const float*)Xold,
+                                                             rows, rp, partials);
+  else
+    update_norm_partials_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+        (const __nv_bfloat16*)X, (const __nv_bfloat16*)Xold, rows, rp, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = launch_sum_partials(partials, grid, out2, st);
+  if (e != cudaSuccess) return e;
+  max_partials_kernel<<<1, 1024, 0, st>>>(partials + grid, grid, out2 + 1);
+  return cudaGetLastError();
+}
+
+}  // namespace dsgdpp

@@ -57,14 +57,226 @@ __device__ __forceinline__ void store_vec<__nv_bfloat16>(__nv_bfloat16* p, const
   *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-template <typename T, int LPN, int VPL>
-__global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t s) {
+// Entries of one chunk, one per lane.
+template <typename C>
+struct ChunkRegs {
+  uint64_t rb;    // first entry of the chunk
+  uint32_t nrec;  // entries in the chunk (<= 32)
+  uint32_t seg;   // segment (block) of the chunk
+  uint32_t row, col;
+  C x, ca, cb;    // value, and f2/nnz1, f2/nnz2 (Nzsl_L2) or f2 (Nzsl_Nzl2) of this lane's entry
+};
+
+// W row and H column vectors of one step (32/LPN entries of a chunk).
+template <int VPL>
+struct StepRegs {
+  uint4 w[VPL], h[VPL];
+  uint32_t row, col;
+};
+
+template <typename T, int LPN, int VPL, bool ATOMIC>
+struct Hogwild {
   using E = Elem<T>;
   using C = typename E::C;
-  constexpr int VW = E::VW;
-  constexpr int NG = 32 / LPN;
-  constexpr bool kSR = sizeof(T) == 2;
+  static constexpr int VW = E::VW;
+  static constexpr int NG = 32 / LPN;  // entries updated at once by a warp
+  static constexpr bool kSR = sizeof(T) == 2;
 
+  const HogwildArgs& a;
+  const Segment* seg;
+  const uint32_t d, total, lane, grp, gl, nwarps;
+  const EpochParams ep;
+  const C eps, f2, tmin, tmax;
+  const uint64_t mulA, addB, hkey;
+  T* const W;
+  T* const H;
+
+  __device__ uint32_t permute(uint32_t lc) const {
+    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
+      return (uint32_t)(mix64(hkey ^ ((uint64_t)lc << 20)) % total);
+    return (uint32_t)((mulA * lc + addB) % total);  // WOR: affine permutation; SEQ: identity
+  }
+
+  __device__ void load_chunk(uint32_t lc, ChunkRegs<C>& c) const {
+    const uint32_t pc = permute(lc);
+    uint32_t lo = 0, hi = d - 1;  // the last segment with chunk_begin <= pc
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (seg[mid].chunk_begin <= pc) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t cin = pc - seg[lo].chunk_begin;
+    c.seg = lo;
+    c.rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
+    c.nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
+    c.row = 0; c.col = 0; c.x = 0; c.ca = 0; c.cb = 0;
+    if (lane < c.nrec) {
+      c.row = a.row[c.rb + lane];
+      c.col = a.col[c.rb + lane];
+      c.x = reinterpret_cast<const C*>(a.val)[c.rb + lane];
+      if (a.update == kUpdNzslL2) {
+        c.ca = f2 * reinterpret_cast<const C*>(a.inv1)[c.row];
+        c.cb = f2 * reinterpret_cast<const C*>(a.inv2)[c.col];
+      } else if (a.update == kUpdNzslNzl2) {
+        c.ca = f2;
+        c.cb = f2;
+      }
+    }
+  }
+
+  __device__ void load_step(const ChunkRegs<C>& c, uint32_t t, StepRegs<VPL>& st) const {
+    const uint32_t ri = t * NG + grp;
+    st.row = __shfl_sync(kFullMask, c.row, ri & 31u);
+    st.col = __shfl_sync(kFullMask, c.col, ri & 31u);
+    const bool valid = ri < c.nrec;
+    const T* wp = W + (size_t)st.row * a.rp;
+    const T* hp = H + (size_t)st.col * a.rp;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      if (valid && e0 < a.rp) {
+        st.w[v] = *reinterpret_cast<const uint4*>(wp + e0);
+        st.h[v] = *reinterpret_cast<const uint4*>(hp + e0);
+      } else {
+        st.w[v] = make_uint4(0, 0, 0, 0);
+        st.h[v] = make_uint4(0, 0, 0, 0);
+      }
+    }
+  }
+
+  __device__ void apply_step(const ChunkRegs<C>& c, uint32_t t, const StepRegs<VPL>& st) const {
+    const uint32_t ri = t * NG + grp;
+    const C x = __shfl_sync(kFullMask, c.x, ri & 31u);
+    const C ca = __shfl_sync(kFullMask, c.ca, ri & 31u);
+    const C cb = __shfl_sync(kFullMask, c.cb, ri & 31u);
+    const bool valid = ri < c.nrec;
+    C wf[VPL][VW], hf[VPL][VW];
+    C dot = 0;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      E::unpack(st.w[v], wf[v]);
+      E::unpack(st.h[v], hf[v]);
+#pragma unroll
+      for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+    }
+#pragma unroll
+    for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+    const Segment& g = seg[c.seg];
+    const C f1 = (C)-2 * eps * (x - dot * (C)g.cwh);
+    const C fw = f1 * (C)g.rho_w, fh = f1 * (C)g.rho_h;
+    T* wp = W + (size_t)st.row * a.rp;
+    T* hp = H + (size_t)st.col * a.rp;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      if (!valid || e0 >= a.rp) continue;
+      C nw[VW], nh[VW];
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+        nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+      }
+      if (!ATOMIC && a.truncate) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          if (e0 + e < a.r) {
+            nw[e] = clampw(nw[e], tmin, tmax, eps);
+            nh[e] = clampw(nh[e], tmin, tmax, eps);
+          }
+      }
+      if constexpr (ATOMIC && !kSR) {
+        // add the update, so concurrent updates of one row are not lost
+        if constexpr (sizeof(T) == 4) {
+          atomicAdd(reinterpret_cast<float4*>(wp + e0),
+                    make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
+          atomicAdd(reinterpret_cast<float4*>(hp + e0),
+                    make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) {
+            atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
+            atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
+          }
+        }
+      } else if constexpr (ATOMIC && kSR) {
+        add_bf16(c.rb + ri, e0, st.w[v], st.h[v], nw, nh, wp + e0, hp + e0);
+      } else {
+        Philox4 rw4, rh4;
+        if constexpr (kSR) {
+          const uint64_t rec = c.rb + ri;
+          rw4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
+          rh4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
+                              ep.key0, ep.key1);
+        }
+        store_vec<T>(wp + e0, nw, &rw4);
+        store_vec<T>(hp + e0, nh, &rh4);
+      }
+    }
+  }
+
+  // BF16: the new value is rounded stochastically against the value read
+  // (exactly as a store would write it), and the difference between that
+  // rounded value and the value read -- exact in BF16 for updates of a few
+  // ulps -- is added with one 16-byte vector atomic.  Without a concurrent
+  // update the row ends exactly as a store would leave it; with one, neither
+  // update is lost.
+  __device__ void add_bf16(uint64_t rec, uint32_t e0, const uint4& wv, const uint4& hv,
+                           const float (&nw)[8], const float (&nh)[8], T* wq, T* hq) const {
+    const Philox4 rw = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0,
+                                     ep.key1);
+    const Philox4 rh = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch,
+                                     e0 | 0x80000000u, ep.key0, ep.key1);
+    red_bf16_increment(wq, wv, nw, rw);
+    red_bf16_increment(hq, hv, nh, rh);
+  }
+
+  __device__ static void red_bf16_increment(T* q, const uint4& old, const float (&nv)[8],
+                                            const Philox4& rnd) {
+    const uint32_t ow[4] = {old.x, old.y, old.z, old.w};
+    uint32_t inc[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      uint32_t halves = 0;
+#pragma unroll
+      for (int hlf = 0; hlf < 2; ++hlf) {
+        const uint32_t rbits = (ow[k] >> (16 * hlf)) & 0xffffu;
+        const uint32_t tbits = bf16_sr_bits(nv[2 * k + hlf], rnd.v[k] >> (16 * hlf)) & 0xffffu;
+        const float d = __uint_as_float(tbits << 16) - __uint_as_float(rbits << 16);
+        const uint32_t dbits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(d));
+        halves |= dbits << (16 * hlf);
+      }
+      inc[k] = halves;
+    }
+    asm volatile("red.relaxed.gpu.global.add.noftz.v4.bf16x2 [%0], {%1, %2, %3, %4};"
+                 :: "l"(q), "r"(inc[0]), "r"(inc[1]), "r"(inc[2]), "r"(inc[3]) : "memory");
+  }
+
+  // all steps of one chunk; with PIPE the next step's vectors load while the
+  // current step computes
+  template <bool PIPE>
+  __device__ void process_chunk(const ChunkRegs<C>& c) const {
+    const uint32_t nsteps = (c.nrec + NG - 1) / NG;
+    if constexpr (PIPE) {
+      StepRegs<VPL> cur, nxt;
+      load_step(c, 0, cur);
+      for (uint32_t t = 0; t < nsteps; ++t) {
+        if (t + 1 < nsteps) load_step(c, t + 1, nxt);
+        apply_step(c, t, cur);
+        cur = nxt;
+      }
+    } else {
+      for (uint32_t t = 0; t < nsteps; ++t) {
+        StepRegs<VPL> cur;
+        load_step(c, t, cur);
+        apply_step(c, t, cur);
+      }
+    }
+  }
+};
+
+template <typename T, int LPN, int VPL, bool ATOMIC, bool PIPE>
+__global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t s) {
+  using HW = Hogwild<T, LPN, VPL, ATOMIC>;
+  using C = typename HW::C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Segment* seg = reinterpret_cast<Segment*>(smem_raw);
   const uint32_t d = a.d;
@@ -73,153 +285,41 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
   __syncthreads();
   const uint32_t total = seg[d].chunk_begin;
   if (total == 0) return;
-
   const EpochParams ep = *a.params;
-  const C eps = (C)ep.eps;
-  const C f2 = (C)(ep.eps * 2.0 * a.lambda);
-  const C tmin = (C)a.tmin, tmax = (C)a.tmax;
-  const uint64_t h = mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)s << 17) ^ ep.epoch);
+  const uint64_t hkey = mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)s << 17) ^ ep.epoch);
   uint64_t mulA = 1, addB = 0;
-  if (a.sgd_order == 2) {  // WOR: affine permutation of the chunks
-    mulA = kPrimes[h & 7u] % total;
-    addB = (h >> 8) % total;
+  if (a.sgd_order == 2) {
+    mulA = kPrimes[hkey & 7u] % total;
+    addB = (hkey >> 8) % total;
   }
-  const C* inv1 = reinterpret_cast<const C*>(a.inv1);
-  const C* inv2 = reinterpret_cast<const C*>(a.inv2);
-  const C* vals = reinterpret_cast<const C*>(a.val);
-  T* W = reinterpret_cast<T*>(a.W);
-  T* H = reinterpret_cast<T*>(a.H);
-
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t grp = lane / LPN, gl = lane % LPN;
-
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  const HW hw{a, seg, d, total, lane, lane / LPN, lane % LPN, nwarps, ep, (C)ep.eps,
+              (C)(ep.eps * 2.0 * a.lambda), (C)a.tmin, (C)a.tmax, mulA, addB, hkey,
+              reinterpret_cast<T*>(a.W), reinterpret_cast<T*>(a.H)};
+  // chunk ids: the first one per warp is the warp's index; later ones come
+  // from the sub-epoch's work counter (offset by the warp count), fetched one
+  // chunk ahead so the atomic's latency hides behind a chunk of updates
+  uint32_t id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (id >= total) return;
+  uint32_t pending = 0;
+  if (lane == 0) pending = nwarps + atomicAdd(a.counters + s, 1u);
+  ChunkRegs<C> cur;
+  hw.load_chunk(id, cur);
   for (;;) {
-    uint32_t lc = 0;
-    if (lane == 0) lc = atomicAdd(a.counters + s, 1u);
-    lc = __shfl_sync(kFullMask, lc, 0);
-    if (lc >= total) break;
-    uint32_t pc;
-    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
-      pc = (uint32_t)(mix64(h ^ ((uint64_t)lc << 20)) % total);
-    else
-      pc = (uint32_t)((mulA * lc + addB) % total);
-
-    // segment holding chunk pc: the last k with chunk_begin <= pc
-    uint32_t lo = 0, hi = d - 1;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi + 1) >> 1;
-      if (seg[mid].chunk_begin <= pc) lo = mid; else hi = mid - 1;
-    }
-    const uint32_t cin = pc - seg[lo].chunk_begin;
-    const uint64_t rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
-    const uint32_t nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
-    const C cwh = (C)seg[lo].cwh, rw = (C)seg[lo].rho_w, rh = (C)seg[lo].rho_h;
-
-    uint32_t my_row = 0, my_col = 0;
-    C my_x = 0, my_a = 0, my_b = 0;
-    if (lane < nrec) {
-      my_row = a.row[rb + lane];
-      my_col = a.col[rb + lane];
-      my_x = vals[rb + lane];
-      if (a.update == kUpdNzslL2) {
-        my_a = f2 * inv1[my_row];
-        my_b = f2 * inv2[my_col];
-      } else if (a.update == kUpdNzslNzl2) {
-        my_a = f2;
-        my_b = f2;
-      }
-    }
-
-    for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
-      const uint32_t ri = t0 + grp;
-      const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
-      const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
-      const C x = __shfl_sync(kFullMask, my_x, ri);
-      const C ca = __shfl_sync(kFullMask, my_a, ri);
-      const C cb = __shfl_sync(kFullMask, my_b, ri);
-      const bool valid = ri < nrec;
-      T* wp = W + (size_t)row * a.rp;
-      T* hp = H + (size_t)col * a.rp;
-
-      uint4 wv[VPL], hv[VPL];
-      bool live[VPL];
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        live[v] = valid && e0 < a.rp;
-        if (live[v]) {
-          wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
-          hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
-        } else {
-          wv[v] = make_uint4(0, 0, 0, 0);
-          hv[v] = make_uint4(0, 0, 0, 0);
-        }
-      }
-      C dot = 0;
-      C wf[VPL][VW], hf[VPL][VW];
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        E::unpack(wv[v], wf[v]);
-        E::unpack(hv[v], hf[v]);
-#pragma unroll
-        for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
-      }
-#pragma unroll
-      for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
-
-      const C f1 = (C)-2 * eps * (x - dot * cwh);
-      const C fw = f1 * rw, fh = f1 * rh;
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        if (!live[v]) continue;
-        C nw[VW], nh[VW];
-#pragma unroll
-        for (int e = 0; e < VW; ++e) {
-          nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
-          nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
-        }
-        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        if (a.truncate) {
-#pragma unroll
-          for (int e = 0; e < VW; ++e)
-            if (e0 + e < a.r) {
-              nw[e] = clampw(nw[e], tmin, tmax, eps);
-              nh[e] = clampw(nh[e], tmin, tmax, eps);
-            }
-        }
-        if constexpr (!kSR) {
-          if (a.atomic) {
-            // classical Hogwild: add the update to the current row/column so
-            // concurrent updates of the same row are not lost
-            C dw[VW], dh[VW];
-#pragma unroll
-            for (int e = 0; e < VW; ++e) {
-              dw[e] = nw[e] - wf[v][e];
-              dh[e] = nh[e] - hf[v][e];
-            }
-            if constexpr (sizeof(T) == 4) {
-              atomicAdd(reinterpret_cast<float4*>(wp + e0), make_float4(dw[0], dw[1], dw[2], dw[3]));
-              atomicAdd(reinterpret_cast<float4*>(hp + e0), make_float4(dh[0], dh[1], dh[2], dh[3]));
-            } else {
-#pragma unroll
-              for (int e = 0; e < VW; ++e) {
-                atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)dw[e]);
-                atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)dh[e]);
-              }
-            }
-            continue;
-          }
-        }
-        Philox4 rw4, rh4;
-        if (kSR) {
-          const uint64_t rec = rb + ri;
-          rw4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
-          rh4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
-                              ep.key0, ep.key1);
-        }
-        store_vec<T>(wp + e0, nw, &rw4);
-        store_vec<T>(hp + e0, nh, &rh4);
-      }
+    const uint32_t next = __shfl_sync(kFullMask, pending, 0);
+    const bool more = next < total;
+    if (more && lane == 0) pending = nwarps + atomicAdd(a.counters + s, 1u);
+    if constexpr (PIPE) {
+      ChunkRegs<C> nxt;
+      if (more) hw.load_chunk(next, nxt);  // in flight while cur is updated
+      hw.template process_chunk<true>(cur);
+      if (!more) break;
+      cur = nxt;
+    } else {
+      hw.template process_chunk<false>(cur);
+      if (!more) break;
+      hw.load_chunk(next, cur);
     }
   }
 }
@@ -438,14 +538,18 @@ __global__ void normalize_kernel<double>(double* W, double* H, uint64_t m, uint6
 }
 
 template <typename T, int LPN, int VPL>
-void* hogwild_fn() {
-  return reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL>);
+void* hogwild_fn(bool atomic, bool pipe) {
+  if (atomic)
+    return pipe ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, true>)
+                : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, false>);
+  return pipe ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, true>)
+              : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, false>);
 }
 
 template <typename T>
-void* pick_hogwild(uint32_t lanes, uint32_t vecs) {
+void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool pipe) {
 #define DSGDPP_CASE(L, V) \
-  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>();
+  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>(atomic, pipe);
   DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
   DSGDPP_CASE(2, 2) DSGDPP_CASE(4, 2) DSGDPP_CASE(8, 2) DSGDPP_CASE(16, 2) DSGDPP_CASE(32, 2)
   DSGDPP_CASE(32, 4)
@@ -453,10 +557,10 @@ void* pick_hogwild(uint32_t lanes, uint32_t vecs) {
   return nullptr;
 }
 
-void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs) {
-  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs);
-  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs);
-  return pick_hogwild<__nv_bfloat16>(lanes, vecs);
+void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe) {
+  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs, atomic, pipe);
+  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs, atomic, pipe);
+  return pick_hogwild<__nv_bfloat16>(lanes, vecs, atomic, pipe);
 }
 
 }  // namespace
@@ -469,8 +573,9 @@ cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs);
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe,
+                        uint32_t d) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, pipe);
   if (!fn) return 0;
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * (d + 1)) !=
@@ -482,7 +587,7 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d
 cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs,
                                     const HogwildArgs& a, uint32_t s, uint32_t grid,
                                     cudaStream_t st) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs);
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.pipe != 0);
   if (!fn) return cudaErrorInvalidValue;
   HogwildArgs args = a;
   uint32_t sub = s;

@@ -70,9 +70,14 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 #define DSGDPP_LAUNCH_STREAM 0 /* 2d kernel launches per epoch */
 #define DSGDPP_LAUNCH_GRAPH 1  /* the epoch captured once as a CUDA graph and replayed */
 /* how a Hogwild update is written back */
-#define DSGDPP_WRITE_AUTO 0   /* ATOMIC for FP32/FP64 without truncation, else STORE */
+#define DSGDPP_WRITE_AUTO 0   /* ATOMIC without truncation, else STORE */
 #define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */
-#define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically (no update is lost) */
+#define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically: vector atomic add (FP32/FP64);
+                                 BF16 adds the increment to the stochastically rounded value */
+/* Hogwild prefetching of the next chunk's entries and the next step's vectors */
+#define DSGDPP_PIPELINE_AUTO 0 /* on */
+#define DSGDPP_PIPELINE_OFF 1
+#define DSGDPP_PIPELINE_ON 2
 /* matrices */
 #define DSGDPP_TRAIN 0
 #define DSGDPP_TEST 1
@@ -103,6 +108,7 @@ typedef struct dsgdpp_config {
   uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
   int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
+  int32_t pipeline;       /* Hogwild prefetching: DSGDPP_PIPELINE_* */
 } dsgdpp_config;
 
 /* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */
@@ -208,6 +214,49 @@ int dsgdpp_nzsl_fp32_noalloc(const uint32_t* rows, const uint32_t* cols, const f
 int dsgdpp_run(dsgdpp_ctx* ctx, uint32_t epochs, int decay, double eps0, double decrease,
                double increase, dsgdpp_trace_row* trace);
 int dsgdpp_sync(dsgdpp_ctx* ctx);
+
+/* ---- step-size control ------------------------------------------------------
+ * No reference counterpart (the reference's adaptive rule is BoldDriver with no
+ * rollback, mf/sgd/decay/decay_bolddriver.h:59-67).  Device-side snapshot of
+ * the factors, for rejecting an epoch whose proposed step raised the training
+ * loss, and the per-row update norms |x_i - x_i(snapshot)| over W and H rows
+ * (mean and maximum) used as controller features. */
+int dsgdpp_save_factors(dsgdpp_ctx* ctx);
+int dsgdpp_restore_factors(dsgdpp_ctx* ctx);
+int dsgdpp_update_norms(dsgdpp_ctx* ctx, double* mean, double* max);
+
+/* The controller network: 16 features -> 64 -> 64 -> 1 (GELU), FP32, output a
+ * log step multiplier clipped to [-1, 1].  Inputs and outputs are host arrays
+ * (batch x 16 features row-major); parameters live on the device. */
+typedef struct dsgdpp_mlp dsgdpp_mlp;
+int dsgdpp_mlp_create(int device, uint64_t seed, dsgdpp_mlp** out);
+void dsgdpp_mlp_destroy(dsgdpp_mlp* mlp);
+int dsgdpp_mlp_param_count(void);
+int dsgdpp_mlp_get_params(dsgdpp_mlp* mlp, float* params);
+int dsgdpp_mlp_set_params(dsgdpp_mlp* mlp, const float* params);
+int dsgdpp_mlp_forward(dsgdpp_mlp* mlp, const float* x, int batch, float* out);
+/* mean squared error against y and its gradient w.r.t. the parameters */
+int dsgdpp_mlp_gradient(dsgdpp_mlp* mlp, const float* x, const float* y, int batch, float* loss,
+                        float* grad);
+/* one Adam step (lr, betas 0.9/0.999, eps 1e-8) on the batch; returns the loss */
+int dsgdpp_mlp_train_step(dsgdpp_mlp* mlp, const float* x, const float* y, int batch, float lr,
+                          float* loss);
+/* defaultRunner with the controller choosing each step: the network proposes
+ * eps * exp(m); if that epoch raises the training loss the factors are
+ * restored and the epoch re-runs with BoldDriver's step (eps * decrease), a
+ * fallback event.  Stops after `epochs` or once the test loss is at most
+ * target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
+ * includes the training loss the decision needs). */
+int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs, double eps0,
+                          double decrease, double increase, double target_test_loss,
+                          dsgdpp_trace_row* trace, uint32_t* epochs_done, uint32_t* fallbacks);
+/* The 16 controller features from the run history: train/test losses of the
+ * last 5 evaluations (index 0 = newest; NaN where missing), the current step,
+ * the mean/max factor-update norms of the last epoch, the epoch fraction and
+ * the last applied log multiplier. */
+void dsgdpp_controller_features(const double* train_hist, const double* test_hist, double eps,
+                                double upd_mean, double upd_max, double epoch_frac,
+                                double last_log_mult, float* out16);
 
 /* ---- host utilities (no GPU needed) --------------------------------------- */
 /* rg::Random32 as pinned by this library (MT19937, Boost bucket nextInt). */

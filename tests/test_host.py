@@ -124,3 +124,28 @@ def test_philox_known_answers():
             [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1])]
     for ctr, key, out in kat:
         assert P.philox4x32_10(ctr, key).tolist() == out
+
+
+def test_controller_features_shape_and_values():
+    f = P.controller_features([90.0, 100.0, 110.0, 120.0, 130.0], [9.0, 10.0, 10.0, 11.0, 12.0],
+                              0.001, 0.02, 0.5, 0.25, 0.1)
+    assert f.shape == (16,) and f.dtype == np.float32
+    assert f[0] == pytest.approx(10 * np.log(90 / 100), rel=1e-6)
+    assert f[8] == pytest.approx(-1.0, rel=1e-6)  # log10(0.001) / 3
+    assert f[11] == pytest.approx(0.25) and f[13] == pytest.approx(0.1) and f[15] == 1.0
+    g = P.controller_features([5.0], [], 0.01, 0.0, 0.0, 0.0, 0.0)  # short history
+    assert np.all(g[0:8] == 0) and np.all(np.isfinite(g))
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(0)
+    p = rng.normal(0, 0.2, 5313)
+    X = rng.normal(0, 1, (7, 16))
+    y = rng.uniform(-0.8, 0.8, 7)
+    _, g = M.loss_and_grad(p, X, y)
+    for k in [0, 100, 1024, 1100, 3000, 5200, 5312]:
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        num = (M.loss_and_grad(p + e, X, y)[0] - M.loss_and_grad(p - e, X, y)[0]) / 2e-6
+        assert g[k] == pytest.approx(num, rel=1e-5, abs=1e-9)
