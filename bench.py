@@ -49,6 +49,12 @@ WORKLOADS = {
                 noise=0.2,
                 text="400,000 x 100,000, 20M entries (+200k test), Zipf(1.1) rows and columns, "
                      "rank 32, Nzsl_L2(1) update, L2(0.05) regularize"),
+    # Netflix-shaped stand-in (lognormal rows, Zipf(0.9) columns, ratings 1..5)
+    "c3": dict(m=480_189, n=17_770, nnz=99_000_000, nnz_test=1_400_000, rank=128, s=None, d=64,
+               noise=0.0, kind="ratings",
+               text="480,189 x 17,770, 99M entries (+1.4M test), lognormal(4.2, 1.3) row degrees, "
+                    "Zipf(0.9) columns, integer ratings 1..5 from a rank-16 truth, rank 128, "
+                    "Nzsl_L2(1) update"),
     "c1": dict(m=100_000, n=100_000, nnz=1_000_000, nnz_test=100_000, rank=10, s=None, d=4,
                noise=0.1,
                text="100,000 x 100,000, 1M uniform entries (+100k test), rank 10, "
@@ -175,9 +181,14 @@ def generate(wl, seed):
     import torch
     from dsgdpp_b200 import synth_gpu
     t0 = time.time()
+    dev = f"cuda:{torch.cuda.current_device()}"
+    if wl.get("kind") == "ratings":
+        data = synth_gpu.make_ratings(wl["m"], wl["n"], wl["nnz"], wl["nnz_test"], wl["rank"], seed,
+                                      device=dev)
+        return data, time.time() - t0
     data = synth_gpu.make(wl["m"], wl["n"], wl["nnz"], wl["nnz_test"], rank_true=wl["rank"],
                           r=wl["rank"], noise=wl["noise"], seed=seed, s_row=wl["s"],
-                          s_col=wl["s"], device=f"cuda:{torch.cuda.current_device()}")
+                          s_col=wl["s"], device=dev)
     return data, time.time() - t0
 
 
@@ -252,6 +263,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--write-mode", default="auto", choices=["auto", "store", "atomic"])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use --d (default 64) instead of tuning d in 64..512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -276,6 +289,14 @@ def main():
                    vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local,
                    write_mode=args.write_mode)
     host = {k: pinned(np.ascontiguousarray(v)) for k, v in data.items()}
+    tune = None
+    if not args.no_autotune and not args.d and args.workload in ("c2", "c2s"):
+        t0 = time.time()
+        cfg, tune_ms = P.autotune(cfg, host["rows"], host["cols"], host["vals"], host["W0"],
+                                  host["H0"], d_candidates=(64, 128, 256, 512))
+        d = cfg.d
+        tune = {"seconds": time.time() - t0, "best_epoch_ms": tune_ms,
+                "candidates_d": [64, 128, 256, 512]}
     ctx = P.Context(cfg)
     t0 = time.time()
     ctx.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
@@ -366,7 +387,7 @@ def main():
                        "nnz": nnz, "precision": args.precision, "exec": "hogwild",
                        "launch": "graph", "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
                        "write_mode": args.write_mode,
-                       "grid": grid, "parallelism": f"replicas x{world}",
+                       "grid": grid, "parallelism": f"replicas x{world}", "autotune": tune,
                        "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,

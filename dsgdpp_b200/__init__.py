@@ -40,7 +40,6 @@ PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
 EXEC = {"replay": 0, "hogwild": 1}
 LAUNCH = {"stream": 0, "graph": 1}
 WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
-PIPELINE = {"auto": 0, "off": 1, "on": 2}
 TRAIN, TEST = 0, 1
 DECAY = {"Const": 0, "BoldDriver": 1}
 
@@ -62,7 +61,6 @@ class _Config(C.Structure):
         ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
         ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
         ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64), ("write_mode", C.c_int32),
-        ("pipeline", C.c_int32),
     ]
 
 
@@ -125,6 +123,9 @@ SIGNATURES = {
                                         C.c_double, C.POINTER(_TraceRow), _u32p, _u32p]),
     "dsgdpp_controller_features": (None, [_f64p, _f64p, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, _f32p]),
+    "dsgdpp_autotune": (C.c_int, [C.POINTER(_Config), C.c_uint64, _u32p, _u32p, _f64p, _f64p,
+                                  _f64p, _u32p, C.c_uint32, C.c_uint32, C.c_double,
+                                  C.POINTER(_Config), _f64p]),
     "dsgdpp_rng_create": (_P, [C.c_uint32]),
     "dsgdpp_rng_destroy": (None, [_P]),
     "dsgdpp_rng_next": (C.c_uint32, [_P]),
@@ -203,7 +204,6 @@ class Config:
     ctas_per_sm: int = 0
     layout_seed: int = 0x5EED5EED
     write_mode: str = "auto"
-    pipeline: str = "auto"
 
     def to_c(self) -> _Config:
         c = _Config()
@@ -223,7 +223,6 @@ class Config:
         c.lanes_per_nnz, c.vecs_per_lane = self.lanes_per_nnz, self.vecs_per_lane
         c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
         c.write_mode = WRITE_MODE[self.write_mode]
-        c.pipeline = PIPELINE[self.pipeline]
         return c
 
 
@@ -386,6 +385,27 @@ class Context:
         return [dict(epoch=r.epoch, loss=r.loss, test_loss=r.test_loss, eps=r.eps,
                      time_eps=r.time_eps, time_epoch=r.time_epoch, time_loss=r.time_loss,
                      time_test_loss=r.time_test_loss) for r in rows]
+
+
+def autotune(config: Config, rows, cols, vals, W, H, d_candidates=(64, 128, 256, 512),
+             epochs: int = 3, eps: float = 0.001):
+    """Fastest (d, lanes, vecs, CTAs/SM) for this data; returns (Config, ms)."""
+    base = config.to_c()
+    r, c, v = _u32(rows), _u32(cols), _f64(vals)
+    w, h = _f64(W), _f64(H)
+    ds = np.array(d_candidates, np.uint32)
+    best = _Config()
+    ms = C.c_double()
+    rc = lib.dsgdpp_autotune(C.byref(base), len(v), _ptr(r, C.c_uint32), _ptr(c, C.c_uint32),
+                             _ptr(v, C.c_double), _ptr(w, C.c_double), _ptr(h, C.c_double),
+                             _ptr(ds, C.c_uint32), len(ds), epochs, eps, C.byref(best),
+                             C.byref(ms))
+    if rc != OK:
+        raise DsgdppError(rc, "autotune")
+    import dataclasses
+    out = dataclasses.replace(config, d=best.d, lanes_per_nnz=best.lanes_per_nnz,
+                              vecs_per_lane=best.vecs_per_lane, ctas_per_sm=best.ctas_per_sm)
+    return out, ms.value
 
 
 # ---- host utilities ---------------------------------------------------------

@@ -71,6 +71,10 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print):
                     ctx.restore_factors()
                     ctx.epoch(eps * math.exp(c))
                     losses.append(ctx.loss())
+                losses = np.array(losses)
+                if np.all(~np.isfinite(losses)) or not np.all(np.isfinite(f)):
+                    break
+                losses[~np.isfinite(losses)] = np.inf
                 X.append(f)
                 y.append(float(CANDIDATES[int(np.argmin(losses))]))
                 # advance by the behaviour policy from the saved state
@@ -92,6 +96,8 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print):
                 eps = nxt
                 if len(X) >= count:
                     break
+                if not math.isfinite(cur) or cur > 4.0 * tr[0]:
+                    break  # the behaviour policy diverged: later states are not useful
         log(f"traces {len(X)}/{count} (m={prob['m']} n={prob['n']} r={prob['r']} "
             f"nnz={prob['nnz']} noise={prob['noise']:.2f}) {time.time() - t0:.0f}s")
     return np.array(X, np.float32), np.array(y, np.float32)
@@ -100,6 +106,8 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print):
 def train(X, y, steps=3000, batch=256, lr=1e-3, seed=0, device=0, val_frac=0.1):
     """Trains a fresh network with the CUDA Adam kernels; returns (net, train, val loss)."""
     rng = np.random.default_rng(seed)
+    keep = np.all(np.isfinite(X), axis=1) & np.isfinite(y)
+    X, y = X[keep], y[keep]
     idx = rng.permutation(len(X))
     nval = max(1, int(val_frac * len(X)))
     val, tr = idx[:nval], idx[nval:]

@@ -13,128 +13,12 @@
 #include <vector>
 
 #include "../../include/dsgdpp.h"
+#include "context.h"
 #include "kernels.cuh"
 #include "schedule.h"
 
 using namespace dsgdpp;
 
-namespace {
-
-struct DevMatrix {
-  bool present = false;
-  uint64_t nnz = 0;
-  uint32_t* row = nullptr;
-  uint32_t* col = nullptr;
-  void* val = nullptr;
-  uint64_t* block_ptr = nullptr;
-  std::vector<uint64_t> h_block_ptr;
-};
-
-class Error {
- public:
-  Error(int code, std::string msg) : code(code), msg(std::move(msg)) {}
-  int code;
-  std::string msg;
-};
-
-inline void check_cuda(cudaError_t e, const char* what) {
-  if (e != cudaSuccess)
-    throw Error(e == cudaErrorMemoryAllocation ? DSGDPP_E_NOMEM : DSGDPP_E_CUDA,
-                std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <typename T>
-T* dalloc(size_t count, const char* what) {
-  void* p = nullptr;
-  if (count == 0) count = 1;
-  check_cuda(cudaMalloc(&p, count * sizeof(T)), what);
-  return static_cast<T*>(p);
-}
-template <typename T>
-T* halloc(size_t count, const char* what) {
-  void* p = nullptr;
-  if (count == 0) count = 1;
-  check_cuda(cudaMallocHost(&p, count * sizeof(T)), what);
-  return static_cast<T*>(p);
-}
-template <typename T>
-void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
-  p = nullptr;
-}
-template <typename T>
-void hfree(T*& p) {
-  if (p) cudaFreeHost((void*)p);
-  p = nullptr;
-}
-
-uint32_t vec_width(int precision) { return precision == kFp64 ? 2 : (precision == kFp32 ? 4 : 8); }
-size_t elem_size(int precision) { return precision == kFp64 ? 8 : (precision == kFp32 ? 4 : 2); }
-
-}  // namespace
-
-struct dsgdpp_ctx {
-  dsgdpp_config cfg{};
-  std::string err;
-  cudaStream_t stream = nullptr;
-  int num_sms = 0;
-  uint32_t d = 0, r = 0, rp = 0;
-  std::vector<uint64_t> off1, off2;  // with the end offset appended
-  uint64_t* d_off1 = nullptr;
-  uint64_t* d_off2 = nullptr;
-  DevMatrix mat[2];
-  void* W = nullptr;
-  void* H = nullptr;
-  bool factors_set = false;
-  uint32_t* cnt1 = nullptr;
-  uint32_t* cnt2 = nullptr;
-  void* inv1 = nullptr;
-  void* inv2 = nullptr;
-  double* staging = nullptr;  // (m + n) * r doubles, factor upload / download
-  void* W_saved = nullptr;    // factor snapshot (dsgdpp_save_factors)
-  void* H_saved = nullptr;
-  // per-epoch inputs (pinned host copies feed the device copies)
-  uint32_t* h_schedule = nullptr;
-  uint32_t* d_schedule = nullptr;
-  EpochParams* h_params = nullptr;
-  EpochParams* d_params = nullptr;
-  float* h_sigma = nullptr;   // [2d][d][3]
-  float* d_sigma = nullptr;
-  float* h_scales = nullptr;  // [2d + 1]
-  float* d_scales = nullptr;
-  Segment* d_segs = nullptr;
-  uint32_t* d_counters = nullptr;
-  // replay
-  uint32_t* h_positions = nullptr;
-  uint32_t* d_positions = nullptr;
-  uint64_t positions_cap = 0;
-  uint64_t* h_pos_offset = nullptr;
-  uint64_t* d_pos_offset = nullptr;
-  uint8_t* h_mask = nullptr;  // [2d][2d]
-  uint8_t* d_mask = nullptr;
-  // losses
-  double* d_partials = nullptr;
-  double* d_out = nullptr;
-  double* h_out = nullptr;
-  uint32_t loss_grid = 0;
-  // Hogwild launch shape
-  uint32_t lanes = 0, vecs = 0, grid = 0;
-  int atomic_writes = 0;
-  int pipeline = 1;
-  // graph of one Hogwild epoch
-  cudaGraphExec_t graph_exec = nullptr;
-  // timing / ordering
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_inputs = nullptr;
-  bool epoch_timed = false;
-  // per-kernel timing of the Hogwild sub-epoch kernels (stream launch only)
-  bool profiling = false;
-  std::vector<cudaEvent_t> prof_ev;  // 2d + 1 events around the sub-epoch kernels
-  double prof_ms = 0;                // summed sub-epoch kernel time of profiled epochs
-  uint64_t prof_launches = 0;
-  bool prof_pending = false;
-  Random32 master{0};
-  uint32_t epoch_counter = 0;
-};
 
 namespace {
 
@@ -172,7 +56,7 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
   if ((uint64_t)lanes * vecs < nvec)
     throw Error(DSGDPP_E_INVALID, "lanes_per_nnz x vecs_per_lane does not cover the rank");
   int per_sm = hogwild_ctas_per_sm(c->cfg.precision, lanes, vecs, c->atomic_writes != 0,
-                                   c->pipeline != 0, c->d);
+                                   c->d + 1);
   if (per_sm <= 0)
     throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
                                       ", vecs_per_lane=" + std::to_string(vecs));
@@ -199,7 +83,6 @@ void validate_config(const dsgdpp_config* c) {
   if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
     throw Error(DSGDPP_E_INVALID, "unknown launch form");
   if (c->write_mode < 0 || c->write_mode > 2) throw Error(DSGDPP_E_INVALID, "unknown write mode");
-  if (c->pipeline < 0 || c->pipeline > 2) throw Error(DSGDPP_E_INVALID, "unknown pipeline mode");
   if (c->update < 0 || c->update > 2) throw Error(DSGDPP_E_INVALID, "unknown update");
   if (c->regularize < 0 || c->regularize > 1) throw Error(DSGDPP_E_INVALID, "unknown regularize");
   if (c->loss < 0 || c->loss > 2) throw Error(DSGDPP_E_INVALID, "unknown loss");
@@ -259,6 +142,13 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   c->d_scales = dalloc<float>(d2 + 1, "scales");
   c->d_segs = dalloc<Segment>((size_t)d2 * (d + 1), "segments");
   c->d_counters = dalloc<uint32_t>(d2, "counters");
+  {  // launch s covers the d segments of sub-epoch s, counter s
+    std::vector<LaunchDesc> ld(d2);
+    for (uint32_t s = 0; s < d2; ++s) ld[s] = LaunchDesc{(uint64_t)s * (d + 1), d, s};
+    c->d_launches = dalloc<LaunchDesc>(d2, "launches");
+    check_cuda(cudaMemcpy(c->d_launches, ld.data(), d2 * sizeof(LaunchDesc), cudaMemcpyHostToDevice),
+               "launches");
+  }
   c->h_pos_offset = halloc<uint64_t>((size_t)d2 * d + 1, "pos_offset");
   c->d_pos_offset = dalloc<uint64_t>((size_t)d2 * d + 1, "pos_offset");
   c->h_mask = halloc<uint8_t>((size_t)d2 * d2, "mask");
@@ -275,7 +165,6 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
     throw Error(DSGDPP_E_UNSUPPORTED, "atomic writes cannot truncate");
   c->atomic_writes = cfg->write_mode == DSGDPP_WRITE_ATOMIC ||
                      (cfg->write_mode == DSGDPP_WRITE_AUTO && !cfg->truncate);
-  c->pipeline = cfg->pipeline != DSGDPP_PIPELINE_OFF;
   if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
 }
 
@@ -291,7 +180,7 @@ void destroy_impl(dsgdpp_ctx* c) {
   dfree(c->W_saved); dfree(c->H_saved);
   hfree(c->h_schedule); dfree(c->d_schedule); hfree(c->h_params); dfree(c->d_params);
   hfree(c->h_sigma); dfree(c->d_sigma); hfree(c->h_scales); dfree(c->d_scales);
-  dfree(c->d_segs); dfree(c->d_counters);
+  dfree(c->d_segs); dfree(c->d_counters); dfree(c->d_launches);
   hfree(c->h_positions); dfree(c->d_positions); hfree(c->h_pos_offset); dfree(c->d_pos_offset);
   hfree(c->h_mask); dfree(c->d_mask);
   dfree(c->d_partials); dfree(c->d_out); hfree(c->h_out);
@@ -519,24 +408,24 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
     check_cuda(cudaMemcpyAsync(c->d_scales, c->h_scales, (d2 + 1) * 4, cudaMemcpyHostToDevice,
                                st), "H2D scales");
   }
-  SegBuildArgs sb{c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr, c->d_segs,
-                  c->d_counters, d};
+  SegBuildArgs sb{c->d_params, c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr,
+                  c->d_segs, c->d_counters, d};
   check_cuda(launch_build_segments(sb, st), "build_segments");
   HogwildArgs a{};
   const DevMatrix& M = c->mat[0];
   a.row = M.row; a.col = M.col; a.val = M.val;
   a.inv1 = c->inv1; a.inv2 = c->inv2;
   a.W = c->W; a.H = c->H;
-  a.segs = c->d_segs; a.counters = c->d_counters; a.params = c->d_params;
-  a.d = d; a.r = c->r; a.rp = c->rp;
+  a.segs = c->d_segs; a.launches = c->d_launches; a.counters = c->d_counters;
+  a.params = c->d_params; a.smem_segs = d + 1;
+  a.r = c->r; a.rp = c->rp;
   a.update = c->cfg.update; a.truncate = c->cfg.truncate; a.sgd_order = c->cfg.sgd_order;
   a.atomic = c->atomic_writes;
-  a.pipe = c->pipeline;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
   for (uint32_t s = 0; s < d2; ++s) {
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[s], st), "event");
-    check_cuda(launch_hogwild_subepoch(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
+    check_cuda(launch_hogwild(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
                "hogwild_subepoch");
   }
   if (prof) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");

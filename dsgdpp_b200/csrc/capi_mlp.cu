@@ -197,12 +197,18 @@ void dsgdpp_controller_features(const double* tr, const double* te, double eps, 
     f[k] = lr(tr[k], tr[k + 1]) * 10.0f;
     f[4 + k] = lr(te[k], te[k + 1]) * 10.0f;
   }
-  f[8] = (float)(std::log10(std::fmax(eps, 1e-30)) / 3.0);
-  f[9] = (float)(std::log10(std::fmax(upd_mean, 1e-30)) / 3.0);
-  f[10] = (float)(std::log10(std::fmax(upd_max, 1e-30)) / 3.0);
-  f[11] = (float)epoch_frac;
+  // log10 of a positive quantity / 3, bounded to [-10, 10]; a non-finite or
+  // huge value (a diverging run) maps to the upper bound
+  auto lg = [](double v) -> float {
+    if (!(v == v) || v > 1e30) return 10.0f;
+    return (float)std::fmax(-10.0, std::fmin(10.0, std::log10(std::fmax(v, 1e-30)) / 3.0));
+  };
+  f[8] = lg(eps);
+  f[9] = lg(upd_mean);
+  f[10] = lg(upd_max);
+  f[11] = (float)std::fmax(0.0, std::fmin(1.0, epoch_frac));
   f[12] = lr(tr[0], te[0]);
-  f[13] = (float)last_log_mult;
+  f[13] = (float)std::fmax(-1.0, std::fmin(1.0, last_log_mult));
   f[14] = (tr[0] > 0 && tr[1] > 0) ? (tr[0] < tr[1] ? 1.0f : -1.0f) : 0.0f;
   f[15] = 1.0f;
 }

@@ -99,6 +99,15 @@ struct Segment {
   float rho_w;           // sigma_H / sigma_W
   float rho_h;           // sigma_W / sigma_H
   uint32_t col_block;    // b2
+  double eps;            // step size of the segment's problem
+};
+
+// One Hogwild launch: segments [seg_begin, seg_begin + nseg) of the segment
+// array (entry nseg holds the chunk total) and its work counter.
+struct LaunchDesc {
+  uint64_t seg_begin;
+  uint32_t nseg;
+  uint32_t counter;
 };
 
 }  // namespace dsgdpp

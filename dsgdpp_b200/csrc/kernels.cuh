@@ -31,13 +31,15 @@ struct HogwildArgs {
   const void* inv2;      // 1/nnz2 per column
   void* W;               // m x rp
   void* H;               // n x rp (column j of H is contiguous)
-  const Segment* segs;   // [2d][d+1]
-  uint32_t* counters;    // [2d] work counters (zeroed by the segment builder)
+  const Segment* segs;          // segment tables of all launches
+  const LaunchDesc* launches;   // per launch: its segments and work counter
+  uint32_t* counters;           // work counters (zeroed before the launches)
   const EpochParams* params;
-  uint32_t d, r, rp;
+  uint32_t smem_segs;           // > 0: every launch's table (at most this many entries) is
+                                // staged in shared memory; 0: searched in global memory
+  uint32_t r, rp;
   int update, truncate, sgd_order;
-  int atomic;            // 1: write the update atomically (vector atomic add; CAS for BF16)
-  int pipe;              // 1: prefetch the next chunk's entries and the next step's vectors
+  int atomic;                   // 1: write the update atomically (vector atomic add)
   double lambda, tmin, tmax;
 };
 
@@ -62,6 +64,7 @@ struct ReplayArgs {
 };
 
 struct SegBuildArgs {
+  const EpochParams* params;  // eps of the epoch
   const uint32_t* schedule;   // [2d][d]
   const uint64_t* block_ptr;  // d*2d+1
   const float* sigma;         // [2d][d][3] lazy L2 scales, or null (all ones)
@@ -72,12 +75,11 @@ struct SegBuildArgs {
 
 // ---- launchers (return cudaError_t) -------------------------------------------
 cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);
-cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs,
-                                    const HogwildArgs& a, uint32_t s, uint32_t grid,
-                                    cudaStream_t st);
+cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
+                           uint32_t launch_index, uint32_t grid, cudaStream_t st);
 // CTAs per SM that the Hogwild kernel sustains for this configuration
-int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe,
-                        uint32_t d);
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
+                        uint32_t smem_segs);
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
 // RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,

@@ -45,8 +45,8 @@ __device__ __forceinline__ float block_sum64(float v, float* sh) {
 }
 
 // One CTA (64 threads) per sample.  out[b] = clip(net(x_b), -1, 1).  With
-// grads != null, also the gradient of (out_raw - y)^2 / batch into
-// grads[b][kParams] (zero where the clip is active) and the sample's loss.
+// grads != null, also the gradient of (net(x_b) - y)^2 / batch (unclipped
+// output) into grads[b][kParams] and the sample's loss.
 __global__ void __launch_bounds__(kHid) mlp_kernel(const float* __restrict__ P, const float* X,
                                                    const float* Y, int batch, float* out,
                                                    float* grads, float* losses) {
@@ -68,10 +68,11 @@ __global__ void __launch_bounds__(kHid) mlp_kernel(const float* __restrict__ P, 
   const float clipped = fminf(1.0f, fmaxf(-1.0f, raw));
   if (j == 0 && out) out[b] = clipped;
   if (!grads) return;
+  // the loss is taken on the unclipped output (the clip applies to the
+  // proposed multiplier only), so a saturated output still gets a gradient
   const float y = Y[b];
-  const bool active = raw > -1.0f && raw < 1.0f;
-  const float dout = active ? 2.0f * (raw - y) / (float)batch : 0.0f;
-  if (j == 0 && losses) losses[b] = (clipped - y) * (clipped - y) / (float)batch;
+  const float dout = 2.0f * (raw - y) / (float)batch;
+  if (j == 0 && losses) losses[b] = (raw - y) * (raw - y) / (float)batch;
   float* g = grads + (size_t)b * kParams;
   g[kW3 + j] = dout * h2;
   if (j == 0) g[kB3] = dout;

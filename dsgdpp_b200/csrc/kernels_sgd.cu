@@ -57,269 +57,203 @@ __device__ __forceinline__ void store_vec<__nv_bfloat16>(__nv_bfloat16* p, const
   *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-// Entries of one chunk, one per lane.
-template <typename C>
-struct ChunkRegs {
-  uint64_t rb;    // first entry of the chunk
-  uint32_t nrec;  // entries in the chunk (<= 32)
-  uint32_t seg;   // segment (block) of the chunk
-  uint32_t row, col;
-  C x, ca, cb;    // value, and f2/nnz1, f2/nnz2 (Nzsl_L2) or f2 (Nzsl_Nzl2) of this lane's entry
-};
+// BF16 atomic write: the new value is rounded stochastically against the
+// value read (exactly as a store would write it), and the difference between
+// that rounded value and the value read -- exact in BF16 for updates of a few
+// ulps -- is added with one 16-byte vector atomic.  Without a concurrent update
+// the row ends exactly as a store would leave it; with one, neither is lost.
+__device__ __forceinline__ void red_bf16_increment(__nv_bfloat16* q, const uint4& old,
+                                                   const float (&nv)[8], const Philox4& rnd) {
+  const uint32_t ow[4] = {old.x, old.y, old.z, old.w};
+  uint32_t inc[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    uint32_t halves = 0;
+#pragma unroll
+    for (int hlf = 0; hlf < 2; ++hlf) {
+      const uint32_t rbits = (ow[k] >> (16 * hlf)) & 0xffffu;
+      const uint32_t tbits = bf16_sr_bits(nv[2 * k + hlf], rnd.v[k] >> (16 * hlf)) & 0xffffu;
+      const float d = __uint_as_float(tbits << 16) - __uint_as_float(rbits << 16);
+      const uint32_t dbits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(d));
+      halves |= dbits << (16 * hlf);
+    }
+    inc[k] = halves;
+  }
+  asm volatile("red.relaxed.gpu.global.add.noftz.v4.bf16x2 [%0], {%1, %2, %3, %4};"
+               ::"l"(q), "r"(inc[0]), "r"(inc[1]), "r"(inc[2]), "r"(inc[3]) : "memory");
+}
 
-// W row and H column vectors of one step (32/LPN entries of a chunk).
-template <int VPL>
-struct StepRegs {
-  uint4 w[VPL], h[VPL];
-  uint32_t row, col;
-};
-
-template <typename T, int LPN, int VPL, bool ATOMIC>
-struct Hogwild {
+// One launch = one work list of segments (a segment = one conflict-free block
+// of a sub-epoch; several problems' segments in the batched form).  Warps take
+// 32-entry chunks from the launch's work counter; a chunk's entries are loaded
+// one per lane, and 32/LPN entries are updated at once, each W/H vector loaded
+// right before it is used.  (Prefetching the next chunk's rows into registers
+// or into shared memory with cp.async measured slower on B200: the extra
+// registers or shared memory cost more resident warps than the prefetch gains.)
+template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM>
+__global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
-  static constexpr int VW = E::VW;
-  static constexpr int NG = 32 / LPN;  // entries updated at once by a warp
-  static constexpr bool kSR = sizeof(T) == 2;
+  constexpr int VW = E::VW;
+  constexpr int NG = 32 / LPN;
+  constexpr bool kSR = sizeof(T) == 2;
 
-  const HogwildArgs& a;
-  const Segment* seg;
-  const uint32_t d, total, lane, grp, gl, nwarps;
-  const EpochParams ep;
-  const C eps, f2, tmin, tmax;
-  const uint64_t mulA, addB, hkey;
-  T* const W;
-  T* const H;
-
-  __device__ uint32_t permute(uint32_t lc) const {
-    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
-      return (uint32_t)(mix64(hkey ^ ((uint64_t)lc << 20)) % total);
-    return (uint32_t)((mulA * lc + addB) % total);  // WOR: affine permutation; SEQ: identity
+  const LaunchDesc ld = a.launches[li];
+  const Segment* gseg = a.segs + ld.seg_begin;
+  const uint32_t nseg = ld.nseg;
+  // SMEM: the segment table is staged in shared memory; otherwise (large
+  // batched tables) it is searched in global memory
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Segment* seg = gseg;
+  if constexpr (SMEM) {
+    Segment* ss = reinterpret_cast<Segment*>(smem_raw);
+    for (uint32_t k = threadIdx.x; k <= nseg; k += blockDim.x) ss[k] = gseg[k];
+    __syncthreads();
+    seg = ss;
   }
+  const uint32_t total = seg[nseg].chunk_begin;
+  if (total == 0 || nseg == 0) return;
+  uint32_t* counter = a.counters + ld.counter;
 
-  __device__ void load_chunk(uint32_t lc, ChunkRegs<C>& c) const {
-    const uint32_t pc = permute(lc);
-    uint32_t lo = 0, hi = d - 1;  // the last segment with chunk_begin <= pc
+  const EpochParams ep = *a.params;
+  const C lambda2 = (C)(2.0 * a.lambda);
+  const C tmin = (C)a.tmin, tmax = (C)a.tmax;
+  const uint64_t h = mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)li << 17) ^ ep.epoch);
+  uint64_t mulA = 1, addB = 0;
+  if (a.sgd_order == 2) {  // WOR: affine permutation of the chunks
+    mulA = kPrimes[h & 7u] % total;
+    addB = (h >> 8) % total;
+  }
+  const C* inv1 = reinterpret_cast<const C*>(a.inv1);
+  const C* inv2 = reinterpret_cast<const C*>(a.inv2);
+  const C* vals = reinterpret_cast<const C*>(a.val);
+  T* W = reinterpret_cast<T*>(a.W);
+  T* H = reinterpret_cast<T*>(a.H);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t grp = lane / LPN, gl = lane % LPN;
+
+  for (;;) {
+    uint32_t lc = 0;
+    if (lane == 0) lc = atomicAdd(counter, 1u);
+    lc = __shfl_sync(kFullMask, lc, 0);
+    if (lc >= total) break;
+    uint32_t pc;
+    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
+      pc = (uint32_t)(mix64(h ^ ((uint64_t)lc << 20)) % total);
+    else
+      pc = (uint32_t)((mulA * lc + addB) % total);
+    uint32_t lo = 0, hi = nseg - 1;  // the last segment with chunk_begin <= pc
     while (lo < hi) {
       const uint32_t mid = (lo + hi + 1) >> 1;
       if (seg[mid].chunk_begin <= pc) lo = mid; else hi = mid - 1;
     }
     const uint32_t cin = pc - seg[lo].chunk_begin;
-    c.seg = lo;
-    c.rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
-    c.nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
-    c.row = 0; c.col = 0; c.x = 0; c.ca = 0; c.cb = 0;
-    if (lane < c.nrec) {
-      c.row = a.row[c.rb + lane];
-      c.col = a.col[c.rb + lane];
-      c.x = reinterpret_cast<const C*>(a.val)[c.rb + lane];
+    const uint64_t rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
+    const uint32_t nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
+    const C eps = (C)seg[lo].eps, f2 = eps * lambda2;
+    const C cwh = (C)seg[lo].cwh, rw = (C)seg[lo].rho_w, rh = (C)seg[lo].rho_h;
+
+    uint32_t my_row = 0, my_col = 0;
+    C my_x = 0, my_a = 0, my_b = 0;
+    if (lane < nrec) {
+      my_row = a.row[rb + lane];
+      my_col = a.col[rb + lane];
+      my_x = vals[rb + lane];
       if (a.update == kUpdNzslL2) {
-        c.ca = f2 * reinterpret_cast<const C*>(a.inv1)[c.row];
-        c.cb = f2 * reinterpret_cast<const C*>(a.inv2)[c.col];
+        my_a = f2 * inv1[my_row];
+        my_b = f2 * inv2[my_col];
       } else if (a.update == kUpdNzslNzl2) {
-        c.ca = f2;
-        c.cb = f2;
+        my_a = f2;
+        my_b = f2;
       }
     }
-  }
 
-  __device__ void load_step(const ChunkRegs<C>& c, uint32_t t, StepRegs<VPL>& st) const {
-    const uint32_t ri = t * NG + grp;
-    st.row = __shfl_sync(kFullMask, c.row, ri & 31u);
-    st.col = __shfl_sync(kFullMask, c.col, ri & 31u);
-    const bool valid = ri < c.nrec;
-    const T* wp = W + (size_t)st.row * a.rp;
-    const T* hp = H + (size_t)st.col * a.rp;
+    for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
+      const uint32_t ri = t0 + grp;
+      const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
+      const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
+      const C x = __shfl_sync(kFullMask, my_x, ri);
+      const C ca = __shfl_sync(kFullMask, my_a, ri);
+      const C cb = __shfl_sync(kFullMask, my_b, ri);
+      const bool valid = ri < nrec;
+      T* wp = W + (size_t)row * a.rp;
+      T* hp = H + (size_t)col * a.rp;
+      uint4 wv[VPL], hv[VPL];
+      bool live[VPL];
 #pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-      if (valid && e0 < a.rp) {
-        st.w[v] = *reinterpret_cast<const uint4*>(wp + e0);
-        st.h[v] = *reinterpret_cast<const uint4*>(hp + e0);
-      } else {
-        st.w[v] = make_uint4(0, 0, 0, 0);
-        st.h[v] = make_uint4(0, 0, 0, 0);
-      }
-    }
-  }
-
-  __device__ void apply_step(const ChunkRegs<C>& c, uint32_t t, const StepRegs<VPL>& st) const {
-    const uint32_t ri = t * NG + grp;
-    const C x = __shfl_sync(kFullMask, c.x, ri & 31u);
-    const C ca = __shfl_sync(kFullMask, c.ca, ri & 31u);
-    const C cb = __shfl_sync(kFullMask, c.cb, ri & 31u);
-    const bool valid = ri < c.nrec;
-    C wf[VPL][VW], hf[VPL][VW];
-    C dot = 0;
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      E::unpack(st.w[v], wf[v]);
-      E::unpack(st.h[v], hf[v]);
-#pragma unroll
-      for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
-    }
-#pragma unroll
-    for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
-    const Segment& g = seg[c.seg];
-    const C f1 = (C)-2 * eps * (x - dot * (C)g.cwh);
-    const C fw = f1 * (C)g.rho_w, fh = f1 * (C)g.rho_h;
-    T* wp = W + (size_t)st.row * a.rp;
-    T* hp = H + (size_t)st.col * a.rp;
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-      if (!valid || e0 >= a.rp) continue;
-      C nw[VW], nh[VW];
-#pragma unroll
-      for (int e = 0; e < VW; ++e) {
-        nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
-        nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
-      }
-      if (!ATOMIC && a.truncate) {
-#pragma unroll
-        for (int e = 0; e < VW; ++e)
-          if (e0 + e < a.r) {
-            nw[e] = clampw(nw[e], tmin, tmax, eps);
-            nh[e] = clampw(nh[e], tmin, tmax, eps);
-          }
-      }
-      if constexpr (ATOMIC && !kSR) {
-        // add the update, so concurrent updates of one row are not lost
-        if constexpr (sizeof(T) == 4) {
-          atomicAdd(reinterpret_cast<float4*>(wp + e0),
-                    make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
-          atomicAdd(reinterpret_cast<float4*>(hp + e0),
-                    make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        live[v] = valid && e0 < a.rp;
+        if (live[v]) {
+          wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
+          hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
         } else {
+          wv[v] = make_uint4(0, 0, 0, 0);
+          hv[v] = make_uint4(0, 0, 0, 0);
+        }
+      }
+      C dot = 0;
+      C wf[VPL][VW], hf[VPL][VW];
 #pragma unroll
-          for (int e = 0; e < VW; ++e) {
-            atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
-            atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
+      for (int v = 0; v < VPL; ++v) {
+        E::unpack(wv[v], wf[v]);
+        E::unpack(hv[v], hf[v]);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+      }
+#pragma unroll
+      for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+      const C f1 = (C)-2 * eps * (x - dot * cwh);
+      const C fw = f1 * rw, fh = f1 * rh;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        if (!live[v]) continue;
+        C nw[VW], nh[VW];
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+          nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+        }
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        if (!ATOMIC && a.truncate) {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            if (e0 + e < a.r) {
+              nw[e] = clampw(nw[e], tmin, tmax, eps);
+              nh[e] = clampw(nh[e], tmin, tmax, eps);
+            }
+        }
+        const uint64_t rec = rb + ri;
+        if constexpr (ATOMIC && !kSR) {
+          // add the update, so concurrent updates of one row are not lost
+          if constexpr (sizeof(T) == 4) {
+            atomicAdd(reinterpret_cast<float4*>(wp + e0),
+                      make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
+            atomicAdd(reinterpret_cast<float4*>(hp + e0),
+                      make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
+          } else {
+#pragma unroll
+            for (int e = 0; e < VW; ++e) {
+              atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
+              atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
+            }
+          }
+        } else {
+          Philox4 r1, r2;
+          if constexpr (kSR) {
+            r1 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
+            r2 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
+                               ep.key0, ep.key1);
+          }
+          if constexpr (ATOMIC && kSR) {
+            red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(wp + e0), wv[v], nw, r1);
+            red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(hp + e0), hv[v], nh, r2);
+          } else {
+            store_vec<T>(wp + e0, nw, &r1);
+            store_vec<T>(hp + e0, nh, &r2);
           }
         }
-      } else if constexpr (ATOMIC && kSR) {
-        add_bf16(c.rb + ri, e0, st.w[v], st.h[v], nw, nh, wp + e0, hp + e0);
-      } else {
-        Philox4 rw4, rh4;
-        if constexpr (kSR) {
-          const uint64_t rec = c.rb + ri;
-          rw4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
-          rh4 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
-                              ep.key0, ep.key1);
-        }
-        store_vec<T>(wp + e0, nw, &rw4);
-        store_vec<T>(hp + e0, nh, &rh4);
       }
-    }
-  }
-
-  // BF16: the new value is rounded stochastically against the value read
-  // (exactly as a store would write it), and the difference between that
-  // rounded value and the value read -- exact in BF16 for updates of a few
-  // ulps -- is added with one 16-byte vector atomic.  Without a concurrent
-  // update the row ends exactly as a store would leave it; with one, neither
-  // update is lost.
-  __device__ void add_bf16(uint64_t rec, uint32_t e0, const uint4& wv, const uint4& hv,
-                           const float (&nw)[8], const float (&nh)[8], T* wq, T* hq) const {
-    const Philox4 rw = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0,
-                                     ep.key1);
-    const Philox4 rh = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch,
-                                     e0 | 0x80000000u, ep.key0, ep.key1);
-    red_bf16_increment(wq, wv, nw, rw);
-    red_bf16_increment(hq, hv, nh, rh);
-  }
-
-  __device__ static void red_bf16_increment(T* q, const uint4& old, const float (&nv)[8],
-                                            const Philox4& rnd) {
-    const uint32_t ow[4] = {old.x, old.y, old.z, old.w};
-    uint32_t inc[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      uint32_t halves = 0;
-#pragma unroll
-      for (int hlf = 0; hlf < 2; ++hlf) {
-        const uint32_t rbits = (ow[k] >> (16 * hlf)) & 0xffffu;
-        const uint32_t tbits = bf16_sr_bits(nv[2 * k + hlf], rnd.v[k] >> (16 * hlf)) & 0xffffu;
-        const float d = __uint_as_float(tbits << 16) - __uint_as_float(rbits << 16);
-        const uint32_t dbits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(d));
-        halves |= dbits << (16 * hlf);
-      }
-      inc[k] = halves;
-    }
-    asm volatile("red.relaxed.gpu.global.add.noftz.v4.bf16x2 [%0], {%1, %2, %3, %4};"
-                 :: "l"(q), "r"(inc[0]), "r"(inc[1]), "r"(inc[2]), "r"(inc[3]) : "memory");
-  }
-
-  // all steps of one chunk; with PIPE the next step's vectors load while the
-  // current step computes
-  template <bool PIPE>
-  __device__ void process_chunk(const ChunkRegs<C>& c) const {
-    const uint32_t nsteps = (c.nrec + NG - 1) / NG;
-    if constexpr (PIPE) {
-      StepRegs<VPL> cur, nxt;
-      load_step(c, 0, cur);
-      for (uint32_t t = 0; t < nsteps; ++t) {
-        if (t + 1 < nsteps) load_step(c, t + 1, nxt);
-        apply_step(c, t, cur);
-        cur = nxt;
-      }
-    } else {
-      for (uint32_t t = 0; t < nsteps; ++t) {
-        StepRegs<VPL> cur;
-        load_step(c, t, cur);
-        apply_step(c, t, cur);
-      }
-    }
-  }
-};
-
-template <typename T, int LPN, int VPL, bool ATOMIC, bool PIPE>
-__global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t s) {
-  using HW = Hogwild<T, LPN, VPL, ATOMIC>;
-  using C = typename HW::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Segment* seg = reinterpret_cast<Segment*>(smem_raw);
-  const uint32_t d = a.d;
-  const Segment* gseg = a.segs + (size_t)s * (d + 1);
-  for (uint32_t k = threadIdx.x; k <= d; k += blockDim.x) seg[k] = gseg[k];
-  __syncthreads();
-  const uint32_t total = seg[d].chunk_begin;
-  if (total == 0) return;
-  const EpochParams ep = *a.params;
-  const uint64_t hkey = mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)s << 17) ^ ep.epoch);
-  uint64_t mulA = 1, addB = 0;
-  if (a.sgd_order == 2) {
-    mulA = kPrimes[hkey & 7u] % total;
-    addB = (hkey >> 8) % total;
-  }
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-  const HW hw{a, seg, d, total, lane, lane / LPN, lane % LPN, nwarps, ep, (C)ep.eps,
-              (C)(ep.eps * 2.0 * a.lambda), (C)a.tmin, (C)a.tmax, mulA, addB, hkey,
-              reinterpret_cast<T*>(a.W), reinterpret_cast<T*>(a.H)};
-  // chunk ids: the first one per warp is the warp's index; later ones come
-  // from the sub-epoch's work counter (offset by the warp count), fetched one
-  // chunk ahead so the atomic's latency hides behind a chunk of updates
-  uint32_t id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (id >= total) return;
-  uint32_t pending = 0;
-  if (lane == 0) pending = nwarps + atomicAdd(a.counters + s, 1u);
-  ChunkRegs<C> cur;
-  hw.load_chunk(id, cur);
-  for (;;) {
-    const uint32_t next = __shfl_sync(kFullMask, pending, 0);
-    const bool more = next < total;
-    if (more && lane == 0) pending = nwarps + atomicAdd(a.counters + s, 1u);
-    if constexpr (PIPE) {
-      ChunkRegs<C> nxt;
-      if (more) hw.load_chunk(next, nxt);  // in flight while cur is updated
-      hw.template process_chunk<true>(cur);
-      if (!more) break;
-      cur = nxt;
-    } else {
-      hw.template process_chunk<false>(cur);
-      if (!more) break;
-      hw.load_chunk(next, cur);
     }
   }
 }
@@ -360,12 +294,14 @@ __global__ void build_segments_kernel(SegBuildArgs a) {
       g.cwh = 1.f; g.rho_w = 1.f; g.rho_h = 1.f;
     }
     g.col_block = b2;
+    g.eps = a.params->eps;
     out[id] = g;
   }
   if (id == 0) {
     Segment e;
     e.rec_begin = 0; e.count = 0; e.chunk_begin = scan[d - 1];
     e.cwh = e.rho_w = e.rho_h = 1.f; e.col_block = 0xffffffffu;
+    e.eps = 0;
     out[d] = e;
     a.counters[s] = 0;
   }
@@ -538,18 +474,18 @@ __global__ void normalize_kernel<double>(double* W, double* H, uint64_t m, uint6
 }
 
 template <typename T, int LPN, int VPL>
-void* hogwild_fn(bool atomic, bool pipe) {
-  if (atomic)
-    return pipe ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, true>)
-                : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, false>);
-  return pipe ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, true>)
-              : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, false>);
+void* hogwild_fn(bool atomic, bool smem) {
+  if (smem)
+    return atomic ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, true>)
+                  : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, true>);
+  return atomic ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, false>)
+                : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, false>);
 }
 
 template <typename T>
-void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool pipe) {
+void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool smem) {
 #define DSGDPP_CASE(L, V) \
-  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>(atomic, pipe);
+  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>(atomic, smem);
   DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
   DSGDPP_CASE(2, 2) DSGDPP_CASE(4, 2) DSGDPP_CASE(8, 2) DSGDPP_CASE(16, 2) DSGDPP_CASE(32, 2)
   DSGDPP_CASE(32, 4)
@@ -557,10 +493,10 @@ void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool pipe) {
   return nullptr;
 }
 
-void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe) {
-  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs, atomic, pipe);
-  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs, atomic, pipe);
-  return pick_hogwild<__nv_bfloat16>(lanes, vecs, atomic, pipe);
+void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool smem) {
+  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs, atomic, smem);
+  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs, atomic, smem);
+  return pick_hogwild<__nv_bfloat16>(lanes, vecs, atomic, smem);
 }
 
 }  // namespace
@@ -573,26 +509,25 @@ cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool pipe,
-                        uint32_t d) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, pipe);
+int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
+                        uint32_t smem_segs) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, smem_segs > 0);
   if (!fn) return 0;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * (d + 1)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * smem_segs) !=
       cudaSuccess)
     return 0;
   return n;
 }
 
-cudaError_t launch_hogwild_subepoch(int precision, uint32_t lanes, uint32_t vecs,
-                                    const HogwildArgs& a, uint32_t s, uint32_t grid,
-                                    cudaStream_t st) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.pipe != 0);
+cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
+                           uint32_t launch_index, uint32_t grid, cudaStream_t st) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.smem_segs > 0);
   if (!fn) return cudaErrorInvalidValue;
   HogwildArgs args = a;
-  uint32_t sub = s;
-  void* params[] = {&args, &sub};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(Segment) * (a.d + 1), st);
+  uint32_t li = launch_index;
+  void* params[] = {&args, &li};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(Segment) * a.smem_segs, st);
 }
 
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st) {

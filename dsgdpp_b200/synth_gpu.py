@@ -34,11 +34,18 @@ def _draw(torch, g, cdf, size, count, device):
     return torch.clamp(torch.searchsorted(cdf, u), max=size - 1)
 
 
-def distinct_pairs(m, n, total, seed, s_row=None, s_col=None, device="cuda"):
+def _cdf(torch, w):
+    c = torch.cumsum(w.to(torch.float64), 0)
+    return c / c[-1]
+
+
+def distinct_pairs(m, n, total, seed, s_row=None, s_col=None, device="cuda", row_weights=None):
+    """`total` distinct (row, col) keys; rows by Zipf(s_row) (or `row_weights`,
+    a length-m tensor), columns by Zipf(s_col); None = uniform."""
     import torch
     g = torch.Generator(device=device)
     g.manual_seed(seed)
-    cr = _weights(torch, g, m, s_row, device)
+    cr = _cdf(torch, row_weights) if row_weights is not None else _weights(torch, g, m, s_row, device)
     cc = _weights(torch, g, n, s_col, device)
     keys = torch.empty(0, dtype=torch.int64, device=device)
     rounds = 0
@@ -77,6 +84,41 @@ def make(m, n, nnz, nnz_test, rank_true, r, noise, seed, s_row=None, s_col=None,
         v += noise * torch.randn(b - a, generator=g, device=device, dtype=torch.float64)
         vals[a:b] = v
     del Ws, Hs
+    W0 = torch.rand(m, r, generator=g, device=device, dtype=torch.float64) - 0.5
+    H0 = torch.rand(n, r, generator=g, device=device, dtype=torch.float64) - 0.5
+    out = dict(
+        rows=rows[:nnz].cpu().numpy().view(np.uint32), cols=cols[:nnz].cpu().numpy().view(np.uint32),
+        vals=vals[:nnz].cpu().numpy(),
+        trows=rows[nnz:].cpu().numpy().view(np.uint32),
+        tcols=cols[nnz:].cpu().numpy().view(np.uint32), tvals=vals[nnz:].cpu().numpy(),
+        W0=W0.cpu().numpy(), H0=H0.cpu().numpy())
+    del rows, cols, vals, W0, H0
+    torch.cuda.empty_cache()
+    return out
+
+
+def make_ratings(m, n, nnz, nnz_test, r, seed, mu=4.2, sigma=1.3, s_col=0.9, rank_true=16,
+                 mean=3.6, std=1.1, device="cuda", chunk=8_000_000):
+    """Netflix-shaped stand-in: row degrees lognormal(mu, sigma) capped at n,
+    column popularity Zipf(s_col), integer ratings 1..5 from rounding and
+    clipping a rank-`rank_true` truth scaled to the given mean and std."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 1)
+    deg = torch.exp(mu + sigma * torch.randn(m, generator=g, device=device, dtype=torch.float64))
+    deg = torch.clamp(deg, max=float(n))
+    keys, g = distinct_pairs(m, n, nnz + nnz_test, seed, None, s_col, device, row_weights=deg)
+    rows = (keys // n).to(torch.int32)
+    cols = (keys % n).to(torch.int32)
+    del keys
+    U = torch.randn(m, rank_true, generator=g, device=device) / math.sqrt(rank_true)
+    V = torch.randn(n, rank_true, generator=g, device=device) / math.sqrt(rank_true)
+    vals = torch.empty(rows.numel(), dtype=torch.float64, device=device)
+    for a in range(0, rows.numel(), chunk):
+        b = min(a + chunk, rows.numel())
+        z = (U[rows[a:b].long()] * V[cols[a:b].long()]).sum(1).double()
+        vals[a:b] = torch.clamp(torch.round(mean + std * z), 1.0, 5.0)
+    del U, V
     W0 = torch.rand(m, r, generator=g, device=device, dtype=torch.float64) - 0.5
     H0 = torch.rand(n, r, generator=g, device=device, dtype=torch.float64) - 0.5
     out = dict(

@@ -74,10 +74,6 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 #define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */
 #define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically: vector atomic add (FP32/FP64);
                                  BF16 adds the increment to the stochastically rounded value */
-/* Hogwild prefetching of the next chunk's entries and the next step's vectors */
-#define DSGDPP_PIPELINE_AUTO 0 /* on */
-#define DSGDPP_PIPELINE_OFF 1
-#define DSGDPP_PIPELINE_ON 2
 /* matrices */
 #define DSGDPP_TRAIN 0
 #define DSGDPP_TEST 1
@@ -108,7 +104,6 @@ typedef struct dsgdpp_config {
   uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
   int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
-  int32_t pipeline;       /* Hogwild prefetching: DSGDPP_PIPELINE_* */
 } dsgdpp_config;
 
 /* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */
@@ -235,7 +230,8 @@ int dsgdpp_mlp_param_count(void);
 int dsgdpp_mlp_get_params(dsgdpp_mlp* mlp, float* params);
 int dsgdpp_mlp_set_params(dsgdpp_mlp* mlp, const float* params);
 int dsgdpp_mlp_forward(dsgdpp_mlp* mlp, const float* x, int batch, float* out);
-/* mean squared error against y and its gradient w.r.t. the parameters */
+/* mean squared error of the unclipped output against y, and its gradient
+ * w.r.t. the parameters */
 int dsgdpp_mlp_gradient(dsgdpp_mlp* mlp, const float* x, const float* y, int batch, float* loss,
                         float* grad);
 /* one Adam step (lr, betas 0.9/0.999, eps 1e-8) on the batch; returns the loss */
@@ -257,6 +253,17 @@ int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs, dou
 void dsgdpp_controller_features(const double* train_hist, const double* test_hist, double eps,
                                 double upd_mean, double upd_max, double epoch_frac,
                                 double last_log_mult, float* out16);
+
+/* ---- autotuning ------------------------------------------------------------- */
+/* No reference counterpart (the reference takes d from --tasks-per-rank).
+ * Times Hogwild epochs of `base` on the given training entries and factors
+ * for each d in d_candidates (NULL/0: 64, 128, 256, 512) and several
+ * lane-to-rank mappings and CTA counts per SM; writes the fastest
+ * configuration to *best and its median epoch time to *best_ms. */
+int dsgdpp_autotune(const dsgdpp_config* base, uint64_t nnz, const uint32_t* rows,
+                    const uint32_t* cols, const double* vals, const double* W, const double* H,
+                    const uint32_t* d_candidates, uint32_t nd, uint32_t epochs, double eps,
+                    dsgdpp_config* best, double* best_ms);
 
 /* ---- host utilities (no GPU needed) --------------------------------------- */
 /* rg::Random32 as pinned by this library (MT19937, Boost bucket nextInt). */
