@@ -74,6 +74,18 @@ class _TraceRow(C.Structure):
 
 _P = C.c_void_p
 _u32p = C.POINTER(C.c_uint32)
+
+
+class _Problem(C.Structure):
+    _fields_ = [
+        ("m", C.c_uint64), ("n", C.c_uint64), ("rank", C.c_uint32), ("d", C.c_uint32),
+        ("nnz", C.c_uint64), ("rows", _u32p), ("cols", _u32p), ("vals", C.POINTER(C.c_double)),
+        ("nnz_test", C.c_uint64), ("trows", _u32p), ("tcols", _u32p),
+        ("tvals", C.POINTER(C.c_double)), ("W", C.POINTER(C.c_double)),
+        ("H", C.POINTER(C.c_double)), ("seed", C.c_uint32), ("eps0", C.c_double),
+    ]
+
+
 _u64p = C.POINTER(C.c_uint64)
 _f64p = C.POINTER(C.c_double)
 _f32p = C.POINTER(C.c_float)
@@ -126,6 +138,14 @@ SIGNATURES = {
     "dsgdpp_autotune": (C.c_int, [C.POINTER(_Config), C.c_uint64, _u32p, _u32p, _f64p, _f64p,
                                   _f64p, _u32p, C.c_uint32, C.c_uint32, C.c_double,
                                   C.POINTER(_Config), _f64p]),
+    "dsgdpp_batch_create": (C.c_int, [C.POINTER(_Config), C.c_uint32, C.POINTER(_Problem),
+                                      C.POINTER(_P)]),
+    "dsgdpp_batch_destroy": (None, [_P]),
+    "dsgdpp_batch_last_error": (C.c_char_p, [_P]),
+    "dsgdpp_batch_run": (C.c_int, [_P, C.c_uint32, C.c_double, C.c_double, _f64p, _f64p,
+                                   _f64p]),
+    "dsgdpp_batch_problem_d": (C.c_int, [_P, C.c_uint32, _u32p]),
+    "dsgdpp_batch_get_factors": (C.c_int, [_P, C.c_uint32, _f64p, _f64p]),
     "dsgdpp_rng_create": (_P, [C.c_uint32]),
     "dsgdpp_rng_destroy": (None, [_P]),
     "dsgdpp_rng_next": (C.c_uint32, [_P]),
@@ -385,6 +405,93 @@ class Context:
         return [dict(epoch=r.epoch, loss=r.loss, test_loss=r.test_loss, eps=r.eps,
                      time_eps=r.time_eps, time_epoch=r.time_epoch, time_loss=r.time_loss,
                      time_test_loss=r.time_test_loss) for r in rows]
+
+
+class Batch:
+    """Many independent factorizations advanced together (dsgdpp_batch_*).
+
+    ``problems`` is a list of dicts with keys m, n, rank, rows, cols, vals,
+    W, H and optionally d (0: chosen per problem), trows/tcols/tvals, seed,
+    eps0.  ``config`` supplies everything the problems share; its m, n,
+    rank and d are ignored.
+    """
+
+    def __init__(self, config: Config, problems):
+        self.config = config
+        self._cfg = config.to_c()
+        self._keep = []
+        arr = (_Problem * len(problems))()
+        for k, p in enumerate(problems):
+            q = arr[k]
+            q.m, q.n, q.rank, q.d = p["m"], p["n"], p["rank"], p.get("d", 0)
+            rows, cols, vals = _u32(p["rows"]), _u32(p["cols"]), _f64(p["vals"])
+            W, H = _f64(p["W"]), _f64(p["H"])
+            q.nnz = len(vals)
+            q.rows, q.cols = _ptr(rows, C.c_uint32), _ptr(cols, C.c_uint32)
+            q.vals = _ptr(vals, C.c_double)
+            q.W, q.H = _ptr(W, C.c_double), _ptr(H, C.c_double)
+            keep = [rows, cols, vals, W, H]
+            if p.get("tvals") is not None and len(p["tvals"]):
+                tr, tc, tv = _u32(p["trows"]), _u32(p["tcols"]), _f64(p["tvals"])
+                q.nnz_test = len(tv)
+                q.trows, q.tcols = _ptr(tr, C.c_uint32), _ptr(tc, C.c_uint32)
+                q.tvals = _ptr(tv, C.c_double)
+                keep += [tr, tc, tv]
+            q.seed = p.get("seed", 0)
+            q.eps0 = p.get("eps0", 0.001)
+            self._keep.append(keep)
+        self.count = len(problems)
+        self.shapes = [(p["m"], p["n"], p["rank"]) for p in problems]
+        h = _P()
+        rc = lib.dsgdpp_batch_create(C.byref(self._cfg), len(problems), arr, C.byref(h))
+        self._keep = None  # the library holds its own copies
+        if rc != OK:
+            raise DsgdppError(rc, "dsgdpp_batch_create failed (details on stderr)")
+        self._h = h
+
+    def _check(self, rc, what):
+        if rc != OK:
+            raise DsgdppError(rc, f"{what}: {lib.dsgdpp_batch_last_error(self._h).decode()}")
+
+    def run(self, epochs: int, decrease: float = 0.5, increase: float = 1.05):
+        """(train losses, test losses, summed epoch device ms) after `epochs` epochs."""
+        tr = np.zeros(self.count)
+        te = np.zeros(self.count)
+        ms = C.c_double()
+        self._check(lib.dsgdpp_batch_run(self._h, epochs, decrease, increase,
+                                         _ptr(tr, C.c_double), _ptr(te, C.c_double),
+                                         C.byref(ms)), "batch_run")
+        return tr, te, ms.value
+
+    def problem_d(self, p: int) -> int:
+        d = C.c_uint32()
+        self._check(lib.dsgdpp_batch_problem_d(self._h, p, C.byref(d)), "batch_problem_d")
+        return d.value
+
+    def get_factors(self, p: int):
+        m, n, r = self.shapes[p]
+        W = np.empty((m, r))
+        H = np.empty((n, r))
+        self._check(lib.dsgdpp_batch_get_factors(self._h, p, _ptr(W, C.c_double),
+                                                 _ptr(H, C.c_double)), "batch_get_factors")
+        return W, H
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def autotune(config: Config, rows, cols, vals, W, H, d_candidates=(64, 128, 256, 512),

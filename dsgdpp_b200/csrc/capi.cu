@@ -153,7 +153,10 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   c->d_pos_offset = dalloc<uint64_t>((size_t)d2 * d + 1, "pos_offset");
   c->h_mask = halloc<uint8_t>((size_t)d2 * d2, "mask");
   c->d_mask = dalloc<uint8_t>((size_t)d2 * d2, "mask");
-  c->loss_grid = (uint32_t)c->num_sms * 4;
+  // one resident wave of the loss kernel; fixed per context, so every loss
+  // of the context is reduced in the same order
+  const int loss_per_sm = nzsl_ctas_per_sm(cfg->precision, c->rp);
+  c->loss_grid = (uint32_t)c->num_sms * (uint32_t)std::max(2, std::min(8, loss_per_sm));
   c->d_partials = dalloc<double>(2 * (size_t)c->loss_grid, "partials");
   c->d_out = dalloc<double>(4, "loss out");
   c->h_out = halloc<double>(4, "loss out");
@@ -177,6 +180,7 @@ void destroy_impl(dsgdpp_ctx* c) {
   dfree(c->d_off1); dfree(c->d_off2);
   dfree(c->W); dfree(c->H); dfree(c->cnt1); dfree(c->cnt2); dfree(c->inv1); dfree(c->inv2);
   dfree(c->staging);
+  dfree(c->scratch);
   dfree(c->W_saved); dfree(c->H_saved);
   hfree(c->h_schedule); dfree(c->d_schedule); hfree(c->h_params); dfree(c->d_params);
   hfree(c->h_sigma); dfree(c->d_sigma); hfree(c->h_scales); dfree(c->d_scales);
@@ -199,6 +203,32 @@ int bit_length(uint64_t v) {
   return b;
 }
 
+// Bump allocation inside one scratch buffer (256-byte aligned pieces); with a
+// null base it only adds up the size.
+struct Carver {
+  char* base = nullptr;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += std::max<size_t>(count, 1) * sizeof(T);
+    return p;
+  }
+};
+
+// record arrays of a matrix, grown only when a larger matrix arrives
+void reserve_records(DevMatrix& M, uint64_t u, bool as_double) {
+  u = std::max<uint64_t>(u, 1);
+  if (M.row && M.cap >= u) return;
+  dfree(M.row); dfree(M.col); dfree(M.val);
+  M.cap = 0;
+  M.row = dalloc<uint32_t>(u, "row");
+  M.col = dalloc<uint32_t>(u, "col");
+  check_cuda(cudaMalloc(&M.val, u * (as_double ? 8 : 4)), "val");
+  M.cap = u;
+}
+
 void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* rows,
                      const uint32_t* cols, const double* vals) {
   if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
@@ -219,16 +249,17 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   const bool shuffled = which == DSGDPP_TRAIN && c->cfg.exec == DSGDPP_EXEC_HOGWILD;
 
   DevMatrix& M = c->mat[which];
-  dfree(M.row); dfree(M.col); dfree(M.val); dfree(M.block_ptr);
   M.present = false;
   M.nnz = 0;
-  M.block_ptr = dalloc<uint64_t>(nblocks + 1, "block_ptr");
+  if (!M.block_ptr || M.nblocks != nblocks) {
+    dfree(M.block_ptr);
+    M.block_ptr = dalloc<uint64_t>(nblocks + 1, "block_ptr");
+    M.nblocks = nblocks;
+  }
   M.h_block_ptr.assign(nblocks + 1, 0);
   if (nnz == 0) {
     check_cuda(cudaMemset(M.block_ptr, 0, (nblocks + 1) * 8), "block_ptr");
-    M.row = dalloc<uint32_t>(1, "row");
-    M.col = dalloc<uint32_t>(1, "col");
-    check_cuda(cudaMalloc(&M.val, 8), "val");
+    reserve_records(M, 1, as_double);
     M.present = true;
     if (which == DSGDPP_TRAIN) {
       check_cuda(cudaMemset(c->cnt1, 0, c->cfg.m * 4), "cnt1");
@@ -237,110 +268,114 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
     return;
   }
 
-  uint32_t* t_rows = dalloc<uint32_t>(nnz, "rows");
-  uint32_t* t_cols = dalloc<uint32_t>(nnz, "cols");
-  double* t_vals = dalloc<double>(nnz, "vals");
-  uint64_t* keys[2] = {dalloc<uint64_t>(nnz, "keys"), dalloc<uint64_t>(nnz, "keys")};
-  uint32_t* idx[2] = {dalloc<uint32_t>(nnz, "idx"), dalloc<uint32_t>(nnz, "idx")};
-  unsigned long long* d_bad = dalloc<unsigned long long>(1, "bad");
-  std::vector<void*> temps = {t_rows, t_cols, t_vals, keys[0], keys[1], idx[0], idx[1], d_bad};
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(st);
-    for (void* p : temps) cudaFree(p);
-  };
-  try {
-    check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
-    check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
-    check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
-    check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
-    BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
-    check_cuda(launch_make_keys(g, t_rows, t_cols, nnz, keys[0], idx[0], d_bad, st), "make_keys");
-    unsigned long long bad = 0;
-    check_cuda(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st), "D2H");
-    check_cuda(cudaStreamSynchronize(st), "sync");
-    if (bad) throw Error(DSGDPP_E_INVALID, std::to_string(bad) + " entries lie outside the matrix");
-
-    const int end_bit = bit_length((uint64_t)nblocks * span - 1);
-    cub::DoubleBuffer<uint64_t> kb(keys[0], keys[1]);
-    cub::DoubleBuffer<uint32_t> vb(idx[0], idx[1]);
-    size_t tb = 0;
-    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int)nnz, 0, end_bit, st), "sort");
-    void* tmp = nullptr;
-    check_cuda(cudaMalloc(&tmp, tb), "sort temp");
-    temps.push_back(tmp);
-    check_cuda(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)nnz, 0, end_bit, st), "sort");
-    uint64_t* skeys = kb.Current();
-    uint32_t* sidx = vb.Current();
-    uint64_t* okeys = kb.Alternate();
-    uint32_t* oidx = vb.Alternate();
-
-    // run heads -> output positions (reuse the alternate index buffer)
-    uint32_t* flags = oidx;
-    uint32_t* pos = dalloc<uint32_t>(nnz, "pos");
-    temps.push_back(pos);
-    check_cuda(launch_head_flags(skeys, nnz, flags, st), "head_flags");
-    size_t sb = 0;
-    check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, sb, flags, pos, (int)nnz, st), "scan");
-    void* stmp = nullptr;
-    check_cuda(cudaMalloc(&stmp, sb), "scan temp");
-    temps.push_back(stmp);
-    check_cuda(cub::DeviceScan::ExclusiveSum(stmp, sb, flags, pos, (int)nnz, st), "scan");
-    uint32_t last_pos = 0, last_flag = 0;
-    check_cuda(cudaMemcpyAsync(&last_pos, pos + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
-    check_cuda(cudaMemcpyAsync(&last_flag, flags + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
-    check_cuda(cudaStreamSynchronize(st), "sync");
-    const uint64_t u = (uint64_t)last_pos + last_flag;
-
-    uint32_t* urow = dalloc<uint32_t>(u, "urow");
-    uint32_t* ucol = dalloc<uint32_t>(u, "ucol");
-    double* uval = dalloc<double>(u, "uval");
-    temps.push_back(urow); temps.push_back(ucol); temps.push_back(uval);
-    check_cuda(launch_merge_runs(g, skeys, sidx, pos, nnz, t_vals, t_rows, t_cols, okeys, urow,
-                                 ucol, uval, st), "merge_runs");
-    uint64_t* ukeys = okeys;
-    check_cuda(launch_block_ptr(ukeys, u, span, nblocks, M.block_ptr, st), "block_ptr");
-
-    M.row = dalloc<uint32_t>(u, "row");
-    M.col = dalloc<uint32_t>(u, "col");
-    check_cuda(cudaMalloc(&M.val, std::max<uint64_t>(u, 1) * (as_double ? 8 : 4)), "val");
-    if (shuffled) {
-      // in-block random layout: key = (block, hash(layout_seed, k))
-      uint64_t* k2 = skeys;   // free now
-      uint32_t* i2 = sidx;
-      check_cuda(launch_shuffle_keys(ukeys, u, span, c->cfg.layout_seed, k2, i2, st), "shuffle");
-      cub::DoubleBuffer<uint64_t> kb2(k2, ukeys);
-      cub::DoubleBuffer<uint32_t> vb2(i2, flags);
-      size_t tb2 = 0;
-      check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, tb2, kb2, vb2, (int)u, 0, 64, st), "sort");
-      void* tmp2 = nullptr;
-      check_cuda(cudaMalloc(&tmp2, tb2), "sort temp");
-      temps.push_back(tmp2);
-      check_cuda(cub::DeviceRadixSort::SortPairs(tmp2, tb2, kb2, vb2, (int)u, 0, 64, st), "sort");
-      check_cuda(launch_gather_records(vb2.Current(), u, urow, ucol, uval, M.row, M.col, M.val,
-                                       as_double, st), "gather");
-    } else {
-      check_cuda(launch_gather_records(nullptr, u, urow, ucol, uval, M.row, M.col, M.val,
-                                       as_double, st), "gather");
-    }
-    check_cuda(cudaMemcpyAsync(M.h_block_ptr.data(), M.block_ptr, (nblocks + 1) * 8,
-                               cudaMemcpyDeviceToHost, st), "D2H block_ptr");
-    if (which == DSGDPP_TRAIN) {
-      check_cuda(cudaMemsetAsync(c->cnt1, 0, c->cfg.m * 4, st), "cnt1");
-      check_cuda(cudaMemsetAsync(c->cnt2, 0, c->cfg.n * 4, st), "cnt2");
-      check_cuda(launch_count_nnz12(M.row, M.col, u, c->cnt1, c->cnt2, st), "nnz12");
-      if (c->inv1) {
-        check_cuda(launch_inverse_counts(c->cnt1, c->cfg.m, c->inv1, as_double, st), "inv1");
-        check_cuda(launch_inverse_counts(c->cnt2, c->cfg.n, c->inv2, as_double, st), "inv2");
-      }
-    }
-    check_cuda(cudaStreamSynchronize(st), "sync");
-    M.nnz = u;
-    M.present = true;
-  } catch (...) {
-    cleanup();
-    throw;
+  // Scratch for the blocking: sized for nnz, kept by the context and reused
+  // by later calls (a matrix of the same size allocates nothing).
+  const int end_bit = bit_length((uint64_t)nblocks * span - 1);
+  const int blk_bits = bit_length((uint64_t)nblocks - 1);
+  const int shuffle_bits = 32 + blk_bits;  // (block, 32-bit hash) layout keys
+  size_t sort_bytes = 0, sort2_bytes = 0, scan_bytes = 0;
+  {
+    cub::DoubleBuffer<uint64_t> kb(nullptr, nullptr);
+    cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
+    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, kb, vb, (int)nnz, 0, end_bit,
+                                               st), "sort size");
+    check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, sort2_bytes, kb, vb, (int)nnz, 0,
+                                               shuffle_bits, st), "sort size");
+    check_cuda(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr,
+                                             (uint32_t*)nullptr, (int)nnz, st), "scan size");
   }
-  cleanup();
+  Carver plan;
+  plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz); plan.take<double>(nnz);   // input
+  plan.take<uint64_t>(nnz); plan.take<uint64_t>(nnz);                          // keys
+  plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz);                          // idx
+  plan.take<uint32_t>(nnz);                                                    // pos
+  plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz); plan.take<double>(nnz);  // merged
+  plan.take<unsigned long long>(1);
+  plan.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
+  if (plan.off > c->scratch_bytes) {
+    dfree(c->scratch);
+    c->scratch_bytes = 0;
+    c->scratch = dalloc<char>(plan.off, "blocking scratch");
+    c->scratch_bytes = plan.off;
+  }
+  Carver cv{static_cast<char*>(c->scratch)};
+  uint32_t* t_rows = cv.take<uint32_t>(nnz);
+  uint32_t* t_cols = cv.take<uint32_t>(nnz);
+  double* t_vals = cv.take<double>(nnz);
+  uint64_t* keys[2] = {cv.take<uint64_t>(nnz), cv.take<uint64_t>(nnz)};
+  uint32_t* idx[2] = {cv.take<uint32_t>(nnz), cv.take<uint32_t>(nnz)};
+  uint32_t* pos = cv.take<uint32_t>(nnz);
+  uint32_t* urow = cv.take<uint32_t>(nnz);
+  uint32_t* ucol = cv.take<uint32_t>(nnz);
+  double* uval = cv.take<double>(nnz);
+  unsigned long long* d_bad = cv.take<unsigned long long>(1);
+  void* tmp = cv.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
+
+  check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
+  check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
+  check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+  check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
+  BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
+  check_cuda(launch_make_keys(g, t_rows, t_cols, nnz, keys[0], idx[0], d_bad, st), "make_keys");
+  unsigned long long bad = 0;
+  check_cuda(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st), "D2H");
+  check_cuda(cudaStreamSynchronize(st), "sync");
+  if (bad) throw Error(DSGDPP_E_INVALID, std::to_string(bad) + " entries lie outside the matrix");
+
+  cub::DoubleBuffer<uint64_t> kb(keys[0], keys[1]);
+  cub::DoubleBuffer<uint32_t> vb(idx[0], idx[1]);
+  check_cuda(cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, kb, vb, (int)nnz, 0, end_bit, st),
+             "sort");
+  uint64_t* skeys = kb.Current();
+  uint32_t* sidx = vb.Current();
+  uint64_t* okeys = kb.Alternate();
+  uint32_t* oidx = vb.Alternate();
+
+  // run heads -> output positions (reuse the alternate index buffer)
+  uint32_t* flags = oidx;
+  check_cuda(launch_head_flags(skeys, nnz, flags, st), "head_flags");
+  check_cuda(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, flags, pos, (int)nnz, st), "scan");
+  uint32_t last_pos = 0, last_flag = 0;
+  check_cuda(cudaMemcpyAsync(&last_pos, pos + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
+  check_cuda(cudaMemcpyAsync(&last_flag, flags + nnz - 1, 4, cudaMemcpyDeviceToHost, st), "D2H");
+  check_cuda(cudaStreamSynchronize(st), "sync");
+  const uint64_t u = (uint64_t)last_pos + last_flag;
+
+  check_cuda(launch_merge_runs(g, skeys, sidx, pos, nnz, t_vals, t_rows, t_cols, okeys, urow,
+                               ucol, uval, st), "merge_runs");
+  uint64_t* ukeys = okeys;
+  check_cuda(launch_block_ptr(ukeys, u, span, nblocks, M.block_ptr, st), "block_ptr");
+
+  reserve_records(M, u, as_double);
+  if (shuffled) {
+    // in-block random layout: key = (block, 32-bit hash(layout_seed, k))
+    uint64_t* k2 = skeys;  // free now
+    uint32_t* i2 = sidx;
+    check_cuda(launch_shuffle_keys(ukeys, u, span, c->cfg.layout_seed, k2, i2, st), "shuffle");
+    cub::DoubleBuffer<uint64_t> kb2(k2, ukeys);
+    cub::DoubleBuffer<uint32_t> vb2(i2, flags);
+    check_cuda(cub::DeviceRadixSort::SortPairs(tmp, sort2_bytes, kb2, vb2, (int)u, 0,
+                                               shuffle_bits, st), "sort");
+    check_cuda(launch_gather_records(vb2.Current(), u, urow, ucol, uval, M.row, M.col, M.val,
+                                     as_double, st), "gather");
+  } else {
+    check_cuda(launch_gather_records(nullptr, u, urow, ucol, uval, M.row, M.col, M.val,
+                                     as_double, st), "gather");
+  }
+  check_cuda(cudaMemcpyAsync(M.h_block_ptr.data(), M.block_ptr, (nblocks + 1) * 8,
+                             cudaMemcpyDeviceToHost, st), "D2H block_ptr");
+  if (which == DSGDPP_TRAIN) {
+    check_cuda(cudaMemsetAsync(c->cnt1, 0, c->cfg.m * 4, st), "cnt1");
+    check_cuda(cudaMemsetAsync(c->cnt2, 0, c->cfg.n * 4, st), "cnt2");
+    check_cuda(launch_count_nnz12(M.row, M.col, u, c->cnt1, c->cnt2, st), "nnz12");
+    if (c->inv1) {
+      check_cuda(launch_inverse_counts(c->cnt1, c->cfg.m, c->inv1, as_double, st), "inv1");
+      check_cuda(launch_inverse_counts(c->cnt2, c->cfg.n, c->inv2, as_double, st), "inv2");
+    }
+  }
+  check_cuda(cudaStreamSynchronize(st), "sync");
+  M.nnz = u;
+  M.present = true;
 }
 
 void ensure_staging(dsgdpp_ctx* c) {

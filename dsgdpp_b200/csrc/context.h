@@ -19,6 +19,8 @@ struct DevMatrix {
   uint32_t* col = nullptr;
   void* val = nullptr;
   uint64_t* block_ptr = nullptr;
+  uint32_t nblocks = 0;  // entries of block_ptr minus one
+  uint64_t cap = 0;      // records the row/col/val arrays hold
   std::vector<uint64_t> h_block_ptr;
 };
 
@@ -87,6 +89,8 @@ struct dsgdpp_ctx {
   void* inv1 = nullptr;
   void* inv2 = nullptr;
   double* staging = nullptr;  // (m + n) * r doubles, factor upload / download
+  void* scratch = nullptr;    // blocking scratch of set_matrix, grown on demand
+  size_t scratch_bytes = 0;
   void* W_saved = nullptr;    // factor snapshot (dsgdpp_save_factors)
   void* H_saved = nullptr;
   // per-epoch inputs (pinned host copies feed the device copies)

@@ -91,6 +91,11 @@ cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n
 cudaError_t launch_normalize(int precision, void* W, void* H, uint64_t m, uint64_t n,
                              uint32_t rp, const float* scales, const uint64_t* off2,
                              uint32_t nb2, cudaStream_t st);
+// Batched lazy-L2 normalisation: W row i is multiplied by scales[w_slot[i]],
+// H row j by scales[h_slot[j]]
+cudaError_t launch_scale_rows(int precision, void* W, uint64_t wrows, void* H, uint64_t hrows,
+                              uint32_t rp, const uint32_t* w_slot, const uint32_t* h_slot,
+                              const float* scales, cudaStream_t st);
 
 // Loss partial sums (FP64); `partials` holds `grid` doubles, then sum_partials
 // writes the total to out[0].
@@ -98,6 +103,8 @@ cudaError_t launch_nzsl_partials(int precision, const uint32_t* row, const uint3
                                  const void* val, uint64_t nnz, const void* W, const void* H,
                                  uint32_t r, uint32_t rp, double* partials, uint32_t grid,
                                  cudaStream_t st);
+// CTAs per SM of the training-loss kernel for this precision and row width
+int nzsl_ctas_per_sm(int precision, uint32_t rp);
 cudaError_t launch_sumsq_partials(int precision, const void* X, uint64_t count,
                                   double* partials, uint32_t grid, cudaStream_t st);
 cudaError_t launch_nzl2_partials(int precision, const void* X, uint64_t rows, uint32_t rp,
@@ -105,6 +112,21 @@ cudaError_t launch_nzl2_partials(int precision, const void* X, uint64_t rows, ui
                                  cudaStream_t st);
 cudaError_t launch_sum_partials(const double* partials, uint32_t count, double* out,
                                 cudaStream_t st);
+
+// Per-problem sums of the batched form: one CTA per range chunk writes
+// partials[chunk]; owner_sums adds partials[owner_begin[p] .. owner_begin[p+1])
+// in order into out[p] for p < owners.
+struct RangeChunk {
+  uint64_t begin, end;
+};
+cudaError_t launch_nzsl_chunks(int precision, const RangeChunk* chunks, uint32_t nchunks,
+                               const uint32_t* row, const uint32_t* col, const void* val,
+                               const void* W, const void* H, uint32_t r, uint32_t rp,
+                               double* partials, cudaStream_t st);
+cudaError_t launch_sumsq_chunks(int precision, const RangeChunk* chunks, uint32_t nchunks,
+                                const void* X, double* partials, cudaStream_t st);
+cudaError_t launch_owner_sums(const double* partials, const uint32_t* owner_begin,
+                              uint32_t owners, double* out, cudaStream_t st);
 
 // Sum (out2[0]) and maximum (out2[1]) over rows of |X_i - Xold_i|; partials
 // holds 2 * grid doubles.
@@ -147,6 +169,10 @@ cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t bloc
 cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
                                   const uint32_t* ucol, const double* uval, uint32_t* row,
                                   uint32_t* col, void* val, int val_is_double, cudaStream_t st);
+// rows_out[k] = rows_in[k] + row0, cols_out[k] = cols_in[k] + col0
+cudaError_t launch_offset_copy(const uint32_t* rows_in, const uint32_t* cols_in, uint64_t nnz,
+                               uint32_t row0, uint32_t col0, uint32_t* rows_out,
+                               uint32_t* cols_out, cudaStream_t st);
 cudaError_t launch_count_nnz12(const uint32_t* row, const uint32_t* col, uint64_t nnz,
                                uint32_t* cnt1, uint32_t* cnt2, cudaStream_t st);
 cudaError_t launch_inverse_counts(const uint32_t* cnt, uint64_t len, void* inv,

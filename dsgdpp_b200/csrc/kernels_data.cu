@@ -7,6 +7,8 @@
 // global COO array and are blocked on the GPU: a 64-bit key
 // (block, local row, local column) is radix-sorted stably, runs of equal keys
 // are merged, and block boundaries are found by binary search.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace dsgdpp {
@@ -96,7 +98,7 @@ __global__ void shuffle_keys_kernel(const uint64_t* ukeys, uint64_t u, uint64_t 
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
     const uint64_t blk = ukeys[k] / span;
-    keys2[k] = (blk << 40) | (mix64(seed ^ (k * 0xD6E8FEB86659FD93ull)) >> 24);
+    keys2[k] = (blk << 32) | (mix64(seed ^ (k * 0xD6E8FEB86659FD93ull)) >> 32);
     idx2[k] = (uint32_t)k;
   }
 }
@@ -111,6 +113,16 @@ __global__ void gather_records_kernel(const uint32_t* idx, uint64_t u, const uin
     col[k] = ucol[q];
     if (val_is_double) reinterpret_cast<double*>(val)[k] = uval[q];
     else reinterpret_cast<float*>(val)[k] = (float)uval[q];
+  }
+}
+
+__global__ void offset_copy_kernel(const uint32_t* rows_in, const uint32_t* cols_in, uint64_t nnz,
+                                   uint32_t row0, uint32_t col0, uint32_t* rows_out,
+                                   uint32_t* cols_out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    rows_out[k] = rows_in[k] + row0;
+    cols_out[k] = cols_in[k] + col0;
   }
 }
 
@@ -216,6 +228,16 @@ cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_
   if (u == 0) return cudaSuccess;
   gather_records_kernel<<<kGrid, 256, 0, st>>>(idx, u, urow, ucol, uval, row, col, val,
                                                val_is_double);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_offset_copy(const uint32_t* rows_in, const uint32_t* cols_in, uint64_t nnz,
+                               uint32_t row0, uint32_t col0, uint32_t* rows_out,
+                               uint32_t* cols_out, cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  const uint64_t blocks = std::min<uint64_t>((nnz + 255) / 256, 4096);
+  offset_copy_kernel<<<(unsigned)blocks, 256, 0, st>>>(rows_in, cols_in, nnz, row0, col0,
+                                                       rows_out, cols_out);
   return cudaGetLastError();
 }
 

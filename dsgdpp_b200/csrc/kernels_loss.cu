@@ -2,14 +2,20 @@
 //
 // Reference: nzsl (mf/loss/nzsl.h:29-52), l2 (mf/loss/l2.h:39-48) and nzl2
 // (mf/loss/nzl2.h:29-87), summed over blocks (mf/matrix/op/sum.h:27-30).
-// Every term is formed exactly as the reference forms it (the inner product
-// summed in z order in FP64, no FMA contraction); the terms are then reduced
-// by a fixed two-level tree (per-CTA partials, then one CTA), so the result is
-// deterministic run to run and within a few ulps of any summation order.
+// With FP64 factors every term is formed exactly as the reference forms it
+// (the inner product summed in z order, no FMA contraction).  With FP32/BF16
+// factors a group of lanes shares an entry (coalesced row loads); products of
+// floats are exact in FP64 and only the order of the inner product's additions
+// differs.  Terms are reduced by a fixed two-level tree (per-CTA partials,
+// then one CTA), so every result is deterministic run to run.
 #include "kernels.cuh"
 
 namespace dsgdpp {
 namespace {
+
+inline uint32_t vec_width_of(int precision) {
+  return precision == kFp64 ? 2 : (precision == kFp32 ? 4 : 8);
+}
 
 __device__ __forceinline__ double block_reduce(double v, double* sh) {
 #pragma unroll
@@ -53,6 +59,212 @@ __global__ void __launch_bounds__(256) nzsl_partials_kernel(const uint32_t* row,
   }
   const double t = block_reduce(acc, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// FP32 / BF16 factors: LPN lanes per entry, each lane loading VPL 16-byte
+// vectors of the W row and H column, so a row is one coalesced request.  A
+// warp takes 32 consecutive entries (one index load per lane), then walks
+// them in LPN rounds of 32 / LPN entries, the factor loads of U rounds issued
+// before any is used.  Products of two floats are exact in FP64; each lane
+// sums its elements in z order and the group adds the lane sums by a fixed
+// butterfly.  Entries [begin, end) are dealt to warps warp, warp + nwarps, ...
+template <typename T, int LPN, int VPL>
+__device__ __forceinline__ double nzsl_lanes(const uint32_t* row, const uint32_t* col,
+                                             const float* val, const T* W, const T* H,
+                                             uint32_t r, uint32_t rp, uint64_t begin,
+                                             uint64_t end, uint64_t warp, uint64_t nwarps) {
+  using E = Elem<T>;
+  constexpr int VW = E::VW;
+  constexpr int NG = 32 / LPN;          // entries per round
+  // rounds with loads in flight together (bounded by the registers they hold)
+  constexpr int U = VPL == 1 ? (LPN < 4 ? LPN : 4) : (VPL == 2 ? 2 : 1);
+  const uint32_t lane = threadIdx.x & 31u, grp = lane / LPN, gl = lane % LPN;
+  const uint32_t nvec = rp / VW;
+  double acc = 0;
+  for (uint64_t base = begin + warp * 32; base < end; base += nwarps * 32) {
+    const uint64_t k = base + lane;
+    uint32_t my_row = 0, my_col = 0;
+    float my_val = 0;
+    if (k < end) {
+      my_row = row[k];
+      my_col = col[k];
+      my_val = val[k];
+    }
+    const uint32_t nrec = (uint32_t)min((uint64_t)32, end - base);
+#pragma unroll 1
+    for (uint32_t t0 = 0; t0 < (uint32_t)LPN; t0 += U) {
+      uint4 wv[U][VPL], hv[U][VPL];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint32_t ri = (t0 + u) * NG + grp;
+        const uint32_t rr = __shfl_sync(kFullMask, my_row, ri);
+        const uint32_t cc = __shfl_sync(kFullMask, my_col, ri);
+        const bool valid = ri < nrec;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const uint32_t vi = v * LPN + gl;
+          if (valid && vi < nvec) {
+            wv[u][v] = __ldg(reinterpret_cast<const uint4*>(W + (size_t)rr * rp + vi * VW));
+            hv[u][v] = __ldg(reinterpret_cast<const uint4*>(H + (size_t)cc * rp + vi * VW));
+          } else {
+            wv[u][v] = make_uint4(0, 0, 0, 0);
+            hv[u][v] = make_uint4(0, 0, 0, 0);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint32_t ri = (t0 + u) * NG + grp;
+        double ip = 0;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          float wf[VW], hf[VW];
+          E::unpack(wv[u][v], wf);
+          E::unpack(hv[u][v], hf);
+          const uint32_t z0 = (v * LPN + gl) * VW;
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            // the product of two floats is exact in FP64, so the fused
+            // multiply-add rounds exactly like the separate add
+            if (z0 + e < r) ip = fma((double)wf[e], (double)hf[e], ip);
+        }
+#pragma unroll
+        for (int off = LPN / 2; off > 0; off >>= 1)
+          ip = __dadd_rn(ip, __shfl_xor_sync(kFullMask, ip, off));
+        const float x = __shfl_sync(kFullMask, my_val, ri);
+        if (ri < nrec && gl == 0) {
+          const double diff = __dsub_rn((double)x, ip);
+          acc = __dadd_rn(acc, __dmul_rn(diff, diff));
+        }
+      }
+    }
+  }
+  return acc;
+}
+
+template <typename T, int LPN, int VPL>
+__global__ void __launch_bounds__(256, VPL == 1 ? 3 : 2) nzsl_lanes_kernel(const uint32_t* row, const uint32_t* col,
+                                                         const float* val, uint64_t nnz,
+                                                         const T* W, const T* H, uint32_t r,
+                                                         uint32_t rp, double* partials) {
+  __shared__ double sh[32];
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const double acc = nzsl_lanes<T, LPN, VPL>(row, col, val, W, H, r, rp, 0, nnz, warp, warps);
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// FP64 factors: one thread per entry, the inner product in z order (as the
+// reference forms it) over entries [begin, end) dealt by `stride`.
+__device__ __forceinline__ double nzsl_exact(const uint32_t* row, const uint32_t* col,
+                                             const double* val, const double* W, const double* H,
+                                             uint32_t r, uint32_t rp, uint64_t first,
+                                             uint64_t end, uint64_t stride) {
+  double acc = 0;
+  for (uint64_t k = first; k < end; k += stride) {
+    const double* w = W + (size_t)row[k] * rp;
+    const double* h = H + (size_t)col[k] * rp;
+    double ip = 0;
+    for (uint32_t z = 0; z < r; ++z) ip = __dadd_rn(ip, __dmul_rn(w[z], h[z]));
+    const double diff = __dsub_rn(val[k], ip);
+    acc = __dadd_rn(acc, __dmul_rn(diff, diff));
+  }
+  return acc;
+}
+
+// ---- per-problem (segmented) reductions of the batched form ----------------------
+// One CTA per chunk of a problem's range; owner_sums then adds each problem's
+// chunk partials in chunk order, so every per-problem sum is deterministic.
+template <typename T, int LPN, int VPL>
+__global__ void __launch_bounds__(256, VPL == 1 ? 3 : 2) nzsl_chunks_kernel(const RangeChunk* chunks,
+                                                          const uint32_t* row, const uint32_t* col,
+                                                          const float* val, const T* W,
+                                                          const T* H, uint32_t r, uint32_t rp,
+                                                          double* partials) {
+  __shared__ double sh[32];
+  const RangeChunk c = chunks[blockIdx.x];
+  const double acc = nzsl_lanes<T, LPN, VPL>(row, col, val, W, H, r, rp, c.begin, c.end,
+                                             threadIdx.x >> 5, blockDim.x >> 5);
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+__global__ void __launch_bounds__(256) nzsl_chunks_exact_kernel(
+    const RangeChunk* chunks, const uint32_t* row, const uint32_t* col, const double* val,
+    const double* W, const double* H, uint32_t r, uint32_t rp, double* partials) {
+  __shared__ double sh[32];
+  const RangeChunk c = chunks[blockIdx.x];
+  const double acc =
+      nzsl_exact(row, col, val, W, H, r, rp, c.begin + threadIdx.x, c.end, blockDim.x);
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+template <typename T>
+__global__ void __launch_bounds__(256) sumsq_chunks_kernel(const RangeChunk* chunks, const T* X,
+                                                           double* partials) {
+  __shared__ double sh[32];
+  const RangeChunk c = chunks[blockIdx.x];
+  double acc = 0;
+  for (uint64_t k = c.begin + threadIdx.x; k < c.end; k += blockDim.x) {
+    const double v = (double)(float)X[k];
+    acc = __dadd_rn(acc, __dmul_rn(v, v));
+  }
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+template <>
+__global__ void __launch_bounds__(256) sumsq_chunks_kernel<double>(const RangeChunk* chunks,
+                                                                   const double* X,
+                                                                   double* partials) {
+  __shared__ double sh[32];
+  const RangeChunk c = chunks[blockIdx.x];
+  double acc = 0;
+  for (uint64_t k = c.begin + threadIdx.x; k < c.end; k += blockDim.x)
+    acc = __dadd_rn(acc, __dmul_rn(X[k], X[k]));
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+__global__ void __launch_bounds__(256) owner_sums_kernel(const double* partials,
+                                                         const uint32_t* owner_begin,
+                                                         double* out) {
+  __shared__ double sh[32];
+  const uint32_t p = blockIdx.x;
+  double acc = 0;
+  for (uint32_t k = owner_begin[p] + threadIdx.x; k < owner_begin[p + 1]; k += blockDim.x)
+    acc = __dadd_rn(acc, partials[k]);
+  const double t = block_reduce(acc, sh);
+  if (threadIdx.x == 0) out[p] = t;
+}
+
+// lane mapping of the FP32 / BF16 loss kernels: LPN = the power of two
+// covering the row's vectors (at most 32), VPL = vectors per lane
+struct LossShape {
+  uint32_t lanes, vecs;
+};
+LossShape loss_shape(uint32_t nvec) {
+  LossShape s{2, 1};
+  while (s.lanes < nvec && s.lanes < 32) s.lanes <<= 1;
+  s.vecs = (nvec + s.lanes - 1) / s.lanes;
+  if (s.vecs == 3) s.vecs = 4;
+  return s;
+}
+
+template <typename T>
+void* nzsl_lanes_fn(LossShape s, bool chunks) {
+#define DSGDPP_CASE(L, V)                                                            \
+  if (s.lanes == L && s.vecs == V)                                                   \
+    return chunks ? reinterpret_cast<void*>(&nzsl_chunks_kernel<T, L, V>)            \
+                  : reinterpret_cast<void*>(&nzsl_lanes_kernel<T, L, V>);
+  DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
+  DSGDPP_CASE(32, 2) DSGDPP_CASE(32, 4)
+#undef DSGDPP_CASE
+  return nullptr;
+}
+
+void* nzsl_fn(int precision, uint32_t rp, bool chunks) {
+  const LossShape s = loss_shape(rp / vec_width_of(precision));
+  return precision == kFp32 ? nzsl_lanes_fn<float>(s, chunks)
+                            : nzsl_lanes_fn<__nv_bfloat16>(s, chunks);
 }
 
 template <typename T>
@@ -120,16 +332,61 @@ cudaError_t launch_nzsl_partials(int precision, const uint32_t* row, const uint3
                                  const void* val, uint64_t nnz, const void* W, const void* H,
                                  uint32_t r, uint32_t rp, double* partials, uint32_t grid,
                                  cudaStream_t st) {
-  if (precision == kFp64)
+  if (precision == kFp64) {
     nzsl_partials_kernel<double, double><<<grid, 256, 0, st>>>(
         row, col, (const double*)val, nnz, (const double*)W, (const double*)H, r, rp, partials);
+    return cudaGetLastError();
+  }
+  void* fn = nzsl_fn(precision, rp, false);
+  if (!fn) return cudaErrorInvalidValue;
+  const float* v = static_cast<const float*>(val);
+  void* params[] = {&row, &col, &v, &nnz, &W, &H, &r, &rp, &partials};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, 0, st);
+}
+
+int nzsl_ctas_per_sm(int precision, uint32_t rp) {
+  void* fn = precision == kFp64 ? reinterpret_cast<void*>(&nzsl_partials_kernel<double, double>)
+                                : nzsl_fn(precision, rp, false);
+  int n = 0;
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, 0) != cudaSuccess) return 0;
+  return n;
+}
+
+cudaError_t launch_nzsl_chunks(int precision, const RangeChunk* chunks, uint32_t nchunks,
+                               const uint32_t* row, const uint32_t* col, const void* val,
+                               const void* W, const void* H, uint32_t r, uint32_t rp,
+                               double* partials, cudaStream_t st) {
+  if (nchunks == 0) return cudaSuccess;
+  if (precision == kFp64) {
+    nzsl_chunks_exact_kernel<<<nchunks, 256, 0, st>>>(chunks, row, col, (const double*)val,
+                                                      (const double*)W, (const double*)H, r, rp,
+                                                      partials);
+    return cudaGetLastError();
+  }
+  void* fn = nzsl_fn(precision, rp, true);
+  if (!fn) return cudaErrorInvalidValue;
+  const float* v = static_cast<const float*>(val);
+  void* params[] = {&chunks, &row, &col, &v, &W, &H, &r, &rp, &partials};
+  return cudaLaunchKernel(fn, dim3(nchunks), dim3(256), params, 0, st);
+}
+
+cudaError_t launch_sumsq_chunks(int precision, const RangeChunk* chunks, uint32_t nchunks,
+                                const void* X, double* partials, cudaStream_t st) {
+  if (nchunks == 0) return cudaSuccess;
+  if (precision == kFp64)
+    sumsq_chunks_kernel<double><<<nchunks, 256, 0, st>>>(chunks, (const double*)X, partials);
   else if (precision == kFp32)
-    nzsl_partials_kernel<float, float><<<grid, 256, 0, st>>>(
-        row, col, (const float*)val, nnz, (const float*)W, (const float*)H, r, rp, partials);
+    sumsq_chunks_kernel<float><<<nchunks, 256, 0, st>>>(chunks, (const float*)X, partials);
   else
-    nzsl_partials_kernel<__nv_bfloat16, float><<<grid, 256, 0, st>>>(
-        row, col, (const float*)val, nnz, (const __nv_bfloat16*)W, (const __nv_bfloat16*)H, r,
-        rp, partials);
+    sumsq_chunks_kernel<__nv_bfloat16><<<nchunks, 256, 0, st>>>(
+        chunks, (const __nv_bfloat16*)X, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_owner_sums(const double* partials, const uint32_t* owner_begin,
+                              uint32_t owners, double* out, cudaStream_t st) {
+  if (owners == 0) return cudaSuccess;
+  owner_sums_kernel<<<owners, 256, 0, st>>>(partials, owner_begin, out);
   return cudaGetLastError();
 }
 

@@ -473,6 +473,26 @@ __global__ void normalize_kernel<double>(double* W, double* H, uint64_t m, uint6
   }
 }
 
+template <typename T>
+__global__ void scale_rows_kernel(T* W, uint64_t wrows, T* H, uint64_t hrows, uint32_t rp,
+                                  const uint32_t* w_slot, const uint32_t* h_slot,
+                                  const float* scales) {
+  const uint64_t wtot = wrows * rp, tot = wtot + hrows * rp;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < tot; q += stride) {
+    if (q < wtot) {
+      const float s = scales[w_slot[q / rp]];
+      if constexpr (sizeof(T) == 8) W[q] *= (double)s;
+      else W[q] = (T)((float)W[q] * s);
+    } else {
+      const uint64_t hq = q - wtot;
+      const float s = scales[h_slot[hq / rp]];
+      if constexpr (sizeof(T) == 8) H[hq] *= (double)s;
+      else H[hq] = (T)((float)H[hq] * s);
+    }
+  }
+}
+
 template <typename T, int LPN, int VPL>
 void* hogwild_fn(bool atomic, bool smem) {
   if (smem)
@@ -559,6 +579,21 @@ cudaError_t launch_normalize(int precision, void* W, void* H, uint64_t m, uint64
   else
     normalize_kernel<__nv_bfloat16><<<1184, 256, 0, st>>>(
         (__nv_bfloat16*)W, (__nv_bfloat16*)H, m, n, rp, scales, off2, nb2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_rows(int precision, void* W, uint64_t wrows, void* H, uint64_t hrows,
+                              uint32_t rp, const uint32_t* w_slot, const uint32_t* h_slot,
+                              const float* scales, cudaStream_t st) {
+  if (precision == kFp64)
+    scale_rows_kernel<double><<<1184, 256, 0, st>>>((double*)W, wrows, (double*)H, hrows, rp,
+                                                    w_slot, h_slot, scales);
+  else if (precision == kFp32)
+    scale_rows_kernel<float><<<1184, 256, 0, st>>>((float*)W, wrows, (float*)H, hrows, rp,
+                                                   w_slot, h_slot, scales);
+  else
+    scale_rows_kernel<__nv_bfloat16><<<1184, 256, 0, st>>>(
+        (__nv_bfloat16*)W, wrows, (__nv_bfloat16*)H, hrows, rp, w_slot, h_slot, scales);
   return cudaGetLastError();
 }
 

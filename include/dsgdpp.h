@@ -265,6 +265,47 @@ int dsgdpp_autotune(const dsgdpp_config* base, uint64_t nnz, const uint32_t* row
                     const uint32_t* d_candidates, uint32_t nd, uint32_t epochs, double eps,
                     dsgdpp_config* best, double* best_ms);
 
+/* ---- batched form: many independent factorizations ----------------------- */
+/* No reference counterpart (the reference runs one factorization per job).
+ * Problems are grouped by padded rank; one epoch of every problem is one
+ * sequence of Hogwild launches, launch s of a group covering sub-epoch s of
+ * all its problems (captured once as a CUDA graph under DSGDPP_LAUNCH_GRAPH).
+ * Step sizes follow BoldDriver per problem on per-problem training losses. */
+typedef struct dsgdpp_batch dsgdpp_batch;
+typedef struct dsgdpp_problem {
+  uint64_t m, n;       /* rows, columns */
+  uint32_t rank;
+  uint32_t d;          /* 0: chosen from the problem's size (at most 16) */
+  uint64_t nnz;        /* training entries (0-based COO, duplicates summed) */
+  const uint32_t* rows;
+  const uint32_t* cols;
+  const double* vals;
+  uint64_t nnz_test;   /* test entries (may be 0) */
+  const uint32_t* trows;
+  const uint32_t* tcols;
+  const double* tvals;
+  const double* W;     /* m x rank row-major initial factors */
+  const double* H;     /* n x rank row-major (row j = column j of H) */
+  uint32_t seed;       /* master generator seed (dsgdpp_seed) */
+  double eps0;         /* first step size */
+} dsgdpp_problem;
+/* `common` supplies precision, update/regularize/loss functions and their
+ * lambdas, stratum and SGD orders, device, launch mode, write mode and the
+ * lane mapping (0 = per group); its m, n, rank and d are ignored.  Only the
+ * Hogwild path without truncation is batched (DSGDPP_E_UNSUPPORTED else). */
+int dsgdpp_batch_create(const dsgdpp_config* common, uint32_t count,
+                        const dsgdpp_problem* problems, dsgdpp_batch** out);
+void dsgdpp_batch_destroy(dsgdpp_batch* b);
+const char* dsgdpp_batch_last_error(const dsgdpp_batch* b);
+/* Runs `epochs` epochs of every problem (BoldDriver per problem from eps0 as
+ * dsgdpp_run, training loss after every epoch, test loss after the last).
+ * train/test get one value per problem (may be NULL); *epoch_ms the summed
+ * device time of the epochs' launches. */
+int dsgdpp_batch_run(dsgdpp_batch* b, uint32_t epochs, double decrease, double increase,
+                     double* train, double* test, double* epoch_ms);
+int dsgdpp_batch_problem_d(dsgdpp_batch* b, uint32_t p, uint32_t* d);
+int dsgdpp_batch_get_factors(dsgdpp_batch* b, uint32_t p, double* W, double* H);
+
 /* ---- host utilities (no GPU needed) --------------------------------------- */
 /* rg::Random32 as pinned by this library (MT19937, Boost bucket nextInt). */
 typedef struct dsgdpp_rng dsgdpp_rng;
