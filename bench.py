@@ -136,15 +136,19 @@ def algorithmic_bytes_per_update(r, precision, update):
     return 12 + 4 * r * s_f + (8 if update == "Nzsl_L2" else 0)
 
 
-def traffic_per_launch(name):
-    """DRAM bytes per launch of the Hogwild kernel from the committed ncu summary."""
+def traffic_per_launch(name, d):
+    """DRAM bytes per launch of the Hogwild kernel from the committed ncu summary
+    (None unless the summary was taken at the same d)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
     except OSError:
         return None
     m = re.search(r"dram_bytes_per_launch_scaled:\s*([0-9.eE+]+)", text)
-    return float(m.group(1)) if m else None
+    md = re.search(r"profiled_d:\s*([0-9]+)", text)
+    if not m or not md or int(md.group(1)) != d:
+        return None
+    return float(m.group(1))
 
 
 def cpu_sample(data, count, seed=1):
@@ -154,12 +158,17 @@ def cpu_sample(data, count, seed=1):
     return data["rows"][:k], data["cols"][:k], data["vals"][:k]
 
 
-def time_cpu_reference(data, wl, steps, warmup, threads=None):
-    """The oracle's threaded epoch (one thread per task, d = threads) on a sample."""
+def time_cpu_reference(data, wl, steps, warmup, threads=None, with_test=False):
+    """The oracle's threaded epoch (one thread per task, d = threads) on a sample;
+    with_test also gives the sample run's final FP64 test RMSE."""
     from oracle import oracle as O
     threads = threads or os.cpu_count() or 1
     rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
-    prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals)
+    if with_test:
+        prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals,
+                         data["trows"], data["tcols"], data["tvals"])
+    else:
+        prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals)
     prob.configure(update="Nzsl_L2", update_lambda=1.0,
                    regularize="L2" if wl["s"] is not None else "None",
                    regularize_lambda=0.05, loss="Nzsl_L2", loss_lambda=1.0)
@@ -171,10 +180,34 @@ def time_cpu_reference(data, wl, steps, warmup, threads=None):
         if e >= warmup:
             times.append(ns * 1e-9)
     t = statistics.median(times)
-    return dict(value=len(vals) / t, unit="updates/s", cores=threads, kind="port",
-                sample=f"{len(vals):,} training entries of the workload (prefix of the random-order "
-                       f"entries), FP64, d={threads} tasks x {2 * threads} column blocks, "
-                       f"median of {steps} epochs", epoch_s=t)
+    out = dict(value=len(vals) / t, unit="updates/s", cores=threads, kind="port",
+               sample=f"{len(vals):,} training entries of the workload (prefix of the random-order "
+                      f"entries), FP64, d={threads} tasks x {2 * threads} column blocks, "
+                      f"median of {steps} epochs", epoch_s=t)
+    if with_test:
+        out["test_rmse"] = float(np.sqrt(prob.nzsl(1) / len(data["tvals"])))
+        out["epochs"] = warmup + steps
+        out["d"] = threads
+    return out
+
+
+def gpu_sample_rmse(P, data, wl, precision, d, epochs, write_mode, device):
+    """Test RMSE of this implementation on the CPU baseline's sample, same d,
+    seed and constant step as the oracle run."""
+    rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
+    l2 = wl["s"] is not None
+    cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=precision,
+                   update="Nzsl_L2", update_lambda=1.0, regularize="L2" if l2 else "None",
+                   regularize_lambda=0.05 if l2 else 0.0, loss="Nzsl_L2", loss_lambda=1.0,
+                   write_mode=write_mode, device=device)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, rows, cols, vals)
+        ctx.set_matrix(P.TEST, data["trows"], data["tcols"], data["tvals"])
+        ctx.set_factors(data["W0"], data["H0"])
+        ctx.seed(1)
+        for _ in range(epochs):
+            ctx.epoch(0.001)
+        return float(np.sqrt(ctx.nzsl(P.TEST) / len(data["tvals"])))
 
 
 def generate(wl, seed):
@@ -341,7 +374,8 @@ def main():
     avg_launch_s = k_ms / 1e3 / max(k_launches, 1)
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
-    traffic = traffic_per_launch(f"hogwild_subepoch_{args.workload}.md")
+    suffix = "" if args.precision == "fp32" else "_" + args.precision
+    traffic = traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", d)
 
     # ---- end to end through the C ABI from pinned host buffers ----
     e2e = None
@@ -374,9 +408,16 @@ def main():
                "final_test_rmse": float(np.sqrt(losses[-1][1] / len(host["tvals"])))}
 
     cpu = None
+    vs_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = time_cpu_reference(data, wl, steps=2, warmup=0)
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        ref = time_cpu_reference(data, wl, steps=2, warmup=0, with_test=True)
+        cpu = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # the same sample, d, seed and steps on the GPU: test RMSE against the FP64 oracle
+        got = gpu_sample_rmse(P, data, wl, args.precision, ref["d"], ref["epochs"],
+                              args.write_mode, local)
+        vs_oracle = {"precision": args.precision, "epochs": ref["epochs"], "d": ref["d"],
+                     "sample": "the CPU baseline's sample", "oracle_fp64_test_rmse": ref["test_rmse"],
+                     "test_rmse": got, "rel_error": (got - ref["test_rmse"]) / ref["test_rmse"]}
 
     ctx.close()
     if rank == 0:
@@ -398,6 +439,7 @@ def main():
                          "bytes_per_update": bpu, "kernel": "hogwild_subepoch_kernel",
                          "avg_launch_us": avg_launch_s * 1e6},
             "cpu_baseline": cpu,
+            "test_rmse_vs_fp64_oracle": vs_oracle,
             "e2e": e2e,
             "gpu_launches": args.steps * (2 * d + 1 + (1 if l2 else 0)),
             "clocks": clk,

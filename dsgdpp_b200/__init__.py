@@ -144,6 +144,8 @@ SIGNATURES = {
     "dsgdpp_batch_last_error": (C.c_char_p, [_P]),
     "dsgdpp_batch_run": (C.c_int, [_P, C.c_uint32, C.c_double, C.c_double, _f64p, _f64p,
                                    _f64p]),
+    "dsgdpp_batch_autotune": (C.c_int, [C.POINTER(_Config), C.c_uint32, C.POINTER(_Problem),
+                                        C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p]),
     "dsgdpp_batch_problem_d": (C.c_int, [_P, C.c_uint32, _u32p]),
     "dsgdpp_batch_get_factors": (C.c_int, [_P, C.c_uint32, _f64p, _f64p]),
     "dsgdpp_rng_create": (_P, [C.c_uint32]),
@@ -407,6 +409,31 @@ class Context:
                      time_test_loss=r.time_test_loss) for r in rows]
 
 
+def _problem_array(problems):
+    """ctypes array of dsgdpp_problem, and the numpy arrays it points into."""
+    arr = (_Problem * len(problems))()
+    keep = []
+    for k, p in enumerate(problems):
+        q = arr[k]
+        q.m, q.n, q.rank, q.d = p["m"], p["n"], p["rank"], p.get("d", 0)
+        rows, cols, vals = _u32(p["rows"]), _u32(p["cols"]), _f64(p["vals"])
+        W, H = _f64(p["W"]), _f64(p["H"])
+        q.nnz = len(vals)
+        q.rows, q.cols = _ptr(rows, C.c_uint32), _ptr(cols, C.c_uint32)
+        q.vals = _ptr(vals, C.c_double)
+        q.W, q.H = _ptr(W, C.c_double), _ptr(H, C.c_double)
+        keep += [rows, cols, vals, W, H]
+        if p.get("tvals") is not None and len(p["tvals"]):
+            tr, tc, tv = _u32(p["trows"]), _u32(p["tcols"]), _f64(p["tvals"])
+            q.nnz_test = len(tv)
+            q.trows, q.tcols = _ptr(tr, C.c_uint32), _ptr(tc, C.c_uint32)
+            q.tvals = _ptr(tv, C.c_double)
+            keep += [tr, tc, tv]
+        q.seed = p.get("seed", 0)
+        q.eps0 = p.get("eps0", 0.001)
+    return arr, keep
+
+
 class Batch:
     """Many independent factorizations advanced together (dsgdpp_batch_*).
 
@@ -419,27 +446,7 @@ class Batch:
     def __init__(self, config: Config, problems):
         self.config = config
         self._cfg = config.to_c()
-        self._keep = []
-        arr = (_Problem * len(problems))()
-        for k, p in enumerate(problems):
-            q = arr[k]
-            q.m, q.n, q.rank, q.d = p["m"], p["n"], p["rank"], p.get("d", 0)
-            rows, cols, vals = _u32(p["rows"]), _u32(p["cols"]), _f64(p["vals"])
-            W, H = _f64(p["W"]), _f64(p["H"])
-            q.nnz = len(vals)
-            q.rows, q.cols = _ptr(rows, C.c_uint32), _ptr(cols, C.c_uint32)
-            q.vals = _ptr(vals, C.c_double)
-            q.W, q.H = _ptr(W, C.c_double), _ptr(H, C.c_double)
-            keep = [rows, cols, vals, W, H]
-            if p.get("tvals") is not None and len(p["tvals"]):
-                tr, tc, tv = _u32(p["trows"]), _u32(p["tcols"]), _f64(p["tvals"])
-                q.nnz_test = len(tv)
-                q.trows, q.tcols = _ptr(tr, C.c_uint32), _ptr(tc, C.c_uint32)
-                q.tvals = _ptr(tv, C.c_double)
-                keep += [tr, tc, tv]
-            q.seed = p.get("seed", 0)
-            q.eps0 = p.get("eps0", 0.001)
-            self._keep.append(keep)
+        arr, self._keep = _problem_array(problems)
         self.count = len(problems)
         self.shapes = [(p["m"], p["n"], p["rank"]) for p in problems]
         h = _P()
@@ -448,6 +455,21 @@ class Batch:
         if rc != OK:
             raise DsgdppError(rc, "dsgdpp_batch_create failed (details on stderr)")
         self._h = h
+
+    @staticmethod
+    def autotune(config: Config, problems, sample_stride: int = 8, epochs: int = 2):
+        """The batched autotuner: (per-problem d list, CTAs per SM, sample epoch ms)."""
+        arr, keep = _problem_array(problems)
+        d = np.zeros(len(problems), np.uint32)
+        ctas = C.c_uint32()
+        ms = C.c_double()
+        cfg = config.to_c()
+        rc = lib.dsgdpp_batch_autotune(C.byref(cfg), len(problems), arr, sample_stride, epochs,
+                                       _ptr(d, C.c_uint32), C.byref(ctas), C.byref(ms))
+        del keep
+        if rc != OK:
+            raise DsgdppError(rc, "dsgdpp_batch_autotune failed (details on stderr)")
+        return [int(v) for v in d], ctas.value, ms.value
 
     def _check(self, rc, what):
         if rc != OK:

@@ -9,9 +9,12 @@ entries.  FP32 factors, Nzsl_L2(1) update, L2(0.02) regularize, BoldDriver per
 problem from eps 0.001, `epochs` epochs each.
 
 Both arms report aggregate updates/s = (sum of training entries) x epochs /
-device time of the epochs.  The batched arm runs every problem's epoch as one
-graph of launches (dsgdpp_batch_run); the looped arm runs each problem in
-its own context (dsgdpp_run) one after another with the same d.
+time.  The batched arm runs every problem's epoch as one graph of launches
+(dsgdpp_batch_run) with d and CTAs per SM from the batched autotuner
+(dsgdpp_batch_autotune, timed on every 8th problem); the looped arm runs each
+problem in its own context (dsgdpp_run) one after another with the same d.
+`speedup_wall` compares wall time of the whole runs (epochs, per-epoch
+losses and step decisions).
 
     python -m dsgdpp_b200.batchbench --count 256 --epochs 30
 """
@@ -68,6 +71,8 @@ def main():
                     help="problems timed in the looped arm (-1: all); the looped rate is "
                          "taken over those problems")
     ap.add_argument("--launch", default="graph")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in d rule (cap 16) and the occupancy CTA count")
     args = ap.parse_args()
 
     dev = f"cuda:{torch.cuda.current_device()}"
@@ -85,6 +90,14 @@ def main():
                        f"problem, {args.epochs} epochs",
            "problems": args.count, "entries": int(total), "generate_s": gen_s}
 
+    if not args.no_autotune:
+        t0 = time.time()
+        ds, ctas, ms = P.Batch.autotune(cfg, probs, sample_stride=8, epochs=2)
+        for p, d in zip(probs, ds):
+            p["d"] = d
+        cfg.ctas_per_sm = ctas
+        out["autotune"] = {"seconds": time.time() - t0, "ctas_per_sm": ctas,
+                           "sample_epoch_ms": ms, "sample": "every 8th problem"}
     t0 = time.time()
     b = P.Batch(cfg, probs)
     out["batch_setup_s"] = time.time() - t0

@@ -6,11 +6,14 @@ fallback whenever a proposed step raises the training loss
 (csrc/controller.cc, ``Context.run_controlled``).
 
 Traces are epochs of the method itself on matrices of the 100M-entry
-workload's family (Zipf row/column weights) with varied rank, noise and
-density.  At each recorded state the factors are saved on the device and
-every candidate log multiplier is tried from the same state; the label is the
-candidate with the lowest training loss after the epoch.  The run then moves
-on by a behaviour policy: BoldDriver's rule or a random multiplier.
+workload's family (Zipf row/column weights) with varied rank, noise, density
+and L2 regularisation.  At each recorded state the factors are saved on the
+device and every candidate log multiplier is tried from the same state for
+`horizon` epochs at that step; the label is the candidate with the lowest
+training loss at the end.  The run then moves on by a behaviour policy:
+BoldDriver's rule, a random multiplier, or a trained network with the
+BoldDriver fallback (so later training rounds see the states the controller
+itself visits, as in DAgger: Ross, Gordon, Bagnell, AISTATS 2011).
 """
 from __future__ import annotations
 
@@ -33,15 +36,18 @@ def family_problem(rng, device=0):
     nnz = int(min(6_000_000, density * m * n))
     r = int(rng.choice([8, 16, 32, 64, 128]))
     noise = float(rng.uniform(0.05, 0.5))
+    l2 = float(rng.choice([0.0, 0.02, 0.05]))
     data = synth_gpu.make(m, n, nnz, max(1000, nnz // 50), rank_true=r, r=r, noise=noise,
                           seed=int(rng.integers(1 << 30)), s_row=1.1, s_col=1.1,
                           device=f"cuda:{device}")
-    return dict(m=m, n=n, r=r, noise=noise, nnz=nnz, data=data)
+    return dict(m=m, n=n, r=r, noise=noise, nnz=nnz, l2=l2, data=data)
 
 
 def _context(prob, precision="fp32", d=16, device=0):
+    l2 = prob.get("l2", 0.0)
     ctx = Context(Config(m=prob["m"], n=prob["n"], rank=prob["r"], d=d, precision=precision,
-                         device=device))
+                         device=device, regularize="L2" if l2 else "None",
+                         regularize_lambda=l2))
     dd = prob["data"]
     ctx.set_matrix(TRAIN, dd["rows"], dd["cols"], dd["vals"])
     ctx.set_matrix(TEST, dd["trows"], dd["tcols"], dd["tvals"])
@@ -49,41 +55,97 @@ def _context(prob, precision="fp32", d=16, device=0):
     return ctx
 
 
-def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print):
-    """(features [count, 16], labels [count]) from the method's own epochs."""
+KEEP_RISE = 0.01  # as kKeepRise in csrc/controller.cc
+MAX_HALVINGS = 8
+
+
+def controlled_step(ctx, net, f, eps, prev_loss, decrease=0.5):
+    """One epoch under the controller with the BoldDriver fallback, exactly as
+    dsgdpp_run_controlled takes it; returns (training loss, next step)."""
+    m = float(net.forward(f[None, :])[0])
+    proposed = eps * math.exp(m)
+    ctx.save_factors()
+    ctx.epoch(proposed)
+    cur = ctx.loss()
+    if cur <= prev_loss:
+        return cur, proposed
+    if cur <= prev_loss * (1.0 + KEEP_RISE):
+        return cur, proposed * decrease
+    step = eps
+    for _ in range(MAX_HALVINGS):
+        step *= decrease
+        ctx.restore_factors()
+        ctx.epoch(step)
+        cur = ctx.loss()
+        if cur <= prev_loss:
+            break
+    return cur, step
+
+
+def label_states(first, last, prev):
+    """Labels from the candidates' lookahead losses: the candidate with the
+    lowest loss after the lookahead among those whose first epoch did not raise
+    the training loss (a proposal that raises it triggers the fallback); the
+    smallest multiplier when every candidate raised it.  first, last:
+    [states, candidates]; prev: [states]."""
+    ok = np.isfinite(last) & (first <= prev[:, None])
+    score = np.where(ok, last, np.inf)
+    idx = np.argmin(score, axis=1)
+    idx[~ok.any(axis=1)] = 0
+    return CANDIDATES[idx].astype(np.float32)
+
+
+def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None, horizon=2,
+                    policies=("bold", "random"), details=False):
+    """(features [count, 16], labels [count]) from the method's own epochs;
+    with details also the lookahead losses (first, last [count, candidates])
+    and the state's training loss (prev [count]) that the labels come from.
+
+    Each run follows one behaviour policy drawn from `policies`: "bold"
+    (BoldDriver), "random" (a random candidate multiplier) or "net" (`net`
+    proposing, with the fallback of dsgdpp_run_controlled)."""
     rng = np.random.default_rng(seed)
-    X, y = [], []
+    X, F1, FL, PV = [], [], [], []
     t0 = time.time()
     while len(X) < count:
         prob = family_problem(rng, device)
+        policy = str(rng.choice(list(policies)))
         with _context(prob, device=device) as ctx:
             ctx.seed(int(rng.integers(1 << 31)))
             eps = float(math.exp(rng.uniform(math.log(3e-4), math.log(3e-3))))
-            bold = rng.random() < 0.5  # behaviour policy of this run
             tr, te = [ctx.loss()], [ctx.nzsl(TEST)]
             upd, last_m = (0.0, 0.0), 0.0
             for e in range(epochs):
                 f = controller_features(tr[::-1][:5], te[::-1][:5], eps, upd[0], upd[1],
                                         e / epochs, last_m)
                 ctx.save_factors()
-                losses = []
+                first, last = [], []
                 for c in CANDIDATES:
                     ctx.restore_factors()
                     ctx.epoch(eps * math.exp(c))
-                    losses.append(ctx.loss())
-                losses = np.array(losses)
-                if np.all(~np.isfinite(losses)) or not np.all(np.isfinite(f)):
+                    first.append(ctx.loss())
+                    for _ in range(horizon - 1):
+                        ctx.epoch(eps * math.exp(c))
+                    last.append(ctx.loss())
+                first, last = np.array(first), np.array(last)
+                if np.all(~np.isfinite(last)) or not np.all(np.isfinite(f)):
                     break
-                losses[~np.isfinite(losses)] = np.inf
+                first[~np.isfinite(first)] = np.inf
+                last[~np.isfinite(last)] = np.inf
                 X.append(f)
-                y.append(float(CANDIDATES[int(np.argmin(losses))]))
+                F1.append(first)
+                FL.append(last)
+                PV.append(tr[-1])
                 # advance by the behaviour policy from the saved state
                 ctx.restore_factors()
-                if bold:
+                if policy == "bold":
                     ctx.epoch(eps)
                     cur = ctx.loss()
                     used_m = 0.0
                     nxt = eps * (0.5 if tr[-1] <= cur else 1.05)
+                elif policy == "net":
+                    cur, nxt = controlled_step(ctx, net, f, eps, tr[-1])
+                    used_m = math.log(nxt / eps)
                 else:
                     used_m = float(rng.choice(CANDIDATES))
                     ctx.epoch(eps * math.exp(used_m))
@@ -98,9 +160,15 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print):
                     break
                 if not math.isfinite(cur) or cur > 4.0 * tr[0]:
                     break  # the behaviour policy diverged: later states are not useful
-        log(f"traces {len(X)}/{count} (m={prob['m']} n={prob['n']} r={prob['r']} "
-            f"nnz={prob['nnz']} noise={prob['noise']:.2f}) {time.time() - t0:.0f}s")
-    return np.array(X, np.float32), np.array(y, np.float32)
+        log(f"traces {len(X)}/{count} ({policy}; m={prob['m']} n={prob['n']} r={prob['r']} "
+            f"nnz={prob['nnz']} l2={prob['l2']} noise={prob['noise']:.2f}) "
+            f"{time.time() - t0:.0f}s")
+    X = np.array(X, np.float32)
+    F1, FL, PV = np.array(F1), np.array(FL), np.array(PV)
+    y = label_states(F1, FL, PV)
+    if details:
+        return X, y, F1, FL, PV
+    return X, y
 
 
 def train(X, y, steps=3000, batch=256, lr=1e-3, seed=0, device=0, val_frac=0.1):
@@ -129,3 +197,51 @@ def time_to_target(trace, target_test_loss):
         if row["test_loss"] <= target_test_loss:
             return int(row["epoch"]), elapsed
     return None, elapsed
+
+
+def train_dagger(rounds=2, first=2000, per_round=1500, epochs=25, horizon=2, device=0,
+                 log=print):
+    """Round 0: traces under BoldDriver / random multipliers; each later round
+    adds traces under the current network (with the fallback) and retrains on
+    everything gathered.  Returns (net, data dict with X, y and the lookahead
+    losses, per-round (train, val) losses)."""
+    quiet = lambda s: None
+    X, y, F1, FL, PV = generate_traces(first, epochs=epochs, seed=0, device=device,
+                                       horizon=horizon, policies=("bold", "random"), log=quiet,
+                                       details=True)
+    net, tl, vl = train(X, y, steps=4000, seed=0, device=device)
+    hist = [(tl, vl)]
+    log(f"round 0: {len(X)} states, labels {np.unique(y, return_counts=True)}, "
+        f"train {tl:.4f} val {vl:.4f}")
+    for rnd in range(1, rounds + 1):
+        X1, y1, F11, FL1, PV1 = generate_traces(per_round, epochs=epochs, seed=100 + rnd,
+                                                device=device, horizon=horizon, net=net,
+                                                policies=("net", "net", "bold"), log=quiet,
+                                                details=True)
+        X, y = np.concatenate([X, X1]), np.concatenate([y, y1])
+        F1, FL, PV = np.concatenate([F1, F11]), np.concatenate([FL, FL1]), np.concatenate([PV, PV1])
+        net, tl, vl = train(X, y, steps=6000, seed=rnd, device=device)
+        hist.append((tl, vl))
+        log(f"round {rnd}: {len(X)} states, labels {np.unique(y1, return_counts=True)}, "
+            f"train {tl:.4f} val {vl:.4f}")
+    return net, dict(X=X, y=y, first=F1, last=FL, prev=PV), hist
+
+
+def main():
+    import argparse
+    import os
+    ap = argparse.ArgumentParser(description="train the step-size controller (DAgger rounds)")
+    ap.add_argument("--rounds", type=int, default=2)
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                                  "controller_params.npy"))
+    ap.add_argument("--traces", default=None, help="also save the (X, y) states here (.npz)")
+    args = ap.parse_args()
+    net, data, _ = train_dagger(rounds=args.rounds)
+    np.save(args.out, net.params)
+    if args.traces:
+        np.savez(args.traces, **data)
+
+
+if __name__ == "__main__":
+    main()
+

@@ -630,6 +630,54 @@ int dsgdpp_batch_run(dsgdpp_batch* b, uint32_t epochs, double decrease, double i
   });
 }
 
+int dsgdpp_batch_autotune(const dsgdpp_config* common, uint32_t count,
+                          const dsgdpp_problem* problems, uint32_t sample_stride, uint32_t epochs,
+                          uint32_t* d_out, uint32_t* ctas_per_sm, double* best_ms) {
+  if (!common || !problems || count == 0 || !d_out || !ctas_per_sm) return DSGDPP_E_INVALID;
+  if (sample_stride == 0) sample_stride = 1;
+  if (epochs == 0) epochs = 2;
+  static const uint32_t kCaps[] = {4, 8, 16, 32};
+  static const uint32_t kCtas[] = {0, 3, 2};  // 0: as many as fit
+  std::vector<dsgdpp_problem> sample;
+  for (uint32_t p = 0; p < count; p += sample_stride) sample.push_back(problems[p]);
+  double best = INFINITY;
+  uint32_t best_cap = 16, best_ctas = 0;
+  int last_rc = DSGDPP_OK;
+  for (uint32_t cap : kCaps) {
+    for (dsgdpp_problem& q : sample) q.d = choose_d(q.m, q.n, q.nnz, cap);
+    for (uint32_t ctas : kCtas) {
+      dsgdpp_config c = *common;
+      c.ctas_per_sm = ctas;
+      dsgdpp_batch* b = nullptr;
+      int rc = dsgdpp_batch_create(&c, (uint32_t)sample.size(), sample.data(), &b);
+      if (rc != DSGDPP_OK) {
+        last_rc = rc;
+        continue;
+      }
+      double ms = 0;
+      rc = dsgdpp_batch_run(b, 1, 1.0, 1.0, nullptr, nullptr, nullptr);  // warm-up, graph capture
+      if (rc == DSGDPP_OK) rc = dsgdpp_batch_run(b, epochs, 1.0, 1.0, nullptr, nullptr, &ms);
+      dsgdpp_batch_destroy(b);
+      if (rc != DSGDPP_OK) {
+        last_rc = rc;
+        continue;
+      }
+      if (ms < best) {
+        best = ms;
+        best_cap = cap;
+        best_ctas = ctas;
+      }
+    }
+  }
+  if (!(best < INFINITY)) return last_rc != DSGDPP_OK ? last_rc : DSGDPP_E_CUDA;
+  for (uint32_t p = 0; p < count; ++p)
+    d_out[p] = problems[p].d ? problems[p].d
+                             : choose_d(problems[p].m, problems[p].n, problems[p].nnz, best_cap);
+  *ctas_per_sm = best_ctas;
+  if (best_ms) *best_ms = best / epochs;
+  return DSGDPP_OK;
+}
+
 int dsgdpp_batch_problem_d(dsgdpp_batch* b, uint32_t p, uint32_t* d) {
   return guard(b, [&]() {
     if (p >= b->probs.size() || !d) throw Error(DSGDPP_E_INVALID, "no such problem");

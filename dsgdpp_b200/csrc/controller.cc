@@ -6,9 +6,13 @@
 //      [-1, 1]; the proposed step is eps * exp(m);
 //   2. the factors are saved on the device and the epoch runs with the
 //      proposed step;
-//   3. if the training loss rose, the proposal is rejected: the factors are
-//      restored and the epoch runs again with BoldDriver's step (eps halved,
-//      decay_bolddriver.h:59-67) -- a fallback event;
+//   3. if the training loss rose, BoldDriver takes over for this decision --
+//      a fallback event (decay_bolddriver.h:59-67: halve the step after a
+//      rise).  A rise of at most kKeepRise is kept, as BoldDriver keeps it,
+//      and the next step is the proposal halved.  A larger rise (or a
+//      non-finite loss) is rolled back: the factors are restored and the
+//      epoch re-runs with the step halved until the loss does not rise (at
+//      most kMaxHalvings times; the last attempt is kept);
 //   4. the run stops early once the test loss reaches the target.
 // No reference counterpart (the reference's BoldDriver never rolls back).
 #include <chrono>
@@ -18,6 +22,9 @@
 #include "../../include/dsgdpp.h"
 
 namespace {
+
+constexpr double kKeepRise = 0.01;  // relative training-loss rise kept without rollback
+constexpr int kMaxHalvings = 8;
 
 double since(std::chrono::steady_clock::time_point a) {
   return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -62,21 +69,28 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
     if ((rc = dsgdpp_epoch(ctx, proposed)) != DSGDPP_OK) return rc;
     double cur = 0;
     if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
-    double used = proposed;
-    if (!(cur <= tr[0])) {  // the proposed step raised the training loss
+    double used = proposed, next = proposed;
+    if (!(cur <= tr[0])) {  // the proposed step raised the training loss: fallback
       ++fb;
-      used = eps * decrease;
-      if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
-      if ((rc = dsgdpp_epoch(ctx, used)) != DSGDPP_OK) return rc;
-      if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
-      last_m = std::log(decrease);
-    } else {
-      last_m = m;
-      (void)increase;
+      if (cur <= tr[0] * (1.0 + kKeepRise)) {
+        next = proposed * decrease;  // kept, as BoldDriver keeps it
+      } else {
+        double step = eps;
+        for (int k = 0; k < kMaxHalvings; ++k) {
+          step *= decrease;
+          if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
+          if ((rc = dsgdpp_epoch(ctx, step)) != DSGDPP_OK) return rc;
+          if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
+          if (cur <= tr[0]) break;
+        }
+        used = next = step;
+      }
     }
+    (void)increase;
+    last_m = std::log(next / eps);
     if ((rc = dsgdpp_update_norms(ctx, &upd_mean, &upd_max)) != DSGDPP_OK) return rc;
     const double t_epoch = since(b);
-    eps = used;
+    eps = next;
     auto c = std::chrono::steady_clock::now();
     if (has_test && (rc = dsgdpp_nzsl(ctx, DSGDPP_TEST, &test)) != DSGDPP_OK) return rc;
     const double t_test = has_test ? since(c) : 0.0;

@@ -36,6 +36,7 @@ def main():
     ap.add_argument("--controller", default=PARAMS)
     ap.add_argument("--seed", type=int, default=777)
     ap.add_argument("--d", type=int, default=0)
+    ap.add_argument("--dump", default=None, help="write every run's trace rows here (JSON)")
     args = ap.parse_args()
 
     wl = bench.WORKLOADS[args.workload]
@@ -67,6 +68,7 @@ def main():
     out["target_test_rmse"] = target_rmse
     _, out["plain_fp32_s_traced"] = time_to_target(plain, -1)
 
+    dump = {"plain_fp32": plain}
     runs = [("bf16_bolddriver", "bf16", None)]
     net = None
     if args.controller and os.path.exists(args.controller):
@@ -83,11 +85,15 @@ def main():
                 tr, fb = ctx.run_controlled(ctl, args.epochs * 2, args.eps,
                                             target_test_loss=target_loss)
             wall = time.perf_counter() - t0
+        dump[name] = tr
         ep, secs = time_to_target(tr, target_loss)
         out[name] = {"epochs_to_target": ep, "seconds_to_target": secs, "wall_s": wall,
                      "final_test_rmse": rmse(tr[-1]["test_loss"]), "fallbacks": fb,
                      "ratio_to_plain": (secs / out["plain_fp32_s_traced"]) if ep else None}
     print(json.dumps(out), flush=True)
+    if args.dump:
+        with open(args.dump, "w") as f:
+            json.dump(dump, f)
 
 
 if __name__ == "__main__":

@@ -238,11 +238,13 @@ int dsgdpp_mlp_gradient(dsgdpp_mlp* mlp, const float* x, const float* y, int bat
 int dsgdpp_mlp_train_step(dsgdpp_mlp* mlp, const float* x, const float* y, int batch, float lr,
                           float* loss);
 /* defaultRunner with the controller choosing each step: the network proposes
- * eps * exp(m); if that epoch raises the training loss the factors are
- * restored and the epoch re-runs with BoldDriver's step (eps * decrease), a
- * fallback event.  Stops after `epochs` or once the test loss is at most
+ * eps * exp(m).  If that epoch raises the training loss, BoldDriver takes
+ * over (a fallback event): a rise of at most 1% is kept and the next step is
+ * the proposal times `decrease`; a larger rise, or a non-finite loss, is
+ * rolled back and the epoch re-run at eps * decrease^k (k = 1..8) until the
+ * loss does not rise.  Stops after `epochs` or once the test loss is at most
  * target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
- * includes the training loss the decision needs). */
+ * includes the training losses the decisions need). */
 int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs, double eps0,
                           double decrease, double increase, double target_test_loss,
                           dsgdpp_trace_row* trace, uint32_t* epochs_done, uint32_t* fallbacks);
@@ -303,6 +305,15 @@ const char* dsgdpp_batch_last_error(const dsgdpp_batch* b);
  * device time of the epochs' launches. */
 int dsgdpp_batch_run(dsgdpp_batch* b, uint32_t epochs, double decrease, double increase,
                      double* train, double* test, double* epoch_ms);
+/* The batched form's autotuner.  Times `epochs` epochs of the problems
+ * problems[0], problems[sample_stride], ... for each cap on the automatic d
+ * (4, 8, 16, 32) and each CTA count per SM (as many as fit, 3, 2), and writes
+ * the fastest choice: d_out[p] for every problem (a problem's own nonzero d
+ * is kept) and *ctas_per_sm (0 = as many as fit) for dsgdpp_config, with the
+ * sample's epoch time in *best_ms. */
+int dsgdpp_batch_autotune(const dsgdpp_config* common, uint32_t count,
+                          const dsgdpp_problem* problems, uint32_t sample_stride, uint32_t epochs,
+                          uint32_t* d_out, uint32_t* ctas_per_sm, double* best_ms);
 int dsgdpp_batch_problem_d(dsgdpp_batch* b, uint32_t p, uint32_t* d);
 int dsgdpp_batch_get_factors(dsgdpp_batch* b, uint32_t p, double* W, double* H);
 

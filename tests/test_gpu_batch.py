@@ -136,3 +136,20 @@ def test_batch_errors():
         P.Batch(P.Config(m=1, n=1, rank=1, d=1), [bad])
     with pytest.raises(P.DsgdppError):
         P.Batch(P.Config(m=1, n=1, rank=1, d=1), [])
+
+
+def test_batch_autotune_picks_valid_shapes():
+    probs = _problems(SHAPES, seed0=71)
+    probs[1]["d"] = 3  # a problem's own d is kept
+    cfg = P.Config(m=1, n=1, rank=1, d=1, precision="fp32")
+    ds, ctas, ms = P.Batch.autotune(cfg, probs, sample_stride=2, epochs=1)
+    assert ds[1] == 3 and ctas in (0, 2, 3) and ms > 0
+    for d, q in zip(ds, probs):
+        assert 1 <= d <= 32 and d <= q["m"] and 2 * d <= q["n"]
+    for p, d in zip(probs, ds):
+        p["d"] = d
+    cfg.ctas_per_sm = ctas
+    with P.Batch(cfg, probs) as b:
+        assert [b.problem_d(k) for k in range(len(probs))] == ds
+        train, _, _ = b.run(2)
+        assert np.all(np.isfinite(train))
