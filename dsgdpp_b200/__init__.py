@@ -40,6 +40,7 @@ PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
 EXEC = {"replay": 0, "hogwild": 1}
 LAUNCH = {"stream": 0, "graph": 1}
 WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
+LAYOUT = {"shuffled": 0, "col_runs": 1, "row_runs": 2, "runs": 3}
 TRAIN, TEST = 0, 1
 DECAY = {"Const": 0, "BoldDriver": 1}
 
@@ -61,6 +62,7 @@ class _Config(C.Structure):
         ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
         ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
         ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64), ("write_mode", C.c_int32),
+        ("layout", C.c_int32),
     ]
 
 
@@ -134,7 +136,7 @@ SIGNATURES = {
     "dsgdpp_run_controlled": (C.c_int, [_P, _P, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.POINTER(_TraceRow), _u32p, _u32p]),
     "dsgdpp_controller_features": (None, [_f64p, _f64p, C.c_double, C.c_double, C.c_double,
-                                          C.c_double, C.c_double, _f32p]),
+                                          C.c_double, C.c_double, C.c_double, _f32p]),
     "dsgdpp_autotune": (C.c_int, [C.POINTER(_Config), C.c_uint64, _u32p, _u32p, _f64p, _f64p,
                                   _f64p, _u32p, C.c_uint32, C.c_uint32, C.c_double,
                                   C.POINTER(_Config), _f64p]),
@@ -226,6 +228,7 @@ class Config:
     ctas_per_sm: int = 0
     layout_seed: int = 0x5EED5EED
     write_mode: str = "auto"
+    layout: str = "shuffled"
 
     def to_c(self) -> _Config:
         c = _Config()
@@ -245,6 +248,7 @@ class Config:
         c.lanes_per_nnz, c.vecs_per_lane = self.lanes_per_nnz, self.vecs_per_lane
         c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
         c.write_mode = WRITE_MODE[self.write_mode]
+        c.layout = LAYOUT[self.layout]
         return c
 
 
@@ -654,14 +658,15 @@ class Mlp:
 
 
 def controller_features(train_hist, test_hist, eps, upd_mean, upd_max, epoch_frac,
-                        last_log_mult) -> np.ndarray:
+                        last_log_mult, fail_eps=0.0) -> np.ndarray:
     tr = np.full(5, np.nan)
     te = np.full(5, np.nan)
     tr[:min(5, len(train_hist))] = list(train_hist)[:5]
     te[:min(5, len(test_hist))] = list(test_hist)[:5]
     out = np.empty(16, np.float32)
     lib.dsgdpp_controller_features(_ptr(tr, C.c_double), _ptr(te, C.c_double), eps, upd_mean,
-                                   upd_max, epoch_frac, last_log_mult, _ptr(out, C.c_float))
+                                   upd_max, epoch_frac, last_log_mult, fail_eps,
+                                   _ptr(out, C.c_float))
     return out
 
 

@@ -55,23 +55,28 @@ def _context(prob, precision="fp32", d=16, device=0):
     return ctx
 
 
-KEEP_RISE = 0.01  # as kKeepRise in csrc/controller.cc
+KEEP_RISE = 0.01  # as kKeepRise, kMaxHalvings, kCapFrac in csrc/controller.cc
 MAX_HALVINGS = 8
+CAP_FRAC = 0.9
+CAP_RELAX = 1.02
 
 
-def controlled_step(ctx, net, f, eps, prev_loss, decrease=0.5):
+def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
     """One epoch under the controller with the BoldDriver fallback, exactly as
-    dsgdpp_run_controlled takes it; returns (training loss, next step)."""
+    dsgdpp_run_controlled takes it; returns (training loss, next step, the
+    smallest step that raised the loss in this decision or 0)."""
     m = float(net.forward(f[None, :])[0])
     proposed = eps * math.exp(m)
+    if fail_eps > 0:
+        proposed = min(proposed, CAP_FRAC * fail_eps)
     ctx.save_factors()
     ctx.epoch(proposed)
     cur = ctx.loss()
     if cur <= prev_loss:
-        return cur, proposed
+        return cur, proposed, 0.0
     if cur <= prev_loss * (1.0 + KEEP_RISE):
-        return cur, proposed * decrease
-    step = eps
+        return cur, proposed * decrease, proposed
+    step, failed = proposed, proposed
     for _ in range(MAX_HALVINGS):
         step *= decrease
         ctx.restore_factors()
@@ -79,7 +84,8 @@ def controlled_step(ctx, net, f, eps, prev_loss, decrease=0.5):
         cur = ctx.loss()
         if cur <= prev_loss:
             break
-    return cur, step
+        failed = step
+    return cur, step, failed
 
 
 def label_states(first, last, prev):
@@ -114,10 +120,10 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None
             ctx.seed(int(rng.integers(1 << 31)))
             eps = float(math.exp(rng.uniform(math.log(3e-4), math.log(3e-3))))
             tr, te = [ctx.loss()], [ctx.nzsl(TEST)]
-            upd, last_m = (0.0, 0.0), 0.0
+            upd, last_m, fail_eps = (0.0, 0.0), 0.0, 0.0
             for e in range(epochs):
                 f = controller_features(tr[::-1][:5], te[::-1][:5], eps, upd[0], upd[1],
-                                        e / epochs, last_m)
+                                        e / epochs, last_m, fail_eps)
                 ctx.save_factors()
                 first, last = [], []
                 for c in CANDIDATES:
@@ -138,19 +144,26 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None
                 PV.append(tr[-1])
                 # advance by the behaviour policy from the saved state
                 ctx.restore_factors()
+                failed = 0.0
                 if policy == "bold":
                     ctx.epoch(eps)
                     cur = ctx.loss()
                     used_m = 0.0
                     nxt = eps * (0.5 if tr[-1] <= cur else 1.05)
+                    failed = eps if not cur <= tr[-1] else 0.0
                 elif policy == "net":
-                    cur, nxt = controlled_step(ctx, net, f, eps, tr[-1])
+                    cur, nxt, failed = controlled_step(ctx, net, f, eps, tr[-1], fail_eps)
                     used_m = math.log(nxt / eps)
                 else:
                     used_m = float(rng.choice(CANDIDATES))
                     ctx.epoch(eps * math.exp(used_m))
                     cur = ctx.loss()
                     nxt = eps * math.exp(used_m)
+                    failed = eps * math.exp(used_m) if not cur <= tr[-1] else 0.0
+                if failed > 0:
+                    fail_eps = min(fail_eps, failed) if fail_eps > 0 else failed
+                elif fail_eps > 0:
+                    fail_eps *= CAP_RELAX
                 upd = ctx.update_norms()
                 tr.append(cur)
                 te.append(ctx.nzsl(TEST))

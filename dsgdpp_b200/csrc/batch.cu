@@ -83,6 +83,7 @@ struct Group {
 
 struct dsgdpp_batch {
   dsgdpp_config cfg{};
+  int layout_key = 0;  // kLayout* shared by every problem (a launch has one kernel)
   std::string err;
   cudaStream_t stream = nullptr;
   int num_sms = 0;
@@ -177,6 +178,11 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
   if (common->loss == DSGDPP_LOSS_NZSL_NZL2)
     throw Error(DSGDPP_E_UNSUPPORTED, "the batched form computes the Nzsl and Nzsl_L2 losses");
   b->cfg = *common;
+  // one record order for all problems: the automatic choice is column runs
+  if (b->cfg.layout == DSGDPP_LAYOUT_RUNS) b->cfg.layout = DSGDPP_LAYOUT_COL_RUNS;
+  b->layout_key = b->cfg.layout == DSGDPP_LAYOUT_COL_RUNS   ? kLayoutColRuns
+                  : b->cfg.layout == DSGDPP_LAYOUT_ROW_RUNS ? kLayoutRowRuns
+                                                            : kLayoutShuffled;
   check_cuda(cudaSetDevice(common->device), "cudaSetDevice");
   check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
   check_cuda(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, common->device),
@@ -234,7 +240,7 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
     for (uint32_t p : G.probs) {
       Problem& P = b->probs[p];
       const auto& q = ps[p];
-      dsgdpp_config c = *common;
+      dsgdpp_config c = b->cfg;
       c.m = P.m; c.n = P.n; c.rank = P.r; c.d = P.d;
       c.launch = DSGDPP_LAUNCH_STREAM;
       dsgdpp_ctx* ctx = nullptr;
@@ -352,7 +358,8 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
     }
     G.smem_segs = most <= kSmemSegs ? most : 0;
     const bool atomic = common->write_mode != DSGDPP_WRITE_STORE;
-    int per_sm = hogwild_ctas_per_sm(prec, G.lanes, G.vecs, atomic, G.smem_segs);
+    int per_sm = hogwild_ctas_per_sm(prec, G.lanes, G.vecs, atomic, G.smem_segs,
+                                     b->layout_key != kLayoutShuffled);
     if (per_sm <= 0)
       throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" +
                                         std::to_string(G.lanes) + ", vecs_per_lane=" +
@@ -466,6 +473,13 @@ void enqueue_epoch(dsgdpp_batch* b) {
     a.row = G.row; a.col = G.col; a.val = G.val;
     a.inv1 = G.inv1; a.inv2 = G.inv2;
     a.W = G.W; a.H = G.H;
+    a.runs = b->layout_key != kLayoutShuffled;
+    if (b->layout_key == kLayoutRowRuns) {  // the kernel caches its "H" side: hand it W
+      a.row = G.col; a.col = G.row;
+      a.inv1 = G.inv2; a.inv2 = G.inv1;
+      a.W = G.H; a.H = G.W;
+      a.swap_sides = 1;
+    }
     a.segs = b->d_segs; a.launches = b->d_launches; a.counters = b->d_counters;
     a.params = b->d_params; a.smem_segs = G.smem_segs;
     a.r = G.rp; a.rp = G.rp;

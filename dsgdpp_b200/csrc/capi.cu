@@ -42,6 +42,15 @@ void release_graph(dsgdpp_ctx* c) {
   c->graph_exec = nullptr;
 }
 
+int resolve_layout(int layout, uint64_t m, uint64_t n) {
+  switch (layout) {
+    case DSGDPP_LAYOUT_COL_RUNS: return kLayoutColRuns;
+    case DSGDPP_LAYOUT_ROW_RUNS: return kLayoutRowRuns;
+    case DSGDPP_LAYOUT_RUNS: return n <= m ? kLayoutColRuns : kLayoutRowRuns;
+    default: return kLayoutShuffled;
+  }
+}
+
 void choose_hogwild_shape(dsgdpp_ctx* c) {
   const uint32_t nvec = c->rp / vec_width(c->cfg.precision);
   uint32_t lanes = c->cfg.lanes_per_nnz, vecs = c->cfg.vecs_per_lane;
@@ -56,7 +65,7 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
   if ((uint64_t)lanes * vecs < nvec)
     throw Error(DSGDPP_E_INVALID, "lanes_per_nnz x vecs_per_lane does not cover the rank");
   int per_sm = hogwild_ctas_per_sm(c->cfg.precision, lanes, vecs, c->atomic_writes != 0,
-                                   c->d + 1);
+                                   c->d + 1, c->layout_key != kLayoutShuffled);
   if (per_sm <= 0)
     throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
                                       ", vecs_per_lane=" + std::to_string(vecs));
@@ -83,6 +92,7 @@ void validate_config(const dsgdpp_config* c) {
   if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
     throw Error(DSGDPP_E_INVALID, "unknown launch form");
   if (c->write_mode < 0 || c->write_mode > 2) throw Error(DSGDPP_E_INVALID, "unknown write mode");
+  if (c->layout < 0 || c->layout > 3) throw Error(DSGDPP_E_INVALID, "unknown layout");
   if (c->update < 0 || c->update > 2) throw Error(DSGDPP_E_INVALID, "unknown update");
   if (c->regularize < 0 || c->regularize > 1) throw Error(DSGDPP_E_INVALID, "unknown regularize");
   if (c->loss < 0 || c->loss > 2) throw Error(DSGDPP_E_INVALID, "unknown loss");
@@ -168,6 +178,7 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
     throw Error(DSGDPP_E_UNSUPPORTED, "atomic writes cannot truncate");
   c->atomic_writes = cfg->write_mode == DSGDPP_WRITE_ATOMIC ||
                      (cfg->write_mode == DSGDPP_WRITE_AUTO && !cfg->truncate);
+  c->layout_key = resolve_layout(cfg->layout, cfg->m, cfg->n);
   if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
 }
 
@@ -348,10 +359,12 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
 
   reserve_records(M, u, as_double);
   if (shuffled) {
-    // in-block random layout: key = (block, 32-bit hash(layout_seed, k))
+    // in-block layout: key = (block, 32-bit hash(layout_seed, k)), or
+    // (block, local column | local row, hash) for runs
     uint64_t* k2 = skeys;  // free now
     uint32_t* i2 = sidx;
-    check_cuda(launch_shuffle_keys(ukeys, u, span, c->cfg.layout_seed, k2, i2, st), "shuffle");
+    check_cuda(launch_shuffle_keys(ukeys, u, span, nB, c->layout_key, c->cfg.layout_seed, k2,
+                                   i2, st), "shuffle");
     cub::DoubleBuffer<uint64_t> kb2(k2, ukeys);
     cub::DoubleBuffer<uint32_t> vb2(i2, flags);
     check_cuda(cub::DeviceRadixSort::SortPairs(tmp, sort2_bytes, kb2, vb2, (int)u, 0,
@@ -451,6 +464,13 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.row = M.row; a.col = M.col; a.val = M.val;
   a.inv1 = c->inv1; a.inv2 = c->inv2;
   a.W = c->W; a.H = c->H;
+  a.runs = c->layout_key != kLayoutShuffled;
+  if (c->layout_key == kLayoutRowRuns) {  // the kernel caches its "H" side: hand it W
+    a.row = M.col; a.col = M.row;
+    a.inv1 = c->inv2; a.inv2 = c->inv1;
+    a.W = c->H; a.H = c->W;
+    a.swap_sides = 1;
+  }
   a.segs = c->d_segs; a.launches = c->d_launches; a.counters = c->d_counters;
   a.params = c->d_params; a.smem_segs = d + 1;
   a.r = c->r; a.rp = c->rp;
@@ -705,6 +725,7 @@ void dsgdpp_config_init(dsgdpp_config* c) {
   c->stratum_order = DSGDPP_STRATUM_COWOR;
   c->device = 0;
   c->layout_seed = 0x5eed5eedull;
+  c->layout = DSGDPP_LAYOUT_SHUFFLED;
 }
 
 int dsgdpp_create(const dsgdpp_config* cfg, dsgdpp_ctx** out) {

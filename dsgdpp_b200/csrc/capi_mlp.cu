@@ -187,7 +187,7 @@ int dsgdpp_mlp_train_step(dsgdpp_mlp* n, const float* x, const float* y, int bat
 
 void dsgdpp_controller_features(const double* tr, const double* te, double eps, double upd_mean,
                                 double upd_max, double epoch_frac, double last_log_mult,
-                                float* f) {
+                                double fail_eps, float* f) {
   auto lr = [](double a, double b) -> float {  // log-ratio of two losses, 0 if missing
     if (!(a > 0) || !(b > 0) || std::isnan(a) || std::isnan(b)) return 0.0f;
     double v = std::log(a / b);
@@ -210,7 +210,12 @@ void dsgdpp_controller_features(const double* tr, const double* te, double eps, 
   f[12] = lr(tr[0], te[0]);
   f[13] = (float)std::fmax(-1.0, std::fmin(1.0, last_log_mult));
   f[14] = (tr[0] > 0 && tr[1] > 0) ? (tr[0] < tr[1] ? 1.0f : -1.0f) : 0.0f;
-  f[15] = 1.0f;
+  // distance (log units, as the multiplier) to the smallest step that raised
+  // the loss; 3 when none has (or the ratio is not a finite positive number)
+  const double ratio = fail_eps / eps;
+  f[15] = (fail_eps > 0 && ratio > 0 && std::isfinite(ratio))
+              ? (float)std::fmax(-3.0, std::fmin(3.0, std::log(ratio)))
+              : 3.0f;
 }
 
 }  // extern "C"

@@ -121,6 +121,7 @@ struct dsgdpp_ctx {
   // Hogwild launch shape
   uint32_t lanes = 0, vecs = 0, grid = 0;
   int atomic_writes = 0;
+  int layout_key = 0;  // kLayout* of the Hogwild training records
   // graph of one Hogwild epoch
   cudaGraphExec_t graph_exec = nullptr;
   // timing / ordering

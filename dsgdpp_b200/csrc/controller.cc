@@ -7,12 +7,16 @@
 //   2. the factors are saved on the device and the epoch runs with the
 //      proposed step;
 //   3. if the training loss rose, BoldDriver takes over for this decision --
-//      a fallback event (decay_bolddriver.h:59-67: halve the step after a
-//      rise).  A rise of at most kKeepRise is kept, as BoldDriver keeps it,
-//      and the next step is the proposal halved.  A larger rise (or a
+//      a fallback event (decay_bolddriver.h:59-67: halve the step that raised
+//      the loss).  A rise of at most kKeepRise is kept, as BoldDriver keeps
+//      it, and the next step is the proposal halved.  A larger rise (or a
 //      non-finite loss) is rolled back: the factors are restored and the
-//      epoch re-runs with the step halved until the loss does not rise (at
-//      most kMaxHalvings times; the last attempt is kept);
+//      epoch re-runs with the proposal halved, again and again until the loss
+//      does not rise (at most kMaxHalvings times; the last attempt is kept).
+//      The smallest step that raised the loss (fail_eps) is a feature of later
+//      decisions and caps them: a proposal is at most kCapFrac * fail_eps,
+//      and fail_eps grows by kCapRelax after every decision without a rise,
+//      so the edge is probed again slowly, as BoldDriver's increase does;
 //   4. the run stops early once the test loss reaches the target.
 // No reference counterpart (the reference's BoldDriver never rolls back).
 #include <chrono>
@@ -25,6 +29,8 @@ namespace {
 
 constexpr double kKeepRise = 0.01;  // relative training-loss rise kept without rollback
 constexpr int kMaxHalvings = 8;
+constexpr double kCapFrac = 0.9;    // proposals stay below this fraction of fail_eps
+constexpr double kCapRelax = 1.02;  // fail_eps growth per decision without a rise
 
 double since(std::chrono::steady_clock::time_point a) {
   return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -54,15 +60,17 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
   if (trace) trace[0] = dsgdpp_trace_row{0, loss, test, NAN, 0, 0, tl, has_test ? since(t1) : 0.0};
   push(tr, loss);
   push(te, test);
-  double eps = eps0, upd_mean = 0, upd_max = 0, last_m = 0;
+  double eps = eps0, upd_mean = 0, upd_max = 0, last_m = 0, fail_eps = 0;
+  auto failed = [&](double step) { fail_eps = fail_eps > 0 ? std::fmin(fail_eps, step) : step; };
   uint32_t fb = 0, e = 0;
   for (; e < epochs; ++e) {
     auto a = std::chrono::steady_clock::now();
     float f[16], m = 0;
     dsgdpp_controller_features(tr.data(), te.data(), eps, upd_mean, upd_max,
-                               (double)e / (double)epochs, last_m, f);
+                               (double)e / (double)epochs, last_m, fail_eps, f);
     if ((rc = dsgdpp_mlp_forward(mlp, f, 1, &m)) != DSGDPP_OK) return rc;
-    const double proposed = eps * std::exp((double)m);
+    double proposed = eps * std::exp((double)m);
+    if (fail_eps > 0) proposed = std::fmin(proposed, kCapFrac * fail_eps);
     const double t_eps = since(a);
     auto b = std::chrono::steady_clock::now();
     if ((rc = dsgdpp_save_factors(ctx)) != DSGDPP_OK) return rc;
@@ -72,19 +80,23 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
     double used = proposed, next = proposed;
     if (!(cur <= tr[0])) {  // the proposed step raised the training loss: fallback
       ++fb;
+      failed(proposed);
       if (cur <= tr[0] * (1.0 + kKeepRise)) {
         next = proposed * decrease;  // kept, as BoldDriver keeps it
       } else {
-        double step = eps;
+        double step = proposed;
         for (int k = 0; k < kMaxHalvings; ++k) {
           step *= decrease;
           if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_epoch(ctx, step)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
           if (cur <= tr[0]) break;
+          failed(step);
         }
         used = next = step;
       }
+    } else if (fail_eps > 0) {
+      fail_eps *= kCapRelax;
     }
     (void)increase;
     last_m = std::log(next / eps);

@@ -40,6 +40,8 @@ struct HogwildArgs {
   uint32_t r, rp;
   int update, truncate, sgd_order;
   int atomic;                   // 1: write the update atomically (vector atomic add)
+  int runs;                     // 1: records come in runs of one H row (see the kernel)
+  int swap_sides;               // 1: W/H (and row/col, inv1/inv2) are passed swapped
   double lambda, tmin, tmax;
 };
 
@@ -79,7 +81,7 @@ cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const H
                            uint32_t launch_index, uint32_t grid, cudaStream_t st);
 // CTAs per SM that the Hogwild kernel sustains for this configuration
 int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
-                        uint32_t smem_segs);
+                        uint32_t smem_segs, bool runs);
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
 // RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
@@ -163,9 +165,12 @@ cudaError_t launch_merge_runs(const BlockingGeom& g, const uint64_t* keys, const
                               uint32_t* urow, uint32_t* ucol, double* uval, cudaStream_t st);
 cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
                              uint32_t nblocks, uint64_t* block_ptr, cudaStream_t st);
+// in-block layout keys of the Hogwild matrix: (block, hash) for a shuffled
+// layout; (block, local column, hash) or (block, local row, hash) for runs
+enum LayoutKey : int { kLayoutShuffled = 0, kLayoutColRuns = 1, kLayoutRowRuns = 2 };
 cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
-                                uint64_t seed, uint64_t* keys2, uint32_t* idx2,
-                                cudaStream_t st);
+                                uint64_t nB, int mode, uint64_t seed, uint64_t* keys2,
+                                uint32_t* idx2, cudaStream_t st);
 cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
                                   const uint32_t* ucol, const double* uval, uint32_t* row,
                                   uint32_t* col, void* val, int val_is_double, cudaStream_t st);

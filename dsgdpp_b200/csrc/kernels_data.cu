@@ -93,12 +93,22 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
-__global__ void shuffle_keys_kernel(const uint64_t* ukeys, uint64_t u, uint64_t span,
-                                    uint64_t seed, uint64_t* keys2, uint32_t* idx2) {
+// 32 low bits of the key: a hash of the record (shuffled), or the local
+// column / row in the high `side_bits` bits above 32 - side_bits hash bits
+__global__ void shuffle_keys_kernel(const uint64_t* ukeys, uint64_t u, uint64_t span, uint64_t nB,
+                                    int mode, int side_bits, uint64_t seed, uint64_t* keys2,
+                                    uint32_t* idx2) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
-    const uint64_t blk = ukeys[k] / span;
-    keys2[k] = (blk << 32) | (mix64(seed ^ (k * 0xD6E8FEB86659FD93ull)) >> 32);
+    const uint64_t blk = ukeys[k] / span, local = ukeys[k] % span;
+    const uint32_t hash = (uint32_t)(mix64(seed ^ (k * 0xD6E8FEB86659FD93ull)) >> 32);
+    uint32_t low = hash;
+    if (mode != kLayoutShuffled) {
+      const uint64_t side = mode == kLayoutColRuns ? local % nB : local / nB;
+      low = side_bits >= 32 ? (uint32_t)side
+                            : (uint32_t)(side << (32 - side_bits)) | (hash >> side_bits);
+    }
+    keys2[k] = (blk << 32) | low;
     idx2[k] = (uint32_t)k;
   }
 }
@@ -215,10 +225,14 @@ cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_s
 }
 
 cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
-                                uint64_t seed, uint64_t* keys2, uint32_t* idx2,
-                                cudaStream_t st) {
+                                uint64_t nB, int mode, uint64_t seed, uint64_t* keys2,
+                                uint32_t* idx2, cudaStream_t st) {
+  const uint64_t side_extent = mode == kLayoutColRuns ? nB : (nB ? block_span / nB : 1);
+  int side_bits = 0;
+  while (side_bits < 32 && (1ull << side_bits) < side_extent) ++side_bits;
   if (u == 0) return cudaSuccess;
-  shuffle_keys_kernel<<<kGrid, 256, 0, st>>>(ukeys, u, block_span, seed, keys2, idx2);
+  shuffle_keys_kernel<<<kGrid, 256, 0, st>>>(ukeys, u, block_span, nB, mode, side_bits, seed,
+                                             keys2, idx2);
   return cudaGetLastError();
 }
 

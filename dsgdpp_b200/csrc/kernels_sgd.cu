@@ -83,6 +83,146 @@ __device__ __forceinline__ void red_bf16_increment(__nv_bfloat16* q, const uint4
                ::"l"(q), "r"(inc[0]), "r"(inc[1]), "r"(inc[2]), "r"(inc[3]) : "memory");
 }
 
+// Writes one updated W or H vector: an atomic add of its change (FP32 /
+// FP64), an atomic add of the change of its stochastically rounded value
+// (BF16), or a store (rounded stochastically for BF16).
+template <typename T, bool ATOMIC>
+__device__ __forceinline__ void write_vec(T* p, const uint4& old,
+                                          const typename Elem<T>::C (&was)[Elem<T>::VW],
+                                          const typename Elem<T>::C (&now)[Elem<T>::VW],
+                                          uint64_t rec, uint32_t tag, const EpochParams& ep) {
+  constexpr int VW = Elem<T>::VW;
+  constexpr bool kSR = sizeof(T) == 2;
+  if constexpr (ATOMIC && !kSR) {
+    if constexpr (sizeof(T) == 4) {
+      atomicAdd(reinterpret_cast<float4*>(p),
+                make_float4(now[0] - was[0], now[1] - was[1], now[2] - was[2], now[3] - was[3]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < VW; ++e) atomicAdd(reinterpret_cast<double*>(p) + e, (double)(now[e] - was[e]));
+    }
+  } else {
+    Philox4 rnd;
+    if constexpr (kSR)
+      rnd = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, tag, ep.key0, ep.key1);
+    if constexpr (ATOMIC && kSR)
+      red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(p), old, now, rnd);
+    else
+      store_vec<T>(p, now, &rnd);
+  }
+}
+
+// Records of a chunk in runs of one H row (the layout sorts each block by
+// column): group g walks records g*LPN .. g*LPN + LPN - 1 in order, keeps the
+// H row of the current run in registers -- the run's updates of it are
+// sequential SGD -- and writes it back once when the run ends.  Every
+// record's W row is read and written as in the shuffled path.  With the sides
+// swapped by the host (runs of one W row) the same code caches the W row.
+template <typename T, int LPN, int VPL, bool ATOMIC>
+__device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint64_t rb,
+                                          uint32_t nrec, uint32_t my_row, uint32_t my_col,
+                                          typename Elem<T>::C my_x, typename Elem<T>::C my_a,
+                                          typename Elem<T>::C my_b, typename Elem<T>::C eps,
+                                          typename Elem<T>::C cwh, typename Elem<T>::C rw,
+                                          typename Elem<T>::C rh, typename Elem<T>::C tmin,
+                                          typename Elem<T>::C tmax, const EpochParams& ep,
+                                          uint32_t grp, uint32_t gl) {
+  using E = Elem<T>;
+  using C = typename E::C;
+  constexpr int VW = E::VW;
+  constexpr uint32_t kNone = 0xffffffffu;
+  uint32_t cur = kNone;  // H row of the open run
+  uint4 hv0[VPL];        // ... as loaded
+  C h0[VPL][VW];         // ... unpacked as loaded
+  C hf[VPL][VW];         // ... as updated so far
+  uint64_t last_rec = 0;
+#pragma unroll 1
+  for (int t = 0; t < LPN; ++t) {
+    const uint32_t ri = grp * LPN + t;
+    const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
+    const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
+    const C x = __shfl_sync(kFullMask, my_x, ri);
+    const C ca = __shfl_sync(kFullMask, my_a, ri);
+    const C cb = __shfl_sync(kFullMask, my_b, ri);
+    const bool valid = ri < nrec;
+    if (cur != kNone && (!valid || col != cur)) {  // the run ends: write its H row back
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        if (e0 < a.rp)
+          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], last_rec,
+                               e0 | 0x80000000u, ep);
+      }
+      cur = kNone;
+    }
+    if (valid && cur == kNone) {  // a run starts: load its H row
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        hv0[v] = e0 < a.rp ? *reinterpret_cast<const uint4*>(H + (size_t)col * a.rp + e0)
+                           : make_uint4(0, 0, 0, 0);
+        E::unpack(hv0[v], h0[v]);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) hf[v][e] = h0[v][e];
+      }
+      cur = col;
+    }
+    T* wp = W + (size_t)row * a.rp;
+    uint4 wv[VPL];
+    C wf[VPL][VW];
+    C dot = 0;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      wv[v] = (valid && e0 < a.rp) ? *reinterpret_cast<const uint4*>(wp + e0)
+                                   : make_uint4(0, 0, 0, 0);
+      E::unpack(wv[v], wf[v]);
+      if (valid) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+      }
+    }
+#pragma unroll
+    for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+    if (!valid) continue;
+    const C f1 = (C)-2 * eps * (x - dot * cwh);
+    const C fw = f1 * rw, fh = f1 * rh;
+    const uint64_t rec = rb + ri;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      if (e0 >= a.rp) continue;
+      C nw[VW], nh[VW];
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+        nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+      }
+      if (!ATOMIC && a.truncate) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          if (e0 + e < a.r) {
+            nw[e] = clampw(nw[e], tmin, tmax, eps);
+            nh[e] = clampw(nh[e], tmin, tmax, eps);
+          }
+      }
+      write_vec<T, ATOMIC>(wp + e0, wv[v], wf[v], nw, rec, e0, ep);
+#pragma unroll
+      for (int e = 0; e < VW; ++e) hf[v][e] = nh[e];
+    }
+    last_rec = rec;
+  }
+  if (cur != kNone) {
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      if (e0 < a.rp)
+        write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], last_rec,
+                             e0 | 0x80000000u, ep);
+    }
+  }
+}
+
 // One launch = one work list of segments (a segment = one conflict-free block
 // of a sub-epoch; several problems' segments in the batched form).  Warps take
 // 32-entry chunks from the launch's work counter; a chunk's entries are loaded
@@ -90,7 +230,7 @@ __device__ __forceinline__ void red_bf16_increment(__nv_bfloat16* q, const uint4
 // right before it is used.  (Prefetching the next chunk's rows into registers
 // or into shared memory with cp.async measured slower on B200: the extra
 // registers or shared memory cost more resident warps than the prefetch gains.)
-template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM>
+template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM, bool RUNS>
 __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
@@ -151,7 +291,9 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
     const uint64_t rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
     const uint32_t nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
     const C eps = (C)seg[lo].eps, f2 = eps * lambda2;
-    const C cwh = (C)seg[lo].cwh, rw = (C)seg[lo].rho_w, rh = (C)seg[lo].rho_h;
+    const C cwh = (C)seg[lo].cwh;
+    const C rw = (C)(a.swap_sides ? seg[lo].rho_h : seg[lo].rho_w);
+    const C rh = (C)(a.swap_sides ? seg[lo].rho_w : seg[lo].rho_h);
 
     uint32_t my_row = 0, my_col = 0;
     C my_x = 0, my_a = 0, my_b = 0;
@@ -168,89 +310,94 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
       }
     }
 
-    for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
-      const uint32_t ri = t0 + grp;
-      const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
-      const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
-      const C x = __shfl_sync(kFullMask, my_x, ri);
-      const C ca = __shfl_sync(kFullMask, my_a, ri);
-      const C cb = __shfl_sync(kFullMask, my_b, ri);
-      const bool valid = ri < nrec;
-      T* wp = W + (size_t)row * a.rp;
-      T* hp = H + (size_t)col * a.rp;
-      uint4 wv[VPL], hv[VPL];
-      bool live[VPL];
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        live[v] = valid && e0 < a.rp;
-        if (live[v]) {
-          wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
-          hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
-        } else {
-          wv[v] = make_uint4(0, 0, 0, 0);
-          hv[v] = make_uint4(0, 0, 0, 0);
-        }
-      }
-      C dot = 0;
-      C wf[VPL][VW], hf[VPL][VW];
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        E::unpack(wv[v], wf[v]);
-        E::unpack(hv[v], hf[v]);
-#pragma unroll
-        for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
-      }
-#pragma unroll
-      for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
-      const C f1 = (C)-2 * eps * (x - dot * cwh);
-      const C fw = f1 * rw, fh = f1 * rh;
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        if (!live[v]) continue;
-        C nw[VW], nh[VW];
-#pragma unroll
-        for (int e = 0; e < VW; ++e) {
-          nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
-          nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
-        }
-        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        if (!ATOMIC && a.truncate) {
-#pragma unroll
-          for (int e = 0; e < VW; ++e)
-            if (e0 + e < a.r) {
-              nw[e] = clampw(nw[e], tmin, tmax, eps);
-              nh[e] = clampw(nh[e], tmin, tmax, eps);
-            }
-        }
-        const uint64_t rec = rb + ri;
-        if constexpr (ATOMIC && !kSR) {
-          // add the update, so concurrent updates of one row are not lost
-          if constexpr (sizeof(T) == 4) {
-            atomicAdd(reinterpret_cast<float4*>(wp + e0),
-                      make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
-            atomicAdd(reinterpret_cast<float4*>(hp + e0),
-                      make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
+    if constexpr (RUNS) {
+      run_chunk<T, LPN, VPL, ATOMIC>(a, W, H, rb, nrec, my_row, my_col, my_x, my_a, my_b, eps,
+                                     cwh, rw, rh, tmin, tmax, ep, grp, gl);
+    } else {
+      for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
+        const uint32_t ri = t0 + grp;
+        const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
+        const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
+        const C x = __shfl_sync(kFullMask, my_x, ri);
+        const C ca = __shfl_sync(kFullMask, my_a, ri);
+        const C cb = __shfl_sync(kFullMask, my_b, ri);
+        const bool valid = ri < nrec;
+        T* wp = W + (size_t)row * a.rp;
+        T* hp = H + (size_t)col * a.rp;
+        uint4 wv[VPL], hv[VPL];
+        bool live[VPL];
+  #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+          live[v] = valid && e0 < a.rp;
+          if (live[v]) {
+            wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
+            hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
           } else {
-#pragma unroll
-            for (int e = 0; e < VW; ++e) {
-              atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
-              atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
+            wv[v] = make_uint4(0, 0, 0, 0);
+            hv[v] = make_uint4(0, 0, 0, 0);
+          }
+        }
+        C dot = 0;
+        C wf[VPL][VW], hf[VPL][VW];
+  #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          E::unpack(wv[v], wf[v]);
+          E::unpack(hv[v], hf[v]);
+  #pragma unroll
+          for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+        }
+  #pragma unroll
+        for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+        const C f1 = (C)-2 * eps * (x - dot * cwh);
+        const C fw = f1 * rw, fh = f1 * rh;
+  #pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          if (!live[v]) continue;
+          C nw[VW], nh[VW];
+  #pragma unroll
+          for (int e = 0; e < VW; ++e) {
+            nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+            nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+          }
+          const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+          if (!ATOMIC && a.truncate) {
+  #pragma unroll
+            for (int e = 0; e < VW; ++e)
+              if (e0 + e < a.r) {
+                nw[e] = clampw(nw[e], tmin, tmax, eps);
+                nh[e] = clampw(nh[e], tmin, tmax, eps);
+              }
+          }
+          const uint64_t rec = rb + ri;
+          if constexpr (ATOMIC && !kSR) {
+            // add the update, so concurrent updates of one row are not lost
+            if constexpr (sizeof(T) == 4) {
+              atomicAdd(reinterpret_cast<float4*>(wp + e0),
+                        make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
+              atomicAdd(reinterpret_cast<float4*>(hp + e0),
+                        make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
+            } else {
+  #pragma unroll
+              for (int e = 0; e < VW; ++e) {
+                atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
+                atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
+              }
             }
-          }
-        } else {
-          Philox4 r1, r2;
-          if constexpr (kSR) {
-            r1 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
-            r2 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
-                               ep.key0, ep.key1);
-          }
-          if constexpr (ATOMIC && kSR) {
-            red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(wp + e0), wv[v], nw, r1);
-            red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(hp + e0), hv[v], nh, r2);
           } else {
-            store_vec<T>(wp + e0, nw, &r1);
-            store_vec<T>(hp + e0, nh, &r2);
+            Philox4 r1, r2;
+            if constexpr (kSR) {
+              r1 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
+              r2 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
+                                 ep.key0, ep.key1);
+            }
+            if constexpr (ATOMIC && kSR) {
+              red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(wp + e0), wv[v], nw, r1);
+              red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(hp + e0), hv[v], nh, r2);
+            } else {
+              store_vec<T>(wp + e0, nw, &r1);
+              store_vec<T>(hp + e0, nh, &r2);
+            }
           }
         }
       }
@@ -493,19 +640,27 @@ __global__ void scale_rows_kernel(T* W, uint64_t wrows, T* H, uint64_t hrows, ui
   }
 }
 
-template <typename T, int LPN, int VPL>
-void* hogwild_fn(bool atomic, bool smem) {
+template <typename T, int LPN, int VPL, bool RUNS>
+void* hogwild_fn3(bool atomic, bool smem) {
   if (smem)
-    return atomic ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, true>)
-                  : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, true>);
-  return atomic ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, false>)
-                : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, false>);
+    return atomic
+               ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, true, RUNS>)
+               : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, true, RUNS>);
+  return atomic
+             ? reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, true, false, RUNS>)
+             : reinterpret_cast<void*>(&hogwild_subepoch_kernel<T, LPN, VPL, false, false, RUNS>);
+}
+
+template <typename T, int LPN, int VPL>
+void* hogwild_fn(bool atomic, bool smem, bool runs) {
+  return runs ? hogwild_fn3<T, LPN, VPL, true>(atomic, smem)
+              : hogwild_fn3<T, LPN, VPL, false>(atomic, smem);
 }
 
 template <typename T>
-void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool smem) {
+void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool smem, bool runs) {
 #define DSGDPP_CASE(L, V) \
-  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>(atomic, smem);
+  if (lanes == L && vecs == V) return hogwild_fn<T, L, V>(atomic, smem, runs);
   DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
   DSGDPP_CASE(2, 2) DSGDPP_CASE(4, 2) DSGDPP_CASE(8, 2) DSGDPP_CASE(16, 2) DSGDPP_CASE(32, 2)
   DSGDPP_CASE(32, 4)
@@ -513,10 +668,11 @@ void* pick_hogwild(uint32_t lanes, uint32_t vecs, bool atomic, bool smem) {
   return nullptr;
 }
 
-void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool smem) {
-  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs, atomic, smem);
-  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs, atomic, smem);
-  return pick_hogwild<__nv_bfloat16>(lanes, vecs, atomic, smem);
+void* hogwild_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs, bool atomic, bool smem,
+                         bool runs) {
+  if (precision == kFp64) return pick_hogwild<double>(lanes, vecs, atomic, smem, runs);
+  if (precision == kFp32) return pick_hogwild<float>(lanes, vecs, atomic, smem, runs);
+  return pick_hogwild<__nv_bfloat16>(lanes, vecs, atomic, smem, runs);
 }
 
 }  // namespace
@@ -530,8 +686,8 @@ cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st) {
 }
 
 int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
-                        uint32_t smem_segs) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, smem_segs > 0);
+                        uint32_t smem_segs, bool runs) {
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, smem_segs > 0, runs);
   if (!fn) return 0;
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * smem_segs) !=
@@ -542,7 +698,8 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomi
 
 cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
                            uint32_t launch_index, uint32_t grid, cudaStream_t st) {
-  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.smem_segs > 0);
+  void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.smem_segs > 0,
+                                a.runs != 0);
   if (!fn) return cudaErrorInvalidValue;
   HogwildArgs args = a;
   uint32_t li = launch_index;

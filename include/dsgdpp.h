@@ -74,6 +74,11 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 #define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */
 #define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically: vector atomic add (FP32/FP64);
                                  BF16 adds the increment to the stochastically rounded value */
+/* order of the Hogwild training records inside each block */
+#define DSGDPP_LAYOUT_SHUFFLED 0 /* random order (hash of layout_seed and the record) */
+#define DSGDPP_LAYOUT_COL_RUNS 1 /* by column, random within a column: runs of one H row */
+#define DSGDPP_LAYOUT_ROW_RUNS 2 /* by row, random within a row: runs of one W row */
+#define DSGDPP_LAYOUT_RUNS 3     /* COL_RUNS when n <= m (more records per column), else ROW_RUNS */
 /* matrices */
 #define DSGDPP_TRAIN 0
 #define DSGDPP_TEST 1
@@ -104,6 +109,7 @@ typedef struct dsgdpp_config {
   uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
   int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
+  int32_t layout;         /* Hogwild record order in a block: DSGDPP_LAYOUT_* */
 } dsgdpp_config;
 
 /* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */
@@ -241,20 +247,23 @@ int dsgdpp_mlp_train_step(dsgdpp_mlp* mlp, const float* x, const float* y, int b
  * eps * exp(m).  If that epoch raises the training loss, BoldDriver takes
  * over (a fallback event): a rise of at most 1% is kept and the next step is
  * the proposal times `decrease`; a larger rise, or a non-finite loss, is
- * rolled back and the epoch re-run at eps * decrease^k (k = 1..8) until the
- * loss does not rise.  Stops after `epochs` or once the test loss is at most
- * target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
+ * rolled back and the epoch re-run at the proposal times decrease^k
+ * (k = 1..8) until the loss does not rise.  Once a step has raised the loss,
+ * proposals are capped at 0.9 times the smallest such step, a cap that grows
+ * by 2% with every decision that does not raise the loss.  Stops after `epochs` or once the
+ * test loss is at most target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
  * includes the training losses the decisions need). */
 int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs, double eps0,
                           double decrease, double increase, double target_test_loss,
                           dsgdpp_trace_row* trace, uint32_t* epochs_done, uint32_t* fallbacks);
 /* The 16 controller features from the run history: train/test losses of the
  * last 5 evaluations (index 0 = newest; NaN where missing), the current step,
- * the mean/max factor-update norms of the last epoch, the epoch fraction and
- * the last applied log multiplier. */
+ * the mean/max factor-update norms of the last epoch, the epoch fraction, the
+ * last applied log multiplier and the smallest step that has raised the
+ * training loss so far in this run (fail_eps; 0 = none), as log(fail_eps/eps). */
 void dsgdpp_controller_features(const double* train_hist, const double* test_hist, double eps,
                                 double upd_mean, double upd_max, double epoch_frac,
-                                double last_log_mult, float* out16);
+                                double last_log_mult, double fail_eps, float* out16);
 
 /* ---- autotuning ------------------------------------------------------------- */
 /* No reference counterpart (the reference takes d from --tasks-per-rank).

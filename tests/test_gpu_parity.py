@@ -247,6 +247,41 @@ def test_hogwild_tracks_fp64_oracle(precision, write_mode, tol, launch):
         assert abs(got - want) <= tol * want, (got, want)
 
 
+# Records in runs of one H row (or W row) per group: the run's updates of the
+# shared row are sequential and written once; the same tolerances hold.
+@pytest.mark.parametrize("layout", ["col_runs", "row_runs"])
+@pytest.mark.parametrize("precision,write_mode,tol", [
+    ("fp64", "atomic", 0.005), ("fp32", "atomic", 0.005), ("bf16", "atomic", 0.01),
+    ("fp32", "store", 0.08)])
+def test_hogwild_runs_layout_tracks_fp64_oracle(layout, precision, write_mode, tol):
+    p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
+    ref, ctx = _pair(p, 10, 4, precision=precision, exec="hogwild", launch="graph",
+                     write_mode=write_mode, layout=layout)
+    with ctx:
+        ctx.seed(9)
+        ref.seed(9)
+        for _ in range(8):
+            ctx.epoch(0.01)
+            ref.epoch(0.01)
+        got = _rmse(ctx, len(p.tvals))
+        want = float(np.sqrt(ref.nzsl(1) / len(p.tvals)))
+        assert abs(got - want) <= tol * want, (got, want)
+
+
+@pytest.mark.parametrize("layout", ["shuffled", "col_runs", "row_runs"])
+def test_hogwild_truncation_bounds_every_factor(layout):
+    p = _problem(m=3000, n=2000, nnz=60000, ntest=100, r=12)
+    cfg = P.Config(m=p.m, n=p.n, rank=12, d=4, precision="fp32", write_mode="store",
+                   truncate=(-0.2, 0.25), layout=layout)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_factors(np.clip(p.W0, -0.2, 0.25), np.clip(p.H0, -0.2, 0.25))
+        for _ in range(3):
+            ctx.epoch(0.05)
+        W, H = ctx.get_factors()
+    assert W.min() >= -0.2 and W.max() <= 0.25 and H.min() >= -0.2 and H.max() <= 0.25
+
+
 def test_hogwild_lazy_l2_scaling_matches_exact():
     # with no training entries the epoch is pure RegularizeL2 scaling: W is
     # scaled 2d times, each H column block d times

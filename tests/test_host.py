@@ -132,9 +132,13 @@ def test_controller_features_shape_and_values():
     assert f.shape == (16,) and f.dtype == np.float32
     assert f[0] == pytest.approx(10 * np.log(90 / 100), rel=1e-6)
     assert f[8] == pytest.approx(-1.0, rel=1e-6)  # log10(0.001) / 3
-    assert f[11] == pytest.approx(0.25) and f[13] == pytest.approx(0.1) and f[15] == 1.0
+    assert f[11] == pytest.approx(0.25) and f[13] == pytest.approx(0.1)
+    assert f[15] == 3.0  # no step has raised the loss
     g = P.controller_features([5.0], [], 0.01, 0.0, 0.0, 0.0, 0.0)  # short history
     assert np.all(g[0:8] == 0) and np.all(np.isfinite(g))
+    h = P.controller_features([5.0], [], 0.01, 0.0, 0.0, 0.0, 0.0, fail_eps=0.02)
+    assert h[15] == pytest.approx(np.log(2.0), rel=1e-6)
+    assert P.controller_features([5.0], [], 0.01, 0, 0, 0, 0, fail_eps=1e9)[15] == 3.0
 
 
 def test_mlp_oracle_gradient_matches_finite_differences():
