@@ -14,7 +14,13 @@ One step = one DSGD++ epoch (2d sub-epochs over all training entries) of the
            (12 B entry + 4 r 4 B of factor rows/columns + 8 B inverse counts per
            update) over its event-timed average launch duration;
 * cpu_baseline: the CPU restatement of the reference (oracle, threaded mode,
-           one thread per task, d = threads) timed on a 10M-entry sample.
+           one thread per task, d = threads) timed on a 10M-entry sample;
+           test_rmse_vs_fp64_oracle compares this implementation's test RMSE
+           with the oracle's on that sample (same d, seed and steps);
+* time_to_target: plain FP32 BoldDriver runs 50 epochs; its final test RMSE
+           (+0.5%) is the target that BF16 + BoldDriver and the learned
+           controller (FP32, BF16) race to, in wall time of every epoch, loss
+           and step decision.
 
 `--impl reference` times only the CPU restatement of the reference path (all
 host cores) on the same sample and prints its own line.
@@ -300,6 +306,8 @@ def main():
                     help="use --d (default 64) instead of tuning d in 64..512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ttt", action="store_true",
+                    help="skip the time-to-target comparison (tuned vs plain FP32)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -420,6 +428,20 @@ def main():
                      "test_rmse": got, "rel_error": (got - ref["test_rmse"]) / ref["test_rmse"]}
 
     ctx.close()
+
+    # ---- time to target test RMSE: BF16 + learned controller vs plain FP32 ----
+    ttt = None
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_ttt:
+        from dsgdpp_b200 import ttt as TT
+        net = P.Mlp(device=local, seed=1)
+        net.params = np.load(TT.PARAMS)
+        r = TT.evaluate(P, wl, data, d, epochs=50, eps0=eps, net=net, device=local)
+        net.close()
+        ttt = {"target": "plain FP32 BoldDriver's test RMSE after 50 epochs, +0.5%",
+               "target_test_rmse": r["target_test_rmse"], "plain_fp32_s": r["plain_fp32_s_traced"]}
+        for k in ("bf16_bolddriver", "fp32_controller", "bf16_controller"):
+            ttt[k] = {q: r[k][q] for q in ("epochs_to_target", "seconds_to_target",
+                                            "ratio_to_plain", "fallbacks")}
     if rank == 0:
         line = {
             "metric": "SGD updates/s (DSGD++ epoch)", "value": value, "unit": "updates/s",
@@ -440,6 +462,7 @@ def main():
                          "avg_launch_us": avg_launch_s * 1e6},
             "cpu_baseline": cpu,
             "test_rmse_vs_fp64_oracle": vs_oracle,
+            "time_to_target": ttt,
             "e2e": e2e,
             "gpu_launches": args.steps * (2 * d + 1 + (1 if l2 else 0)),
             "clocks": clk,

@@ -58,7 +58,7 @@ def _context(prob, precision="fp32", d=16, device=0):
 KEEP_RISE = 0.01  # as kKeepRise, kMaxHalvings, kCapFrac in csrc/controller.cc
 MAX_HALVINGS = 8
 CAP_FRAC = 0.9
-CAP_RELAX = 1.02
+CAP_RELAX = 1.05
 
 
 def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
@@ -82,10 +82,10 @@ def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
         ctx.restore_factors()
         ctx.epoch(step)
         cur = ctx.loss()
-        if cur <= prev_loss:
+        if cur <= prev_loss * (1.0 + KEEP_RISE):
             break
         failed = step
-    return cur, step, failed
+    return cur, (step if cur <= prev_loss else step * decrease), failed
 
 
 def label_states(first, last, prev):

@@ -12,11 +12,12 @@
 //      it, and the next step is the proposal halved.  A larger rise (or a
 //      non-finite loss) is rolled back: the factors are restored and the
 //      epoch re-runs with the proposal halved, again and again until the loss
-//      does not rise (at most kMaxHalvings times; the last attempt is kept).
+//      rises by at most kKeepRise (at most kMaxHalvings times; the last
+//      attempt is kept).
 //      The smallest step that raised the loss (fail_eps) is a feature of later
 //      decisions and caps them: a proposal is at most kCapFrac * fail_eps,
-//      and fail_eps grows by kCapRelax after every decision without a rise,
-//      so the edge is probed again slowly, as BoldDriver's increase does;
+//      and fail_eps grows by kCapRelax (BoldDriver's increase) after every
+//      decision without a rise, so the edge is probed again slowly;
 //   4. the run stops early once the test loss reaches the target.
 // No reference counterpart (the reference's BoldDriver never rolls back).
 #include <chrono>
@@ -30,7 +31,7 @@ namespace {
 constexpr double kKeepRise = 0.01;  // relative training-loss rise kept without rollback
 constexpr int kMaxHalvings = 8;
 constexpr double kCapFrac = 0.9;    // proposals stay below this fraction of fail_eps
-constexpr double kCapRelax = 1.02;  // fail_eps growth per decision without a rise
+constexpr double kCapRelax = 1.05;  // fail_eps growth per decision without a rise
 
 double since(std::chrono::steady_clock::time_point a) {
   return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -90,10 +91,11 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
           if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_epoch(ctx, step)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
-          if (cur <= tr[0]) break;
+          if (cur <= tr[0] * (1.0 + kKeepRise)) break;  // kept, as the first attempt
           failed(step);
         }
-        used = next = step;
+        used = step;
+        next = cur <= tr[0] ? step : step * decrease;
       }
     } else if (fail_eps > 0) {
       fail_eps *= kCapRelax;

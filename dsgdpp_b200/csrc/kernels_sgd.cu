@@ -131,6 +131,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   using C = typename E::C;
   constexpr int VW = E::VW;
   constexpr uint32_t kNone = 0xffffffffu;
+  constexpr int kRunCap = 8;
   uint32_t cur = kNone;  // H row of the open run
   uint4 hv0[VPL];        // ... as loaded
   C h0[VPL][VW];         // ... unpacked as loaded
@@ -145,7 +146,10 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
     const C ca = __shfl_sync(kFullMask, my_a, ri);
     const C cb = __shfl_sync(kFullMask, my_b, ri);
     const bool valid = ri < nrec;
-    if (cur != kNone && (!valid || col != cur)) {  // the run ends: write its H row back
+    // a run ends at a new column, or after kRunCap records: the row is then
+    // written back and re-read, so other warps' updates of a hot row reach
+    // this group at least every kRunCap records
+    if (cur != kNone && (!valid || col != cur || (t % kRunCap) == 0)) {
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;

@@ -9,6 +9,7 @@
 //   --exec hogwild|replay        replay = the reference's sequential point
 //                                order per block, FP64 only (default hogwild)
 //   --launch graph|stream        epoch as one CUDA graph or 2d launches
+//   --layout shuffled|col-runs|row-runs|runs   Hogwild record order in a block
 // Extension: --regularize L2(l) is accepted (the reference rejects every
 // regularizer other than None, tools/mfdsgdpp.cc:165-258).
 #include <cmath>
@@ -46,14 +47,14 @@ struct Args {
   int sgdOrder = DSGDPP_SGD_WOR, stratumOrder = DSGDPP_STRATUM_COWOR;
   // added options
   int device = 0;
-  std::string precision = "fp32", exec = "hogwild", launch = "graph";
+  std::string precision = "fp32", exec = "hogwild", launch = "graph", layout = "shuffled";
 };
 
 const char* kOptions[] = {
     "help", "input-file", "input-test-file", "input-row-file", "input-col-file",
     "output-row-file", "output-col-file", "trace", "trace-var", "epochs", "tasks-per-rank",
     "sgd-order", "stratum-order", "seed", "rank", "update", "regularize", "loss", "abs",
-    "truncate", "decay", "balance", "device", "precision", "exec", "launch"};
+    "truncate", "decay", "balance", "device", "precision", "exec", "launch", "layout"};
 
 void usage() {
   std::cout << "mfsgdpp [options]\n\nOptions:\n"
@@ -87,7 +88,9 @@ void usage() {
             << "  --device arg           CUDA device [0]\n"
             << "  --precision arg        factor storage fp64|fp32|bf16 [fp32]\n"
             << "  --exec arg             hogwild|replay [hogwild]\n"
-            << "  --launch arg           graph|stream [graph]\n";
+            << "  --launch arg           graph|stream [graph]\n"
+            << "  --layout arg           Hogwild record order in a block:\n"
+            << "                         shuffled|col-runs|row-runs|runs [shuffled]\n";
 }
 
 // parse::parseArg (tools/parse.h:38-61): "Name(a,b,...)" -> name + doubles
@@ -341,6 +344,10 @@ int run(Args& args, const Job& job) {
   cfg.precision = args.precision == "fp64" ? DSGDPP_FP64 : args.precision == "bf16" ? DSGDPP_BF16 : DSGDPP_FP32;
   cfg.exec = args.exec == "replay" ? DSGDPP_EXEC_REPLAY : DSGDPP_EXEC_HOGWILD;
   cfg.launch = args.launch == "stream" ? DSGDPP_LAUNCH_STREAM : DSGDPP_LAUNCH_GRAPH;
+  cfg.layout = args.layout == "col-runs"   ? DSGDPP_LAYOUT_COL_RUNS
+               : args.layout == "row-runs" ? DSGDPP_LAYOUT_ROW_RUNS
+               : args.layout == "runs"     ? DSGDPP_LAYOUT_RUNS
+                                           : DSGDPP_LAYOUT_SHUFFLED;
   cfg.update = job.update;
   cfg.update_lambda = job.update_lambda;
   cfg.regularize = job.regularize;
@@ -507,6 +514,12 @@ int main(int argc, char** argv) {
   args.precision = get("precision", "fp32");
   args.exec = get("exec", "hogwild");
   args.launch = get("launch", "graph");
+  args.layout = get("layout", "shuffled");
+  if (args.layout != "shuffled" && args.layout != "col-runs" && args.layout != "row-runs" &&
+      args.layout != "runs") {
+    std::cerr << "unknown --layout " << args.layout << std::endl;
+    return 1;
+  }
 
   Log::info("main", "Input");
   Log::info("main", "    Input file: " + args.inputMatrixFile);

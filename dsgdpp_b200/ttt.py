@@ -23,45 +23,33 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PARAMS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "controller_params.npy")
 
 
-def main():
-    sys.path.insert(0, ROOT)
-    import bench
-    import dsgdpp_b200 as P
+def evaluate(P, wl, data, d, epochs=50, eps0=0.001, net=None, seed=777, device=0,
+             layout="shuffled", log_dump=None):
+    """Plain FP32 BoldDriver for `epochs` epochs sets the target (its final test
+    RMSE, +0.5%); then BF16 + BoldDriver and, with `net`, the controller at
+    FP32 and BF16 run until they reach it.  Returns the summary dict."""
     from dsgdpp_b200.controller import time_to_target
-
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="c2")
-    ap.add_argument("--epochs", type=int, default=50)
-    ap.add_argument("--eps", type=float, default=0.001)
-    ap.add_argument("--controller", default=PARAMS)
-    ap.add_argument("--seed", type=int, default=777)
-    ap.add_argument("--d", type=int, default=0)
-    ap.add_argument("--dump", default=None, help="write every run's trace rows here (JSON)")
-    args = ap.parse_args()
-
-    wl = bench.WORKLOADS[args.workload]
-    d = args.d or wl["d"]
-    data, _ = bench.generate(wl, args.seed)
     ntest = len(data["tvals"])
 
     def ctx_for(precision):
         l2 = wl["s"] is not None
         ctx = P.Context(P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=precision,
                                  regularize="L2" if l2 else "None",
-                                 regularize_lambda=0.05 if l2 else 0.0))
+                                 regularize_lambda=0.05 if l2 else 0.0, device=device,
+                                 layout=layout))
         ctx.set_matrix(P.TRAIN, data["rows"], data["cols"], data["vals"])
         ctx.set_matrix(P.TEST, data["trows"], data["tcols"], data["tvals"])
         ctx.set_factors(data["W0"], data["H0"])
-        ctx.seed(args.seed)
+        ctx.seed(seed)
         return ctx
 
     def rmse(loss):
         return math.sqrt(loss / ntest)
 
-    out = {"workload": wl["text"], "d": d, "epochs": args.epochs, "eps0": args.eps}
+    out = {"workload": wl["text"], "d": d, "epochs": epochs, "eps0": eps0, "layout": layout}
     with ctx_for("fp32") as ctx:
         t0 = time.perf_counter()
-        plain = ctx.run(args.epochs, "BoldDriver", args.eps)
+        plain = ctx.run(epochs, "BoldDriver", eps0)
         out["plain_fp32_s"] = time.perf_counter() - t0
     target_rmse = rmse(plain[-1]["test_loss"])
     target_loss = (target_rmse * 1.005) ** 2 * ntest
@@ -70,30 +58,53 @@ def main():
 
     dump = {"plain_fp32": plain}
     runs = [("bf16_bolddriver", "bf16", None)]
-    net = None
-    if args.controller and os.path.exists(args.controller):
-        net = P.Mlp(seed=1)
-        net.params = np.load(args.controller)
+    if net is not None:
         runs += [("fp32_controller", "fp32", net), ("bf16_controller", "bf16", net)]
     for name, prec, ctl in runs:
         with ctx_for(prec) as ctx:
             t0 = time.perf_counter()
             if ctl is None:
-                tr = ctx.run(args.epochs * 2, "BoldDriver", args.eps)
+                tr = ctx.run(epochs * 2, "BoldDriver", eps0)
                 fb = None
             else:
-                tr, fb = ctx.run_controlled(ctl, args.epochs * 2, args.eps,
-                                            target_test_loss=target_loss)
+                tr, fb = ctx.run_controlled(ctl, epochs * 2, eps0, target_test_loss=target_loss)
             wall = time.perf_counter() - t0
         dump[name] = tr
         ep, secs = time_to_target(tr, target_loss)
         out[name] = {"epochs_to_target": ep, "seconds_to_target": secs, "wall_s": wall,
                      "final_test_rmse": rmse(tr[-1]["test_loss"]), "fallbacks": fb,
                      "ratio_to_plain": (secs / out["plain_fp32_s_traced"]) if ep else None}
-    print(json.dumps(out), flush=True)
-    if args.dump:
-        with open(args.dump, "w") as f:
+    if log_dump:
+        with open(log_dump, "w") as f:
             json.dump(dump, f)
+    return out
+
+
+def main():
+    sys.path.insert(0, ROOT)
+    import bench
+    import dsgdpp_b200 as P
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--epochs", type=int, default=50)
+    ap.add_argument("--eps", type=float, default=0.001)
+    ap.add_argument("--controller", default=PARAMS)
+    ap.add_argument("--seed", type=int, default=777)
+    ap.add_argument("--d", type=int, default=0)
+    ap.add_argument("--layout", default="shuffled")
+    ap.add_argument("--dump", default=None, help="write every run's trace rows here (JSON)")
+    args = ap.parse_args()
+
+    wl = bench.WORKLOADS[args.workload]
+    data, _ = bench.generate(wl, args.seed)
+    net = None
+    if args.controller and os.path.exists(args.controller):
+        net = P.Mlp(seed=1)
+        net.params = np.load(args.controller)
+    out = evaluate(P, wl, data, args.d or wl["d"], args.epochs, args.eps, net, args.seed,
+                   layout=args.layout, log_dump=args.dump)
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":
