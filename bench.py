@@ -61,6 +61,11 @@ WORKLOADS = {
                text="480,189 x 17,770, 99M entries (+1.4M test), lognormal(4.2, 1.3) row degrees, "
                     "Zipf(0.9) columns, integer ratings 1..5 from a rank-16 truth, rank 128, "
                     "Nzsl_L2(1) update"),
+    # the controller's evaluation matrix: the 100M-entry workload's family at 300M entries
+    "c5": dict(m=2_000_000, n=1_000_000, nnz=300_000_000, nnz_test=3_000_000, rank=64, s=1.1,
+               d=64, noise=0.2,
+               text="2,000,000 x 1,000,000, 300M entries (+3M test), Zipf(1.1) rows and columns, "
+                    "rank 64, Nzsl_L2(1) update, L2(0.05) regularize, BoldDriver(0.001) first step"),
     "c1": dict(m=100_000, n=100_000, nnz=1_000_000, nnz_test=100_000, rank=10, s=None, d=4,
                noise=0.1,
                text="100,000 x 100,000, 1M uniform entries (+100k test), rank 10, "
@@ -197,7 +202,7 @@ def time_cpu_reference(data, wl, steps, warmup, threads=None, with_test=False):
     return out
 
 
-def gpu_sample_rmse(P, data, wl, precision, d, epochs, write_mode, device):
+def gpu_sample_rmse(P, data, wl, precision, d, epochs, write_mode, device, layout):
     """Test RMSE of this implementation on the CPU baseline's sample, same d,
     seed and constant step as the oracle run."""
     rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
@@ -205,7 +210,7 @@ def gpu_sample_rmse(P, data, wl, precision, d, epochs, write_mode, device):
     cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=precision,
                    update="Nzsl_L2", update_lambda=1.0, regularize="L2" if l2 else "None",
                    regularize_lambda=0.05 if l2 else 0.0, loss="Nzsl_L2", loss_lambda=1.0,
-                   write_mode=write_mode, device=device)
+                   write_mode=write_mode, device=device, layout=layout)
     with P.Context(cfg) as ctx:
         ctx.set_matrix(P.TRAIN, rows, cols, vals)
         ctx.set_matrix(P.TEST, data["trows"], data["tcols"], data["tvals"])
@@ -302,6 +307,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--write-mode", default="auto", choices=["auto", "store", "atomic"])
+    ap.add_argument("--layout", default="runs",
+                    choices=["runs", "shuffled", "col_runs", "row_runs"])
     ap.add_argument("--no-autotune", action="store_true",
                     help="use --d (default 64) instead of tuning d in 64..512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -322,13 +329,13 @@ def main():
     wl = WORKLOADS[args.workload]
     d = args.d or wl["d"]
     data, gen_s = generate(wl, args.seed + rank)
-    l2 = args.workload in ("c2", "c2s")
+    l2 = wl["s"] is not None and wl.get("kind") != "ratings"
     cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=args.precision,
                    exec="hogwild", launch="graph", update="Nzsl_L2", update_lambda=1.0,
                    regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,
                    loss="Nzsl_L2", loss_lambda=1.0, lanes_per_nnz=args.lanes,
                    vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local,
-                   write_mode=args.write_mode)
+                   write_mode=args.write_mode, layout=args.layout)
     host = {k: pinned(np.ascontiguousarray(v)) for k, v in data.items()}
     tune = None
     if not args.no_autotune and not args.d and args.workload in ("c2", "c2s"):
@@ -422,7 +429,7 @@ def main():
         cpu = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
         # the same sample, d, seed and steps on the GPU: test RMSE against the FP64 oracle
         got = gpu_sample_rmse(P, data, wl, args.precision, ref["d"], ref["epochs"],
-                              args.write_mode, local)
+                              args.write_mode, local, args.layout)
         vs_oracle = {"precision": args.precision, "epochs": ref["epochs"], "d": ref["d"],
                      "sample": "the CPU baseline's sample", "oracle_fp64_test_rmse": ref["test_rmse"],
                      "test_rmse": got, "rel_error": (got - ref["test_rmse"]) / ref["test_rmse"]}
@@ -435,7 +442,8 @@ def main():
         from dsgdpp_b200 import ttt as TT
         net = P.Mlp(device=local, seed=1)
         net.params = np.load(TT.PARAMS)
-        r = TT.evaluate(P, wl, data, d, epochs=50, eps0=eps, net=net, device=local)
+        r = TT.evaluate(P, wl, data, d, epochs=50, eps0=eps, net=net, device=local,
+                        layout=args.layout)
         net.close()
         ttt = {"target": "plain FP32 BoldDriver's test RMSE after 50 epochs, +0.5%",
                "target_test_rmse": r["target_test_rmse"], "plain_fp32_s": r["plain_fp32_s_traced"]}
@@ -452,7 +460,7 @@ def main():
             "config": {"workload": wl["text"], "d": d, "blocks": f"{d} x {2 * d}",
                        "nnz": nnz, "precision": args.precision, "exec": "hogwild",
                        "launch": "graph", "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
-                       "write_mode": args.write_mode,
+                       "write_mode": args.write_mode, "layout": args.layout,
                        "grid": grid, "parallelism": f"replicas x{world}", "autotune": tune,
                        "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -228,7 +228,7 @@ class Config:
     ctas_per_sm: int = 0
     layout_seed: int = 0x5EED5EED
     write_mode: str = "auto"
-    layout: str = "shuffled"
+    layout: str = "runs"
 
     def to_c(self) -> _Config:
         c = _Config()

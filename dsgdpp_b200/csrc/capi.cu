@@ -725,7 +725,7 @@ void dsgdpp_config_init(dsgdpp_config* c) {
   c->stratum_order = DSGDPP_STRATUM_COWOR;
   c->device = 0;
   c->layout_seed = 0x5eed5eedull;
-  c->layout = DSGDPP_LAYOUT_SHUFFLED;
+  c->layout = DSGDPP_LAYOUT_RUNS;
 }
 
 int dsgdpp_create(const dsgdpp_config* cfg, dsgdpp_ctx** out) {

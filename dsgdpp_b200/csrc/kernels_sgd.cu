@@ -131,7 +131,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   using C = typename E::C;
   constexpr int VW = E::VW;
   constexpr uint32_t kNone = 0xffffffffu;
-  constexpr int kRunCap = 8;
+  constexpr int kRunCap = 2;
   uint32_t cur = kNone;  // H row of the open run
   uint4 hv0[VPL];        // ... as loaded
   C h0[VPL][VW];         // ... unpacked as loaded
@@ -148,7 +148,9 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
     const bool valid = ri < nrec;
     // a run ends at a new column, or after kRunCap records: the row is then
     // written back and re-read, so other warps' updates of a hot row reach
-    // this group at least every kRunCap records
+    // this group at least every kRunCap records (longer runs measured less
+    // stable: on the 100M-entry Zipf matrix, runs of 4 or 8 diverged within
+    // 60 BoldDriver epochs where runs of 2 and the shuffled order did not)
     if (cur != kNone && (!valid || col != cur || (t % kRunCap) == 0)) {
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {

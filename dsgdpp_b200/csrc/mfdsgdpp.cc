@@ -47,7 +47,7 @@ struct Args {
   int sgdOrder = DSGDPP_SGD_WOR, stratumOrder = DSGDPP_STRATUM_COWOR;
   // added options
   int device = 0;
-  std::string precision = "fp32", exec = "hogwild", launch = "graph", layout = "shuffled";
+  std::string precision = "fp32", exec = "hogwild", launch = "graph", layout = "runs";
 };
 
 const char* kOptions[] = {
@@ -90,7 +90,7 @@ void usage() {
             << "  --exec arg             hogwild|replay [hogwild]\n"
             << "  --launch arg           graph|stream [graph]\n"
             << "  --layout arg           Hogwild record order in a block:\n"
-            << "                         shuffled|col-runs|row-runs|runs [shuffled]\n";
+            << "                         shuffled|col-runs|row-runs|runs [runs]\n";
 }
 
 // parse::parseArg (tools/parse.h:38-61): "Name(a,b,...)" -> name + doubles
@@ -514,7 +514,7 @@ int main(int argc, char** argv) {
   args.precision = get("precision", "fp32");
   args.exec = get("exec", "hogwild");
   args.launch = get("launch", "graph");
-  args.layout = get("layout", "shuffled");
+  args.layout = get("layout", "runs");
   if (args.layout != "shuffled" && args.layout != "col-runs" && args.layout != "row-runs" &&
       args.layout != "runs") {
     std::cerr << "unknown --layout " << args.layout << std::endl;

@@ -24,7 +24,7 @@ PARAMS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "controller_pa
 
 
 def evaluate(P, wl, data, d, epochs=50, eps0=0.001, net=None, seed=777, device=0,
-             layout="shuffled", log_dump=None):
+             layout="runs", log_dump=None):
     """Plain FP32 BoldDriver for `epochs` epochs sets the target (its final test
     RMSE, +0.5%); then BF16 + BoldDriver and, with `net`, the controller at
     FP32 and BF16 run until they reach it.  Returns the summary dict."""
@@ -92,7 +92,7 @@ def main():
     ap.add_argument("--controller", default=PARAMS)
     ap.add_argument("--seed", type=int, default=777)
     ap.add_argument("--d", type=int, default=0)
-    ap.add_argument("--layout", default="shuffled")
+    ap.add_argument("--layout", default="runs")
     ap.add_argument("--dump", default=None, help="write every run's trace rows here (JSON)")
     args = ap.parse_args()
 

@@ -121,7 +121,8 @@ typedef struct dsgdpp_trace_row {
 
 /* ---- context ------------------------------------------------------------ */
 /* Fills c with the reference defaults: WOR / COWOR, Nzsl_L2(1) update and
- * loss, regularize None, FP32 Hogwild, graph launch, auto tuning. */
+ * loss, regularize None, FP32 Hogwild, graph launch, automatic lane mapping,
+ * DSGDPP_LAYOUT_RUNS record order. */
 void dsgdpp_config_init(dsgdpp_config* c);
 /* replaces: DsgdPpJob / DsgdPpFactorizationData construction
  * (mf/sgd/dsgdpp.h:38-59, mf/sgd/dsgdpp-factorization.h:58-64) */

@@ -231,7 +231,7 @@ def test_hogwild_tracks_fp64_oracle(precision, write_mode, tol, launch):
     p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
     d = 4
     ref, ctx = _pair(p, 10, d, precision=precision, exec="hogwild", launch=launch,
-                     write_mode=write_mode)
+                     write_mode=write_mode, layout="shuffled")
     with ctx:
         ctx.seed(9)
         ref.seed(9)
