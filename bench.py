@@ -307,6 +307,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--write-mode", default="auto", choices=["auto", "store", "atomic"])
+    ap.add_argument("--launch", default="graph", choices=["graph", "persistent", "stream"],
+                    help="epoch as a graph of 2d launches, or one persistent launch")
     ap.add_argument("--layout", default="runs",
                     choices=["runs", "shuffled", "col_runs", "row_runs"])
     ap.add_argument("--no-autotune", action="store_true",
@@ -331,7 +333,7 @@ def main():
     data, gen_s = generate(wl, args.seed + rank)
     l2 = wl["s"] is not None and wl.get("kind") != "ratings"
     cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=d, precision=args.precision,
-                   exec="hogwild", launch="graph", update="Nzsl_L2", update_lambda=1.0,
+                   exec="hogwild", launch=args.launch, update="Nzsl_L2", update_lambda=1.0,
                    regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,
                    loss="Nzsl_L2", loss_lambda=1.0, lanes_per_nnz=args.lanes,
                    vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local,
@@ -385,21 +387,22 @@ def main():
     k_ms, k_launches = ctx.kernel_timing()
     ctx.set_kernel_timing(False)
     bpu = algorithmic_bytes_per_update(wl["rank"], args.precision, "Nzsl_L2")
-    bytes_per_launch = nnz * bpu / (2 * d)
+    # two epochs: 2 x 2d sub-epoch launches, or 2 persistent epoch launches
+    bytes_per_launch = 2 * nnz * bpu / max(k_launches, 1)
     avg_launch_s = k_ms / 1e3 / max(k_launches, 1)
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
     suffix = "" if args.precision == "fp32" else "_" + args.precision
-    traffic = traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", d)
+    traffic = (traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", d)
+               if args.launch != "persistent" else None)
 
     # ---- end to end through the C ABI from pinned host buffers ----
     e2e = None
     if not args.no_e2e:
         barrier(pg)
-        W = np.empty((wl["m"], wl["rank"]), np.float64)
-        H = np.empty((wl["n"], wl["rank"]), np.float64)
-        W[:] = 0.0  # fault the result pages in before the timed region
-        H[:] = 0.0
+        # results land in pinned host buffers, as the inputs come from them
+        W = pinned(np.zeros((wl["m"], wl["rank"]), np.float64))
+        H = pinned(np.zeros((wl["n"], wl["rank"]), np.float64))
         t0 = time.perf_counter()
         ctx.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
         ctx.set_matrix(P.TEST, host["trows"], host["tcols"], host["tvals"])
@@ -459,20 +462,23 @@ def main():
             "data": "synthetic (seeded; no public dataset)",
             "config": {"workload": wl["text"], "d": d, "blocks": f"{d} x {2 * d}",
                        "nnz": nnz, "precision": args.precision, "exec": "hogwild",
-                       "launch": "graph", "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
+                       "launch": args.launch, "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
                        "write_mode": args.write_mode, "layout": args.layout,
                        "grid": grid, "parallelism": f"replicas x{world}", "autotune": tune,
                        "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": peak_kind,
-                         "bytes_per_update": bpu, "kernel": "hogwild_subepoch_kernel",
+                         "bytes_per_update": bpu,
+                         "kernel": ("hogwild_epoch_kernel" if args.launch == "persistent"
+                                    else "hogwild_subepoch_kernel"),
                          "avg_launch_us": avg_launch_s * 1e6},
             "cpu_baseline": cpu,
             "test_rmse_vs_fp64_oracle": vs_oracle,
             "time_to_target": ttt,
             "e2e": e2e,
-            "gpu_launches": args.steps * (2 * d + 1 + (1 if l2 else 0)),
+            "gpu_launches": args.steps * ((2 if args.launch == "persistent" else 2 * d + 1)
+                                          + (1 if l2 else 0)),
             "clocks": clk,
             "wall_s_timed": wall, "setup_s": setup_s, "generate_s": gen_s,
         }

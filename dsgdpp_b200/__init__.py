@@ -38,7 +38,7 @@ SGD_ORDER = {"SEQ": 0, "WR": 1, "WOR": 2}
 STRATUM_ORDER = {"SEQ": 0, "RSEQ": 1, "WR": 2, "WOR": 3, "COWOR": 4}
 PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}
 EXEC = {"replay": 0, "hogwild": 1}
-LAUNCH = {"stream": 0, "graph": 1}
+LAUNCH = {"stream": 0, "graph": 1, "persistent": 2}
 WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
 LAYOUT = {"shuffled": 0, "col_runs": 1, "row_runs": 2, "runs": 3}
 TRAIN, TEST = 0, 1

@@ -69,6 +69,10 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
   if (per_sm <= 0)
     throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
                                       ", vecs_per_lane=" + std::to_string(vecs));
+  if (c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT) {
+    per_sm = hogwild_epoch_ctas_per_sm(c->cfg.precision, lanes, vecs, c->d);
+    if (per_sm <= 0) throw Error(DSGDPP_E_INVALID, "no persistent epoch kernel for this rank");
+  }
   if (c->cfg.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm);
   c->grid = (uint32_t)(per_sm * c->num_sms);
 }
@@ -89,7 +93,8 @@ void validate_config(const dsgdpp_config* c) {
     throw Error(DSGDPP_E_UNSUPPORTED, "replay mode runs FP64 factors only");
   if (c->exec == DSGDPP_EXEC_REPLAY && c->rank > 256)
     throw Error(DSGDPP_E_UNSUPPORTED, "replay mode supports rank <= 256");
-  if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH)
+  if (c->launch != DSGDPP_LAUNCH_STREAM && c->launch != DSGDPP_LAUNCH_GRAPH &&
+      c->launch != DSGDPP_LAUNCH_PERSISTENT)
     throw Error(DSGDPP_E_INVALID, "unknown launch form");
   if (c->write_mode < 0 || c->write_mode > 2) throw Error(DSGDPP_E_INVALID, "unknown write mode");
   if (c->layout < 0 || c->layout > 3) throw Error(DSGDPP_E_INVALID, "unknown layout");
@@ -179,6 +184,19 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   c->atomic_writes = cfg->write_mode == DSGDPP_WRITE_ATOMIC ||
                      (cfg->write_mode == DSGDPP_WRITE_AUTO && !cfg->truncate);
   c->layout_key = resolve_layout(cfg->layout, cfg->m, cfg->n);
+  if (cfg->launch == DSGDPP_LAUNCH_PERSISTENT) {
+    if (cfg->exec != DSGDPP_EXEC_HOGWILD || !c->atomic_writes ||
+        c->layout_key == kLayoutShuffled || cfg->sgd_order == DSGDPP_SGD_WR)
+      throw Error(DSGDPP_E_UNSUPPORTED,
+                  "the persistent epoch runs the Hogwild path with atomic writes, a run layout "
+                  "and the SEQ or WOR order");
+    c->d_done = dalloc<uint32_t>((size_t)d2 * d, "segment counters");
+    c->d_dep_col = dalloc<int32_t>((size_t)d2 * d, "column dependencies");
+    c->h_dep_col = halloc<int32_t>((size_t)d2 * d, "column dependencies");
+    c->d_ticket = dalloc<uint32_t>(2, "ticket");  // [0] ticket, [1] error flag
+    c->h_error = halloc<uint32_t>(1, "error flag");
+    *c->h_error = 0;
+  }
   if (cfg->exec == DSGDPP_EXEC_HOGWILD) choose_hogwild_shape(c);
 }
 
@@ -196,6 +214,8 @@ void destroy_impl(dsgdpp_ctx* c) {
   hfree(c->h_schedule); dfree(c->d_schedule); hfree(c->h_params); dfree(c->d_params);
   hfree(c->h_sigma); dfree(c->d_sigma); hfree(c->h_scales); dfree(c->d_scales);
   dfree(c->d_segs); dfree(c->d_counters); dfree(c->d_launches);
+  dfree(c->d_done); dfree(c->d_dep_col); hfree(c->h_dep_col); dfree(c->d_ticket);
+  hfree(c->h_error);
   hfree(c->h_positions); dfree(c->d_positions); hfree(c->h_pos_offset); dfree(c->d_pos_offset);
   hfree(c->h_mask); dfree(c->d_mask);
   dfree(c->d_partials); dfree(c->d_out); hfree(c->h_out);
@@ -438,6 +458,19 @@ void fill_sigma(dsgdpp_ctx* c, double eps) {
   c->h_scales[d2] = (float)sw;
 }
 
+// persistent epoch: for segment (s, i) the last earlier segment of the epoch
+// that worked on the same column block of H (flat index s2 * d + j), or -1
+void fill_deps(dsgdpp_ctx* c) {
+  const uint32_t d = c->d, d2 = 2 * d;
+  std::vector<int32_t> last(d2, -1);
+  for (uint32_t s = 0; s < d2; ++s) {
+    for (uint32_t i = 0; i < d; ++i)
+      c->h_dep_col[(size_t)s * d + i] = last[c->h_schedule[(size_t)s * d + i]];
+    for (uint32_t i = 0; i < d; ++i)
+      last[c->h_schedule[(size_t)s * d + i]] = (int32_t)(s * d + i);
+  }
+}
+
 bool lazy_l2(const dsgdpp_ctx* c) {
   return c->cfg.regularize == DSGDPP_REGULARIZE_L2 && c->cfg.regularize_lambda != 0;
 }
@@ -459,6 +492,13 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   SegBuildArgs sb{c->d_params, c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr,
                   c->d_segs, c->d_counters, d};
   check_cuda(launch_build_segments(sb, st), "build_segments");
+  const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
+  if (persistent) {
+    check_cuda(cudaMemcpyAsync(c->d_dep_col, c->h_dep_col, (size_t)d2 * d * 4,
+                               cudaMemcpyHostToDevice, st), "H2D dependencies");
+    check_cuda(cudaMemsetAsync(c->d_done, 0, (size_t)d2 * d * 4, st), "segment counters");
+    check_cuda(cudaMemsetAsync(c->d_ticket, 0, 8, st), "ticket");
+  }
   HogwildArgs a{};
   const DevMatrix& M = c->mat[0];
   a.row = M.row; a.col = M.col; a.val = M.val;
@@ -478,12 +518,21 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.atomic = c->atomic_writes;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
-  for (uint32_t s = 0; s < d2; ++s) {
+  if (persistent) {
+    EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d};
+    if (prof) check_cuda(cudaEventRecord(c->prof_ev[0], st), "event");
+    check_cuda(launch_hogwild_epoch(c->cfg.precision, c->lanes, c->vecs, a, dp, c->grid, st),
+               "hogwild_epoch");
+    if (prof) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
+    check_cuda(cudaMemcpyAsync(c->h_error, c->d_ticket + 1, 4, cudaMemcpyDeviceToHost, st),
+               "D2H error flag");
+  }
+  for (uint32_t s = 0; s < d2 && !persistent; ++s) {
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[s], st), "event");
     check_cuda(launch_hogwild(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
                "hogwild_subepoch");
   }
-  if (prof) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
+  if (prof && !persistent) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
   if (l2)
     check_cuda(launch_normalize(c->cfg.precision, c->W, c->H, c->cfg.m, c->cfg.n, c->rp,
                                 c->d_scales, c->d_off2, d2, st), "normalize");
@@ -494,6 +543,13 @@ void collect_profile(dsgdpp_ctx* c) {
   c->prof_pending = false;
   const uint32_t d2 = 2 * c->d;
   check_cuda(cudaEventSynchronize(c->prof_ev[d2]), "event sync");
+  if (c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT) {  // one launch per epoch
+    float f = 0;
+    check_cuda(cudaEventElapsedTime(&f, c->prof_ev[0], c->prof_ev[d2]), "elapsed");
+    c->prof_ms += f;
+    c->prof_launches += 1;
+    return;
+  }
   for (uint32_t s = 0; s < d2; ++s) {
     float f = 0;
     check_cuda(cudaEventElapsedTime(&f, c->prof_ev[s], c->prof_ev[s + 1]), "elapsed");
@@ -504,10 +560,12 @@ void collect_profile(dsgdpp_ctx* c) {
 
 void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
   if (lazy_l2(c)) fill_sigma(c, eps);
+  const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
+  if (persistent) fill_deps(c);
   cudaStream_t st = c->stream;
   collect_profile(c);
   check_cuda(cudaEventRecord(c->ev_begin, st), "event");
-  if (c->cfg.launch == DSGDPP_LAUNCH_GRAPH && !c->profiling) {
+  if ((c->cfg.launch == DSGDPP_LAUNCH_GRAPH || persistent) && !c->profiling) {
     if (!c->graph_exec) {
       cudaGraph_t g = nullptr;
       check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
@@ -531,6 +589,13 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
   check_cuda(cudaEventRecord(c->ev_end, st), "event");
   check_cuda(cudaEventRecord(c->ev_inputs, st), "event");
   c->epoch_timed = true;
+  if (persistent) {  // a dependency wait that gave up leaves the epoch incomplete
+    check_cuda(cudaEventSynchronize(c->ev_end), "event sync");
+    if (*c->h_error) {
+      *c->h_error = 0;
+      throw Error(DSGDPP_E_CUDA, "persistent epoch: a dependency wait gave up");
+    }
+  }
 }
 
 void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {

@@ -105,6 +105,12 @@ struct dsgdpp_ctx {
   Segment* d_segs = nullptr;
   dsgdpp::LaunchDesc* d_launches = nullptr;
   uint32_t* d_counters = nullptr;
+  // persistent epoch
+  uint32_t* d_done = nullptr;     // [2d][d] finished chunks per segment
+  int32_t* d_dep_col = nullptr;   // [2d][d] last earlier segment on the same H block
+  int32_t* h_dep_col = nullptr;
+  uint32_t* d_ticket = nullptr;   // [0] chunk ticket, [1] error flag
+  uint32_t* h_error = nullptr;    // error flag read back after each epoch
   // replay
   uint32_t* h_positions = nullptr;
   uint32_t* d_positions = nullptr;

@@ -75,6 +75,18 @@ struct SegBuildArgs {
   uint32_t d;
 };
 
+// Persistent epoch: one launch walks every sub-epoch; a chunk of segment
+// (s, i) starts once segment (s-1, i) -- the task's previous block, on the same
+// rows of W -- and the last earlier segment on the same column block of H
+// (dep_col) have finished all their chunks.
+struct EpochDeps {
+  const int32_t* dep_col;  // [2d][d]: s2 * d + j of that segment, or -1
+  uint32_t* done;          // [2d][d] chunks finished per segment (zeroed per epoch)
+  uint32_t* ticket;        // chunks handed out (zeroed per epoch)
+  uint32_t* error;         // set when a dependency wait gave up
+  uint32_t d;
+};
+
 // ---- launchers (return cudaError_t) -------------------------------------------
 cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);
 cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
@@ -82,6 +94,10 @@ cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const H
 // CTAs per SM that the Hogwild kernel sustains for this configuration
 int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
                         uint32_t smem_segs, bool runs);
+// the persistent epoch (column / row runs, atomic writes, SEQ or WOR order)
+cudaError_t launch_hogwild_epoch(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
+                                 const EpochDeps& dp, uint32_t grid, cudaStream_t st);
+int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d);
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
 // RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,

@@ -143,7 +143,7 @@ __device__ __forceinline__ double nzsl_lanes(const uint32_t* row, const uint32_t
 }
 
 template <typename T, int LPN, int VPL>
-__global__ void __launch_bounds__(256, VPL == 1 ? 3 : 2) nzsl_lanes_kernel(const uint32_t* row, const uint32_t* col,
+__global__ void __launch_bounds__(256, 3) nzsl_lanes_kernel(const uint32_t* row, const uint32_t* col,
                                                          const float* val, uint64_t nnz,
                                                          const T* W, const T* H, uint32_t r,
                                                          uint32_t rp, double* partials) {
@@ -177,7 +177,7 @@ __device__ __forceinline__ double nzsl_exact(const uint32_t* row, const uint32_t
 // One CTA per chunk of a problem's range; owner_sums then adds each problem's
 // chunk partials in chunk order, so every per-problem sum is deterministic.
 template <typename T, int LPN, int VPL>
-__global__ void __launch_bounds__(256, VPL == 1 ? 3 : 2) nzsl_chunks_kernel(const RangeChunk* chunks,
+__global__ void __launch_bounds__(256, 3) nzsl_chunks_kernel(const RangeChunk* chunks,
                                                           const uint32_t* row, const uint32_t* col,
                                                           const float* val, const T* W,
                                                           const T* H, uint32_t r, uint32_t rp,

@@ -118,7 +118,15 @@ __device__ __forceinline__ void write_vec(T* p, const uint4& old,
 // sequential SGD -- and writes it back once when the run ends.  Every
 // record's W row is read and written as in the shuffled path.  With the sides
 // swapped by the host (runs of one W row) the same code caches the W row.
-template <typename T, int LPN, int VPL, bool ATOMIC>
+// 16-byte factor load; CG reads through L2 only (the persistent epoch, whose
+// chunks of different sub-epochs share an SM's L1 within one launch)
+template <bool CG>
+__device__ __forceinline__ uint4 ld_vec(const void* p) {
+  if constexpr (CG) return __ldcg(reinterpret_cast<const uint4*>(p));
+  else return *reinterpret_cast<const uint4*>(p);
+}
+
+template <typename T, int LPN, int VPL, bool ATOMIC, bool CG = false>
 __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint64_t rb,
                                           uint32_t nrec, uint32_t my_row, uint32_t my_col,
                                           typename Elem<T>::C my_x, typename Elem<T>::C my_a,
@@ -165,8 +173,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        hv0[v] = e0 < a.rp ? *reinterpret_cast<const uint4*>(H + (size_t)col * a.rp + e0)
-                           : make_uint4(0, 0, 0, 0);
+        hv0[v] = e0 < a.rp ? ld_vec<CG>(H + (size_t)col * a.rp + e0) : make_uint4(0, 0, 0, 0);
         E::unpack(hv0[v], h0[v]);
 #pragma unroll
         for (int e = 0; e < VW; ++e) hf[v][e] = h0[v][e];
@@ -180,8 +187,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
 #pragma unroll
     for (int v = 0; v < VPL; ++v) {
       const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-      wv[v] = (valid && e0 < a.rp) ? *reinterpret_cast<const uint4*>(wp + e0)
-                                   : make_uint4(0, 0, 0, 0);
+      wv[v] = (valid && e0 < a.rp) ? ld_vec<CG>(wp + e0) : make_uint4(0, 0, 0, 0);
       E::unpack(wv[v], wf[v]);
       if (valid) {
 #pragma unroll
@@ -408,6 +414,136 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
         }
       }
     }
+  }
+}
+
+// A dependency wait polls for about 8 s at most, then the epoch gives up (error
+// flag) instead of waiting for ever.
+constexpr uint32_t kWaitLimit = 1u << 23;
+
+__device__ __forceinline__ uint32_t load_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// polls until *done >= need; false if it gave up (or another warp did)
+__device__ __forceinline__ bool wait_done(const uint32_t* done, uint32_t need, uint32_t* error) {
+  uint32_t it = 0;
+  while (load_acquire(done) < need) {
+    if (++it >= kWaitLimit || *reinterpret_cast<volatile uint32_t*>(error)) {
+      atomicExch(error, 1u);
+      return false;
+    }
+    __nanosleep(1000);
+  }
+  return true;
+}
+
+// One launch per epoch.  Warps take chunk tickets in sub-epoch order (the
+// chunks of sub-epoch s in the same order as the launch-per-sub-epoch form); a
+// chunk of segment (s, i) first waits for segment (s-1, i) and for
+// dep_col[s][i].  Every chunk waited for holds a smaller ticket, and tickets
+// go to running warps only, so the waits end; each is bounded anyway.  A
+// finished chunk publishes its writes (fence) before it counts itself done.
+template <typename T, int LPN, int VPL>
+__global__ void __launch_bounds__(256) hogwild_epoch_kernel(HogwildArgs a, EpochDeps dp) {
+  using E = Elem<T>;
+  using C = typename E::C;
+  extern __shared__ __align__(16) uint32_t prefix[];  // [2d + 1] chunk offsets per sub-epoch
+  const uint32_t d = dp.d, nsub = 2 * d;
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t s = 0; s < nsub; ++s) {
+      prefix[s] = acc;
+      const LaunchDesc L = a.launches[s];
+      acc += a.segs[L.seg_begin + L.nseg].chunk_begin;
+    }
+    prefix[nsub] = acc;
+  }
+  __syncthreads();
+  const uint32_t total = prefix[nsub];
+  const EpochParams ep = *a.params;
+  const C lambda2 = (C)(2.0 * a.lambda);
+  const C tmin = (C)a.tmin, tmax = (C)a.tmax;
+  const C* inv1 = reinterpret_cast<const C*>(a.inv1);
+  const C* inv2 = reinterpret_cast<const C*>(a.inv2);
+  const C* vals = reinterpret_cast<const C*>(a.val);
+  T* W = reinterpret_cast<T*>(a.W);
+  T* H = reinterpret_cast<T*>(a.H);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t grp = lane / LPN, gl = lane % LPN;
+  uint32_t ready_seg = 0xffffffffu;  // segment whose dependencies this warp saw met
+
+  for (;;) {
+    uint32_t tk = total;
+    if (lane == 0 && !*reinterpret_cast<volatile uint32_t*>(dp.error)) tk = atomicAdd(dp.ticket, 1u);
+    tk = __shfl_sync(kFullMask, tk, 0);
+    if (tk >= total) break;
+    uint32_t s = 0, hs = nsub - 1;  // the sub-epoch: the last s with prefix[s] <= tk
+    while (s < hs) {
+      const uint32_t mid = (s + hs + 1) >> 1;
+      if (prefix[mid] <= tk) s = mid; else hs = mid - 1;
+    }
+    const uint32_t cnt_s = prefix[s + 1] - prefix[s], lc = tk - prefix[s];
+    const LaunchDesc L = a.launches[s];
+    const Segment* seg = a.segs + L.seg_begin;
+    uint32_t pc = lc;
+    if (a.sgd_order == 2) {  // WOR: the affine chunk permutation of sub-epoch s
+      const uint64_t h =
+          mix64(((uint64_t)ep.key0 << 32 | ep.key1) ^ ((uint64_t)s << 17) ^ ep.epoch);
+      const uint64_t mulA = kPrimes[h & 7u] % cnt_s, addB = (h >> 8) % cnt_s;
+      pc = (uint32_t)((mulA * lc + addB) % cnt_s);
+    }
+    uint32_t lo = 0, hi = L.nseg - 1;  // the last segment with chunk_begin <= pc
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(&seg[mid].chunk_begin) <= pc) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t me = s * d + lo;
+    if (me != ready_seg) {
+      uint32_t ok = 1;
+      if (lane == 0 && s > 0) {
+        const Segment* ps = a.segs + a.launches[s - 1].seg_begin;
+        ok = wait_done(dp.done + (me - d), ps[lo + 1].chunk_begin - ps[lo].chunk_begin, dp.error);
+        const int32_t dc = dp.dep_col[me];
+        if (ok && dc >= 0) {
+          const uint32_t ds = (uint32_t)dc / d, dj = (uint32_t)dc % d;
+          const Segment* qs = a.segs + a.launches[ds].seg_begin;
+          ok = wait_done(dp.done + dc, qs[dj + 1].chunk_begin - qs[dj].chunk_begin, dp.error);
+        }
+      }
+      if (!__shfl_sync(kFullMask, ok, 0)) break;
+      __threadfence();
+      ready_seg = me;
+    }
+    const Segment sg = seg[lo];
+    const uint32_t cin = pc - sg.chunk_begin;
+    const uint64_t rb = sg.rec_begin + (uint64_t)cin * kChunk;
+    const uint32_t nrec = min((uint32_t)kChunk, sg.count - cin * kChunk);
+    const C eps = (C)sg.eps, f2 = eps * lambda2;
+    const C cwh = (C)sg.cwh;
+    const C rw = (C)(a.swap_sides ? sg.rho_h : sg.rho_w);
+    const C rh = (C)(a.swap_sides ? sg.rho_w : sg.rho_h);
+    uint32_t my_row = 0, my_col = 0;
+    C my_x = 0, my_a = 0, my_b = 0;
+    if (lane < nrec) {
+      my_row = a.row[rb + lane];
+      my_col = a.col[rb + lane];
+      my_x = vals[rb + lane];
+      if (a.update == kUpdNzslL2) {
+        my_a = f2 * inv1[my_row];
+        my_b = f2 * inv2[my_col];
+      } else if (a.update == kUpdNzslNzl2) {
+        my_a = f2;
+        my_b = f2;
+      }
+    }
+    run_chunk<T, LPN, VPL, true, true>(a, W, H, rb, nrec, my_row, my_col, my_x, my_a, my_b, eps,
+                                       cwh, rw, rh, tmin, tmax, ep, grp, gl);
+    __threadfence();  // this lane's writes, before the chunk counts as done
+    __syncwarp();
+    if (lane == 0) atomicAdd(dp.done + me, 1u);
   }
 }
 
@@ -758,6 +894,50 @@ cudaError_t launch_scale_rows(int precision, void* W, uint64_t wrows, void* H, u
     scale_rows_kernel<__nv_bfloat16><<<1184, 256, 0, st>>>(
         (__nv_bfloat16*)W, wrows, (__nv_bfloat16*)H, hrows, rp, w_slot, h_slot, scales);
   return cudaGetLastError();
+}
+
+}  // namespace dsgdpp
+
+namespace dsgdpp {
+namespace {
+
+template <typename T>
+void* pick_epoch(uint32_t lanes, uint32_t vecs) {
+#define DSGDPP_CASE(L, V) \
+  if (lanes == L && vecs == V) return reinterpret_cast<void*>(&hogwild_epoch_kernel<T, L, V>);
+  DSGDPP_CASE(2, 1) DSGDPP_CASE(4, 1) DSGDPP_CASE(8, 1) DSGDPP_CASE(16, 1) DSGDPP_CASE(32, 1)
+  DSGDPP_CASE(2, 2) DSGDPP_CASE(4, 2) DSGDPP_CASE(8, 2) DSGDPP_CASE(16, 2) DSGDPP_CASE(32, 2)
+  DSGDPP_CASE(32, 4)
+#undef DSGDPP_CASE
+  return nullptr;
+}
+
+void* epoch_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs) {
+  if (precision == kFp64) return pick_epoch<double>(lanes, vecs);
+  if (precision == kFp32) return pick_epoch<float>(lanes, vecs);
+  return pick_epoch<__nv_bfloat16>(lanes, vecs);
+}
+
+}  // namespace
+
+int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d) {
+  void* fn = epoch_kernel_ptr(precision, lanes, vecs);
+  if (!fn) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(uint32_t) * (2 * d + 1)) !=
+      cudaSuccess)
+    return 0;
+  return n;
+}
+
+cudaError_t launch_hogwild_epoch(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
+                                 const EpochDeps& dp, uint32_t grid, cudaStream_t st) {
+  void* fn = epoch_kernel_ptr(precision, lanes, vecs);
+  if (!fn || a.atomic == 0 || a.runs == 0) return cudaErrorInvalidValue;
+  HogwildArgs args = a;
+  EpochDeps deps = dp;
+  void* params[] = {&args, &deps};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(uint32_t) * (2 * dp.d + 1), st);
 }
 
 }  // namespace dsgdpp

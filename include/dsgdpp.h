@@ -69,6 +69,10 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 /* launch form of an epoch */
 #define DSGDPP_LAUNCH_STREAM 0 /* 2d kernel launches per epoch */
 #define DSGDPP_LAUNCH_GRAPH 1  /* the epoch captured once as a CUDA graph and replayed */
+#define DSGDPP_LAUNCH_PERSISTENT 2 /* one launch per epoch (graph-captured): a block of
+                                      sub-epoch s starts when the blocks it depends on in
+                                      earlier sub-epochs are done (Hogwild, atomic writes,
+                                      a run layout, SEQ or WOR order) */
 /* how a Hogwild update is written back */
 #define DSGDPP_WRITE_AUTO 0   /* ATOMIC without truncation, else STORE */
 #define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */

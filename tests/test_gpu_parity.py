@@ -309,3 +309,41 @@ def test_epoch_time_is_reported():
     with ctx:
         ctx.epoch(0.01)
         assert ctx.last_epoch_ms() > 0
+
+
+# One persistent launch per epoch: a block starts when the blocks it depends on
+# (its task's previous block, the previous block on its column block) are done.
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.005), ("fp32", 0.005), ("bf16", 0.01)])
+@pytest.mark.parametrize("sgd_order", ["SEQ", "WOR"])
+@pytest.mark.parametrize("layout", ["col_runs", "row_runs"])
+def test_persistent_epoch_tracks_fp64_oracle(precision, tol, sgd_order, layout):
+    p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
+    ref, ctx = _pair(p, 10, 4, precision=precision, exec="hogwild", launch="persistent",
+                     layout=layout, sgd_order=sgd_order)
+    with ctx:
+        ctx.seed(9)
+        ref.seed(9)
+        for _ in range(8):
+            ctx.epoch(0.01)
+            ref.epoch(0.01)
+        got = _rmse(ctx, len(p.tvals))
+        want = float(np.sqrt(ref.nzsl(1) / len(p.tvals)))
+        assert abs(got - want) <= tol * want, (got, want)
+
+
+def test_persistent_epoch_kernel_timing_and_unsupported_forms():
+    p = _problem(m=3000, n=2000, nnz=60000, ntest=100, r=12)
+    cfg = P.Config(m=p.m, n=p.n, rank=12, d=8, launch="persistent", layout="col_runs")
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_factors(p.W0, p.H0)
+        ctx.set_kernel_timing(True)
+        for _ in range(3):
+            ctx.epoch(0.01)
+        ms, launches = ctx.kernel_timing()
+        assert launches == 3 and ms > 0
+    for bad in (dict(sgd_order="WR"), dict(write_mode="store"), dict(layout="shuffled"),
+                dict(exec="replay", precision="fp64")):
+        with pytest.raises(P.DsgdppError):
+            P.Context(P.Config(m=p.m, n=p.n, rank=12, d=8, launch="persistent",
+                               **dict(dict(layout="col_runs"), **bad)))
