@@ -347,3 +347,23 @@ def test_persistent_epoch_kernel_timing_and_unsupported_forms():
         with pytest.raises(P.DsgdppError):
             P.Context(P.Config(m=p.m, n=p.n, rank=12, d=8, launch="persistent",
                                **dict(dict(layout="col_runs"), **bad)))
+
+
+def test_small_cpu_workload_replay_run_matches_oracle():
+    # the reference's CPU-runnable case at full size: 100,000 x 100,000, 1M
+    # uniform entries (+100k test), rank 10, FP64, Nzsl_L2(1), d = 4 (4 x 8
+    # blocks), BoldDriver(0.001); 3 epochs of the 50 (the oracle is sequential)
+    p = synth.make(100_000, 100_000, 1_000_000, 100_000, rank_true=10, r=10, noise=0.1, seed=2024)
+    ref, ctx = _pair(p, 10, 4, precision="fp64", exec="replay", launch="graph")
+    with ctx:
+        ctx.seed(1)
+        ref.seed(1)
+        tr = ctx.run(3, "BoldDriver", 0.001)
+        rt = ref.run(3, "BoldDriver", 0.001)
+        for k, row in enumerate(tr):
+            assert row["loss"] == pytest.approx(rt[k, 0], rel=LOSS_RTOL)
+            assert row["test_loss"] == pytest.approx(rt[k, 1], rel=LOSS_RTOL)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
