@@ -41,6 +41,7 @@ EXEC = {"replay": 0, "hogwild": 1}
 LAUNCH = {"stream": 0, "graph": 1, "persistent": 2}
 WRITE_MODE = {"auto": 0, "store": 1, "atomic": 2}
 LAYOUT = {"shuffled": 0, "col_runs": 1, "row_runs": 2, "runs": 3}
+METHOD = {"dsgdpp": 0, "dsgd": 1}
 TRAIN, TEST = 0, 1
 DECAY = {"Const": 0, "BoldDriver": 1}
 
@@ -62,7 +63,7 @@ class _Config(C.Structure):
         ("sgd_order", C.c_int32), ("stratum_order", C.c_int32), ("device", C.c_int32),
         ("lanes_per_nnz", C.c_uint32), ("vecs_per_lane", C.c_uint32),
         ("ctas_per_sm", C.c_uint32), ("layout_seed", C.c_uint64), ("write_mode", C.c_int32),
-        ("layout", C.c_int32),
+        ("layout", C.c_int32), ("method", C.c_int32),
     ]
 
 
@@ -229,6 +230,7 @@ class Config:
     layout_seed: int = 0x5EED5EED
     write_mode: str = "auto"
     layout: str = "runs"
+    method: str = "dsgdpp"
 
     def to_c(self) -> _Config:
         c = _Config()
@@ -249,6 +251,7 @@ class Config:
         c.ctas_per_sm, c.layout_seed = self.ctas_per_sm, self.layout_seed
         c.write_mode = WRITE_MODE[self.write_mode]
         c.layout = LAYOUT[self.layout]
+        c.method = METHOD[self.method]
         return c
 
 
@@ -313,9 +316,11 @@ class Context:
                     "get_factors")
 
     def block_nnz(self, which: int = TRAIN) -> np.ndarray:
-        out = np.empty(2 * self.config.d * self.config.d, np.uint64)
+        d = self.config.d
+        nb2 = d if self.config.method == "dsgd" else 2 * d  # column blocks
+        out = np.empty(d * nb2, np.uint64)
         self._check(lib.dsgdpp_block_nnz(self._h, which, _ptr(out, C.c_uint64)), "block_nnz")
-        return out.reshape(self.config.d, 2 * self.config.d)
+        return out.reshape(d, nb2)
 
     def nnz12(self):
         a = np.empty(self.config.m, np.uint64)

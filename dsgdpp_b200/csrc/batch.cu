@@ -175,6 +175,8 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
   if (common->exec != DSGDPP_EXEC_HOGWILD)
     throw Error(DSGDPP_E_UNSUPPORTED, "the batched form runs the Hogwild path");
   if (common->truncate) throw Error(DSGDPP_E_UNSUPPORTED, "the batched form does not truncate");
+  if (common->method != DSGDPP_METHOD_DSGDPP)
+    throw Error(DSGDPP_E_UNSUPPORTED, "the batched form runs DSGD++ (d x 2d blocks)");
   if (common->loss == DSGDPP_LOSS_NZSL_NZL2)
     throw Error(DSGDPP_E_UNSUPPORTED, "the batched form computes the Nzsl and Nzsl_L2 losses");
   b->cfg = *common;

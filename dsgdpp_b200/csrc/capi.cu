@@ -51,6 +51,19 @@ int resolve_layout(int layout, uint64_t m, uint64_t n) {
   }
 }
 
+// The master generator's draws of one epoch: DsgdPpRunner::epoch
+// (mf/sgd/dsgdpp_impl.h:289-344) or DsgdRunner::epoch (mf/sgd/dsgd_impl.h:
+// 328-350: the d x d schedule of computeDsgdSchedule, then one seed per task).
+void draw_epoch(dsgdpp_ctx* c, uint32_t* sched, uint32_t* seeds) {
+  if (c->cfg.method == DSGDPP_METHOD_DSGD) {
+    const std::vector<uint32_t> S = dsgd_schedule(1, c->d, c->cfg.stratum_order, c->master);
+    std::copy(S.begin(), S.end(), sched);
+    for (uint32_t id = 0; id < c->d; ++id) seeds[id] = c->master.next();
+  } else {
+    dsgdpp_schedule(c->master, c->d, c->cfg.stratum_order, sched, seeds);
+  }
+}
+
 void choose_hogwild_shape(dsgdpp_ctx* c) {
   const uint32_t nvec = c->rp / vec_width(c->cfg.precision);
   uint32_t lanes = c->cfg.lanes_per_nnz, vecs = c->cfg.vecs_per_lane;
@@ -70,7 +83,7 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
     throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" + std::to_string(lanes) +
                                       ", vecs_per_lane=" + std::to_string(vecs));
   if (c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT) {
-    per_sm = hogwild_epoch_ctas_per_sm(c->cfg.precision, lanes, vecs, c->d);
+    per_sm = hogwild_epoch_ctas_per_sm(c->cfg.precision, lanes, vecs, c->nb2);
     if (per_sm <= 0) throw Error(DSGDPP_E_INVALID, "no persistent epoch kernel for this rank");
   }
   if (c->cfg.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm);
@@ -83,8 +96,13 @@ void validate_config(const dsgdpp_config* c) {
   if (c->m > 0xFFFFFFFFull || c->n > 0xFFFFFFFFull)
     throw Error(DSGDPP_E_INVALID, "m and n must fit in 32 bits");
   if (c->d < 1 || c->d > 1024) throw Error(DSGDPP_E_INVALID, "d must be in [1, 1024]");
-  if ((uint64_t)2 * c->d > c->n || c->d > c->m)
-    throw Error(DSGDPP_E_INVALID, "the d x 2d blocking needs m >= d and n >= 2d");
+  if (c->method != DSGDPP_METHOD_DSGDPP && c->method != DSGDPP_METHOD_DSGD)
+    throw Error(DSGDPP_E_INVALID, "unknown method");
+  const uint64_t nb2 = c->method == DSGDPP_METHOD_DSGD ? c->d : 2ull * c->d;
+  if (nb2 > c->n || c->d > c->m)
+    throw Error(DSGDPP_E_INVALID, c->method == DSGDPP_METHOD_DSGD
+                                      ? "the d x d blocking needs m >= d and n >= d"
+                                      : "the d x 2d blocking needs m >= d and n >= 2d");
   if (c->rank < 1) throw Error(DSGDPP_E_INVALID, "rank must be positive");
   if (c->precision < 0 || c->precision > 2) throw Error(DSGDPP_E_INVALID, "unknown precision");
   if (c->exec != DSGDPP_EXEC_REPLAY && c->exec != DSGDPP_EXEC_HOGWILD)
@@ -121,10 +139,11 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg->device),
              "cudaDeviceGetAttribute");
   c->d = cfg->d;
+  c->nb2 = cfg->method == DSGDPP_METHOD_DSGD ? cfg->d : 2 * cfg->d;
   c->r = cfg->rank;
   const uint32_t vw = vec_width(cfg->precision);
   c->rp = (c->r + vw - 1) / vw * vw;
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   c->off1 = block_offsets(cfg->m, d);
   c->off1.push_back(cfg->m);
   c->off2 = block_offsets(cfg->n, d2);
@@ -269,7 +288,7 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   check_cuda(cudaStreamSynchronize(c->stream), "sync");
   release_graph(c);
   cudaStream_t st = c->stream;
-  const uint32_t d = c->d, d2 = 2 * d, nblocks = d * d2;
+  const uint32_t d = c->d, d2 = c->nb2, nblocks = d * d2;
   uint64_t mB = 0, nB = 0;
   for (uint32_t b = 0; b < d; ++b) mB = std::max(mB, c->off1[b + 1] - c->off1[b]);
   for (uint32_t b = 0; b < d2; ++b) nB = std::max(nB, c->off2[b + 1] - c->off2[b]);
@@ -433,7 +452,7 @@ void fill_epoch_params(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
 // scale of H block b2 is f^(earlier visits of b2); both are folded into the
 // update and applied to the factors once at the end of the epoch.
 void fill_sigma(dsgdpp_ctx* c, double eps) {
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   const bool l2 = c->cfg.regularize == DSGDPP_REGULARIZE_L2 && c->cfg.regularize_lambda != 0;
   double factor = 1.0;
   if (l2) {
@@ -461,7 +480,7 @@ void fill_sigma(dsgdpp_ctx* c, double eps) {
 // persistent epoch: for segment (s, i) the last earlier segment of the epoch
 // that worked on the same column block of H (flat index s2 * d + j), or -1
 void fill_deps(dsgdpp_ctx* c) {
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   std::vector<int32_t> last(d2, -1);
   for (uint32_t s = 0; s < d2; ++s) {
     for (uint32_t i = 0; i < d; ++i)
@@ -477,7 +496,7 @@ bool lazy_l2(const dsgdpp_ctx* c) {
 
 void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   cudaStream_t st = c->stream;
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   const bool l2 = lazy_l2(c);
   check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
                              cudaMemcpyHostToDevice, st), "H2D schedule");
@@ -490,7 +509,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
                                st), "H2D scales");
   }
   SegBuildArgs sb{c->d_params, c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr,
-                  c->d_segs, c->d_counters, d};
+                  c->d_segs, c->d_counters, d, d2};
   check_cuda(launch_build_segments(sb, st), "build_segments");
   const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
   if (persistent) {
@@ -519,7 +538,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
   if (persistent) {
-    EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d};
+    EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d, d2};
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[0], st), "event");
     check_cuda(launch_hogwild_epoch(c->cfg.precision, c->lanes, c->vecs, a, dp, c->grid, st),
                "hogwild_epoch");
@@ -541,7 +560,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
 void collect_profile(dsgdpp_ctx* c) {
   if (!c->prof_pending) return;
   c->prof_pending = false;
-  const uint32_t d2 = 2 * c->d;
+  const uint32_t d2 = c->nb2;
   check_cuda(cudaEventSynchronize(c->prof_ev[d2]), "event sync");
   if (c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT) {  // one launch per epoch
     float f = 0;
@@ -599,7 +618,7 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
 }
 
 void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   const DevMatrix& M = c->mat[0];
   // point orders, one generator per task (mf/sgd/dsgdpp_impl.h:79,112)
   uint64_t total = 0;
@@ -661,14 +680,14 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
   a.W = static_cast<double*>(c->W); a.H = static_cast<double*>(c->H);
   a.block_ptr = M.block_ptr; a.schedule = c->d_schedule;
   a.positions = c->d_positions; a.pos_offset = c->d_pos_offset; a.params = c->d_params;
-  a.d = d; a.r = c->r; a.rp = c->rp;
+  a.d = d; a.r = c->r; a.rp = c->rp; a.nb2 = d2;
   a.update = c->cfg.update; a.truncate = c->cfg.truncate;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   for (uint32_t s = 0; s < d2; ++s) {
     check_cuda(launch_replay_subepoch(a, s, st), "replay_subepoch");
     if (l2 && c->cfg.regularize_lambda != 0)
       check_cuda(launch_regularize_exact(a.W, a.H, c->cfg.m, c->cfg.n, c->rp, c->r, c->d_off2,
-                                         c->d_mask + (size_t)s * d2, d, c->d_params,
+                                         c->d_mask + (size_t)s * d2, d, d2, c->d_params,
                                          c->cfg.regularize_lambda, c->cfg.truncate,
                                          c->cfg.truncate_min, c->cfg.truncate_max, st),
                  "regularize");
@@ -684,7 +703,7 @@ void epoch_explicit_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
   if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
   if (!c->factors_set) throw Error(DSGDPP_E_STATE, "factors not set");
   if (!std::isfinite(eps)) throw Error(DSGDPP_E_INVALID, "step size is not finite");
-  const uint32_t d = c->d, d2 = 2 * d;
+  const uint32_t d = c->d, d2 = c->nb2;
   for (size_t k = 0; k < (size_t)d2 * d; ++k)
     if (schedule[k] >= d2) throw Error(DSGDPP_E_INVALID, "schedule entry out of range");
   check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
@@ -869,7 +888,7 @@ int dsgdpp_block_nnz(dsgdpp_ctx* c, int which, uint64_t* out) {
     if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
     const DevMatrix& M = c->mat[which];
     if (!M.present) throw Error(DSGDPP_E_STATE, "matrix not set");
-    const size_t nb = (size_t)c->d * 2 * c->d;
+    const size_t nb = (size_t)c->d * c->nb2;
     for (size_t b = 0; b < nb; ++b) out[b] = M.h_block_ptr[b + 1] - M.h_block_ptr[b];
     return DSGDPP_OK;
   });
@@ -906,8 +925,8 @@ int dsgdpp_seed(dsgdpp_ctx* c, uint32_t seed) {
 int dsgdpp_epoch(dsgdpp_ctx* c, double eps) {
   return guarded(c, [&]() {
     const uint32_t d = c->d;
-    std::vector<uint32_t> sched((size_t)2 * d * d), seeds(d);
-    dsgdpp_schedule(c->master, d, c->cfg.stratum_order, sched.data(), seeds.data());
+    std::vector<uint32_t> sched((size_t)c->nb2 * d), seeds(d);
+    draw_epoch(c, sched.data(), seeds.data());
     epoch_explicit_impl(c, eps, sched.data(), seeds.data());
     return DSGDPP_OK;
   });
@@ -938,7 +957,7 @@ int dsgdpp_set_kernel_timing(dsgdpp_ctx* c, int on) {
     check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
     collect_profile(c);
     if (on && c->prof_ev.empty()) {
-      c->prof_ev.resize(2 * c->d + 1);
+      c->prof_ev.resize(c->nb2 + 1);
       for (auto& e : c->prof_ev) check_cuda(cudaEventCreate(&e), "event");
     }
     c->profiling = on != 0;
@@ -1020,7 +1039,7 @@ int dsgdpp_run(dsgdpp_ctx* c, uint32_t epochs, int decay, double eps0, double de
     }
     double prev = 0, eps_state = eps0;
     const uint32_t d = c->d;
-    std::vector<uint32_t> sched((size_t)2 * d * d), seeds(d);
+    std::vector<uint32_t> sched((size_t)c->nb2 * d), seeds(d);
     for (uint32_t e = 0; e < epochs; ++e) {
       auto a = clock::now();
       double eps;
@@ -1033,7 +1052,7 @@ int dsgdpp_run(dsgdpp_ctx* c, uint32_t epochs, int decay, double eps0, double de
         eps = eps_state;
       }
       auto b = clock::now();
-      dsgdpp_schedule(c->master, d, c->cfg.stratum_order, sched.data(), seeds.data());
+      draw_epoch(c, sched.data(), seeds.data());
       epoch_explicit_impl(c, eps, sched.data(), seeds.data());
       check_cuda(cudaEventSynchronize(c->ev_end), "event sync");
       auto e1 = clock::now();

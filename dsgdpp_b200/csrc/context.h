@@ -77,6 +77,7 @@ struct dsgdpp_ctx {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   uint32_t d = 0, r = 0, rp = 0;
+  uint32_t nb2 = 0;  // column blocks = sub-epochs per epoch: 2d (DSGD++) or d (DSGD)
   std::vector<uint64_t> off1, off2;  // with the end offset appended
   uint64_t* d_off1 = nullptr;
   uint64_t* d_off2 = nullptr;

@@ -55,24 +55,26 @@ struct ReplayArgs {
   const uint32_t* cnt2;  // nnz2 per column
   double* W;
   double* H;
-  const uint64_t* block_ptr;  // d*2d+1
-  const uint32_t* schedule;   // [2d][d]
+  const uint64_t* block_ptr;  // d*nb2+1
+  const uint32_t* schedule;   // [nb2][d]
   const uint32_t* positions;  // point order, concatenated per (sub-epoch, task)
-  const uint64_t* pos_offset; // [2d*d+1]
+  const uint64_t* pos_offset; // [nb2*d+1]
   const EpochParams* params;
   uint32_t d, r, rp;
+  uint32_t nb2;               // column blocks (2d for DSGD++, d for DSGD)
   int update, truncate;
   double lambda, tmin, tmax;
 };
 
 struct SegBuildArgs {
   const EpochParams* params;  // eps of the epoch
-  const uint32_t* schedule;   // [2d][d]
-  const uint64_t* block_ptr;  // d*2d+1
-  const float* sigma;         // [2d][d][3] lazy L2 scales, or null (all ones)
-  Segment* segs;              // [2d][d+1]
-  uint32_t* counters;         // [2d]
+  const uint32_t* schedule;   // [nb2][d]
+  const uint64_t* block_ptr;  // d*nb2+1
+  const float* sigma;         // [nb2][d][3] lazy L2 scales, or null (all ones)
+  Segment* segs;              // [nb2][d+1]
+  uint32_t* counters;         // [nb2]
   uint32_t d;
+  uint32_t nb2;               // column blocks = sub-epochs (2d for DSGD++, d for DSGD)
 };
 
 // Persistent epoch: one launch walks every sub-epoch; a chunk of segment
@@ -80,11 +82,12 @@ struct SegBuildArgs {
 // rows of W -- and the last earlier segment on the same column block of H
 // (dep_col) have finished all their chunks.
 struct EpochDeps {
-  const int32_t* dep_col;  // [2d][d]: s2 * d + j of that segment, or -1
-  uint32_t* done;          // [2d][d] chunks finished per segment (zeroed per epoch)
+  const int32_t* dep_col;  // [nsub][d]: s2 * d + j of that segment, or -1
+  uint32_t* done;          // [nsub][d] chunks finished per segment (zeroed per epoch)
   uint32_t* ticket;        // chunks handed out (zeroed per epoch)
   uint32_t* error;         // set when a dependency wait gave up
   uint32_t d;
+  uint32_t nsub;           // sub-epochs (2d for DSGD++, d for DSGD)
 };
 
 // ---- launchers (return cudaError_t) -------------------------------------------
@@ -97,12 +100,12 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomi
 // the persistent epoch (column / row runs, atomic writes, SEQ or WOR order)
 cudaError_t launch_hogwild_epoch(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
                                  const EpochDeps& dp, uint32_t grid, cudaStream_t st);
-int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d);
+int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t nsub);
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st);
 // RegularizeL2 after sub-epoch s, exactly as the reference (all W, stratum H)
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
                                     uint32_t r, const uint64_t* off2, const uint8_t* mask,
-                                    uint32_t d, const EpochParams* params, double lambda,
+                                    uint32_t d, uint32_t nb2, const EpochParams* params, double lambda,
                                     int truncate, double tmin, double tmax, cudaStream_t st);
 // Lazy-L2 normalisation at the end of a Hogwild epoch: H column block b2 is
 // multiplied by scales[b2], all of W by scales[nb2] (device memory)

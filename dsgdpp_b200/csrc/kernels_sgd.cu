@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(256) hogwild_epoch_kernel(HogwildArgs a, Epoch
   using E = Elem<T>;
   using C = typename E::C;
   extern __shared__ __align__(16) uint32_t prefix[];  // [2d + 1] chunk offsets per sub-epoch
-  const uint32_t d = dp.d, nsub = 2 * d;
+  const uint32_t d = dp.d, nsub = dp.nsub;
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (uint32_t s = 0; s < nsub; ++s) {
@@ -556,7 +556,7 @@ __global__ void build_segments_kernel(SegBuildArgs a) {
   uint32_t cnt = 0, b2 = 0;
   if (id < d) {
     b2 = a.schedule[(size_t)s * d + id];
-    const uint64_t blk = (uint64_t)id * 2 * d + b2;
+    const uint64_t blk = (uint64_t)id * a.nb2 + b2;
     rb = a.block_ptr[blk];
     cnt = (uint32_t)(a.block_ptr[blk + 1] - rb);
     chunks = (cnt + kChunk - 1) / kChunk;
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint
   if (id >= a.d) return;
   const uint32_t d = a.d, r = a.r;
   const uint32_t b2 = a.schedule[(size_t)s * d + id];
-  const uint64_t blk = (uint64_t)id * 2 * d + b2;
+  const uint64_t blk = (uint64_t)id * a.nb2 + b2;
   const uint64_t rb = a.block_ptr[blk];
   const uint64_t n = a.block_ptr[blk + 1] - rb;
   const uint32_t* pos = a.positions + a.pos_offset[(size_t)s * d + id];
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint
 // after sub-epoch s: each W block and the sub-epoch's H blocks are scaled.
 __global__ void regularize_exact_kernel(double* W, double* H, uint64_t m, uint64_t n,
                                         uint32_t rp, uint32_t r, const uint64_t* off2,
-                                        const uint8_t* mask, uint32_t d,
+                                        const uint8_t* mask, uint32_t d, uint32_t nb2,
                                         const EpochParams* params, double lambda, int truncate,
                                         double tmin, double tmax) {
   const double eps = __ddiv_rn(params->eps, (double)d);  // eps/d: rescaleStratumStepsize()
@@ -698,7 +698,7 @@ __global__ void regularize_exact_kernel(double* W, double* H, uint64_t m, uint64
     } else {
       const uint64_t hq = q - wtot, j = hq / rp;
       // column block of j
-      uint32_t lo = 0, hi = 2 * d - 1;
+      uint32_t lo = 0, hi = nb2 - 1;
       while (lo < hi) {
         uint32_t mid = (lo + hi + 1) >> 1;
         if (off2[mid] <= j) lo = mid; else hi = mid - 1;
@@ -823,7 +823,7 @@ cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st) {
   uint32_t threads = 32;
   while (threads < a.d) threads <<= 1;
   if (threads > 1024) return cudaErrorInvalidValue;
-  build_segments_kernel<<<2 * a.d, threads, 0, st>>>(a);
+  build_segments_kernel<<<a.nb2, threads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -859,10 +859,11 @@ cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t
 
 cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n, uint32_t rp,
                                     uint32_t r, const uint64_t* off2, const uint8_t* mask,
-                                    uint32_t d, const EpochParams* params, double lambda,
-                                    int truncate, double tmin, double tmax, cudaStream_t st) {
-  regularize_exact_kernel<<<1184, 256, 0, st>>>(W, H, m, n, rp, r, off2, mask, d, params, lambda,
-                                                truncate, tmin, tmax);
+                                    uint32_t d, uint32_t nb2, const EpochParams* params,
+                                    double lambda, int truncate, double tmin, double tmax,
+                                    cudaStream_t st) {
+  regularize_exact_kernel<<<1184, 256, 0, st>>>(W, H, m, n, rp, r, off2, mask, d, nb2, params,
+                                                lambda, truncate, tmin, tmax);
   return cudaGetLastError();
 }
 
@@ -920,11 +921,11 @@ void* epoch_kernel_ptr(int precision, uint32_t lanes, uint32_t vecs) {
 
 }  // namespace
 
-int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t d) {
+int hogwild_epoch_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, uint32_t nsub) {
   void* fn = epoch_kernel_ptr(precision, lanes, vecs);
   if (!fn) return 0;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(uint32_t) * (2 * d + 1)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(uint32_t) * (nsub + 1)) !=
       cudaSuccess)
     return 0;
   return n;
@@ -937,7 +938,7 @@ cudaError_t launch_hogwild_epoch(int precision, uint32_t lanes, uint32_t vecs, c
   HogwildArgs args = a;
   EpochDeps deps = dp;
   void* params[] = {&args, &deps};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(uint32_t) * (2 * dp.d + 1), st);
+  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(uint32_t) * (dp.nsub + 1), st);
 }
 
 }  // namespace dsgdpp

@@ -10,6 +10,10 @@
 //                                order per block, FP64 only (default hogwild)
 //   --launch graph|stream        epoch as one CUDA graph or 2d launches
 //   --layout shuffled|col-runs|row-runs|runs   Hogwild record order in a block
+// Invoked as `mfdsgd` (the same binary under that name) it is the drop-in for
+// tools/mfdsgd.cc instead: DSGD with d x d blocks and d sub-epochs per epoch
+// (mf/sgd/dsgd_impl.h), plus the --map-reduce option (on one GPU the H blocks
+// stay in device memory either way, so it changes no result).
 // Extension: --regularize L2(l) is accepted (the reference rejects every
 // regularizer other than None, tools/mfdsgdpp.cc:165-258).
 #include <cmath>
@@ -43,6 +47,7 @@ struct Args {
   unsigned seed = 0;
   int tasksPerRank = 1;
   bool abs = false;
+  bool mapReduce = false;  // mfdsgd --map-reduce
   double epsilon = NAN, epsDecrease = NAN, epsIncrease = NAN;
   int sgdOrder = DSGDPP_SGD_WOR, stratumOrder = DSGDPP_STRATUM_COWOR;
   // added options
@@ -50,14 +55,17 @@ struct Args {
   std::string precision = "fp32", exec = "hogwild", launch = "graph", layout = "runs";
 };
 
+bool g_dsgd = false;  // running as mfdsgd
+
 const char* kOptions[] = {
     "help", "input-file", "input-test-file", "input-row-file", "input-col-file",
     "output-row-file", "output-col-file", "trace", "trace-var", "epochs", "tasks-per-rank",
     "sgd-order", "stratum-order", "seed", "rank", "update", "regularize", "loss", "abs",
-    "truncate", "decay", "balance", "device", "precision", "exec", "launch", "layout"};
+    "truncate", "decay", "balance", "device", "precision", "exec", "launch", "layout",
+    "map-reduce"};
 
 void usage() {
-  std::cout << "mfsgdpp [options]\n\nOptions:\n"
+  std::cout << (g_dsgd ? "mfdsgd" : "mfsgdpp") << " [options]\n\nOptions:\n"
             << "  --help                 produce help message\n"
             << "  --input-file arg       filename of data matrix\n"
             << "  --input-test-file arg  filename of test matrix\n"
@@ -274,6 +282,7 @@ std::string blocks_list(uint64_t b1, uint64_t b2) {
 
 int run(Args& args, const Job& job) {
   const uint32_t d = (uint32_t)args.tasksPerRank;
+  const uint32_t nb2 = g_dsgd ? d : 2 * d;  // column blocks: d x d (DSGD) or d x 2d (DSGD++)
   if (args.decayName != "BoldDriver" && args.decayName != "Const") {
     std::cerr << "not implemented: decay" << std::endl;  // rg::NotImplementedException
     return 1;
@@ -283,17 +292,19 @@ int run(Args& args, const Job& job) {
     BlockedDescriptor desc;
     if (!ends_with(f, ".xml")) {
       Log::info("mf", "File '" + f + "' is not blocked; it will be blocked automatically");
-      Log::info("mf", "Constructing blocks " + blocks_list(d, 2 * d) + " of '" + f + "'");
+      Log::info("mf", "Constructing blocks " + blocks_list(d, nb2) + " of '" + f + "'");
     }
     Coo m = read_sparse(f, &desc);
     if (ends_with(f, ".xml")) {
-      // the descriptor's blocking must be the job's d x 2d default blocking
-      // (checkBlockingDsgdPp, mf/sgd/dsgdpp-factorization.h:21-33)
-      std::vector<uint64_t> o1(d), o2(2 * d);
+      // the descriptor's blocking must be the job's default blocking, d x 2d
+      // (checkBlockingDsgdPp, mf/sgd/dsgdpp-factorization.h:21-33) or d x d
+      std::vector<uint64_t> o1(d), o2(nb2);
       dsgdpp_block_offsets(desc.size1, d, o1.data());
-      dsgdpp_block_offsets(desc.size2, 2 * d, o2.data());
-      if (desc.blocks1 != d || desc.blocks2 != 2 * d || desc.offsets1 != o1 || desc.offsets2 != o2)
-        throw std::invalid_argument("blocking of " + f + " does not match the d x 2d job blocking");
+      dsgdpp_block_offsets(desc.size2, nb2, o2.data());
+      if (desc.blocks1 != d || desc.blocks2 != nb2 || desc.offsets1 != o1 || desc.offsets2 != o2)
+        throw std::invalid_argument("blocking of " + f + " does not match the d x " +
+                                    (g_dsgd ? std::string("d") : std::string("2d")) +
+                                    " job blocking");
     }
     return m;
   };
@@ -304,11 +315,11 @@ int run(Args& args, const Job& job) {
     T = load_sparse(args.inputTestMatrixFile);
     Log::info("mf", "Test matrix: " + std::to_string(T.size1) + " x " + std::to_string(T.size2) +
                         ", " + std::to_string(T.vals.size()) + " nonzeros, " + std::to_string(d) +
-                        " x " + std::to_string(2 * d) + " blocks");
+                        " x " + std::to_string(nb2) + " blocks");
   }
   Log::info("mf", "Data matrix: " + std::to_string(V.size1) + " x " + std::to_string(V.size2) +
                       ", " + std::to_string(V.vals.size()) + " nonzeros, " + std::to_string(d) +
-                      " x " + std::to_string(2 * d) + " blocks");
+                      " x " + std::to_string(nb2) + " blocks");
   Log::info("mf", "File '" + args.inputRowFacFile + "' is not blocked; it will be blocked automatically");
   Dense Wf = read_mm_array(args.inputRowFacFile);
   Log::info("mf", "Row factor matrix: " + std::to_string(Wf.size1) + " x " +
@@ -316,7 +327,7 @@ int run(Args& args, const Job& job) {
   Log::info("mf", "File '" + args.inputColFacFile + "' is not blocked; it will be blocked automatically");
   Dense Hf = read_mm_array(args.inputColFacFile);
   Log::info("mf", "Column factor matrix: " + std::to_string(Hf.size1) + " x " +
-                      std::to_string(Hf.size2) + ", 1 x " + std::to_string(2 * d) + " blocks");
+                      std::to_string(Hf.size2) + ", 1 x " + std::to_string(nb2) + " blocks");
   // conformity (mf/factorization.h:27-33)
   if (Wf.size1 != V.size1 || Hf.size2 != V.size2 || Wf.size2 != Hf.size1 ||
       (has_test && (T.size1 != V.size1 || T.size2 != V.size2)))
@@ -341,6 +352,7 @@ int run(Args& args, const Job& job) {
   cfg.n = n;
   cfg.rank = (uint32_t)r;
   cfg.d = d;
+  cfg.method = g_dsgd ? DSGDPP_METHOD_DSGD : DSGDPP_METHOD_DSGDPP;
   cfg.precision = args.precision == "fp64" ? DSGDPP_FP64 : args.precision == "bf16" ? DSGDPP_BF16 : DSGDPP_FP32;
   cfg.exec = args.exec == "replay" ? DSGDPP_EXEC_REPLAY : DSGDPP_EXEC_HOGWILD;
   cfg.launch = args.launch == "stream" ? DSGDPP_LAUNCH_STREAM : DSGDPP_LAUNCH_GRAPH;
@@ -395,8 +407,11 @@ int run(Args& args, const Job& job) {
     decay.increase = args.epsIncrease;
   }
   if (has_test) Log::info("main", "Using NzslLoss for test data");
-  Log::info("mf", "Starting DSGD++ on " + std::string(args.exec) + " " + args.precision +
-                      " (B200, one GPU)");
+  Log::info("mf", std::string(g_dsgd ? "Starting DSGD" : "Starting DSGD++") + " on " +
+                      std::string(args.exec) + " " + args.precision + " (B200, one GPU)");
+  if (g_dsgd)  // mf/sgd/dsgd_impl.h:56-60
+    Log::info("mf", args.mapReduce ? "Using slow MapReduce-style implementation"
+                                   : "Using fast DSGD+ implementation");
   static const char* kStrata[] = {"SEQ", "RSEQ", "WR", "WOR", "COWOR"};
   static const char* kPoints[] = {"SEQ", "WR", "WOR"};
   Log::info("mf", std::string("Using ") + kStrata[args.stratumOrder] + " order for selecting strata");
@@ -405,7 +420,7 @@ int run(Args& args, const Job& job) {
   auto r0 = std::chrono::steady_clock::now();
   default_runner(ctx, args.epochs, decay, trace, has_test);
   auto r1 = std::chrono::steady_clock::now();
-  Log::info("mf", "Finished DSGD++");
+  Log::info("mf", g_dsgd ? "Finished DSGD" : "Finished DSGD++");
   Log::info("main", "Total time: " +
                         fmt_secs((double)std::chrono::duration_cast<std::chrono::nanoseconds>(r1 - r0).count()));
 
@@ -441,6 +456,11 @@ int run(Args& args, const Job& job) {
 }  // namespace
 
 int main(int argc, char** argv) {
+  {
+    const std::string self = argc > 0 ? std::string(argv[0]) : std::string();
+    const size_t slash = self.find_last_of('/');
+    g_dsgd = self.substr(slash == std::string::npos ? 0 : slash + 1) == "mfdsgd";
+  }
   Args args;
   std::map<std::string, std::string> vm;
   std::vector<std::string> positional;
@@ -460,7 +480,8 @@ int main(int argc, char** argv) {
         }
         val = argv[++k];
       }
-      if (std::find(flags.begin(), flags.end(), key) == flags.end()) {
+      if (std::find(flags.begin(), flags.end(), key) == flags.end() ||
+          (key == "map-reduce" && !g_dsgd)) {
         std::cerr << "unrecognised option '--" << key << "'" << std::endl;
         return 1;
       }
@@ -537,7 +558,7 @@ int main(int argc, char** argv) {
   Log::info("main", "Parallelization");
   Log::info("main", "    MPI ranks: 1");
   Log::info("main", "    Tasks per rank: " + std::to_string(args.tasksPerRank));
-  Log::info("main", "DSGD++ options");
+  Log::info("main", g_dsgd ? "DSGD options" : "DSGD++ options");
   Log::info("main", "    Seed: " + std::to_string(args.seed));
   Log::info("main", "    Epochs: " + std::to_string(args.epochs));
   Log::info("main", "    Factorization rank: " + std::to_string(args.rank));
@@ -585,6 +606,19 @@ int main(int argc, char** argv) {
   }
   args.stratumOrder = so;
   Log::info("main", "    DSGD stratum sequence: " + args.stratumOrderString);
+  if (g_dsgd) {  // tools/mfdsgd.cc:63,108,211 (boost bool syntax)
+    const std::string mr = vm.count("map-reduce") ? vm["map-reduce"] : "0";
+    if (mr == "1" || mr == "true" || mr == "yes" || mr == "on") {
+      args.mapReduce = true;
+    } else if (mr == "0" || mr == "false" || mr == "no" || mr == "off") {
+      args.mapReduce = false;
+    } else {
+      std::cerr << "the argument ('" << mr << "') for option '--map-reduce' is invalid" << std::endl;
+      return 1;
+    }
+    Log::info("main", std::string("    Slow MapReduce implementation: ") +
+                          (args.mapReduce ? "1" : "0"));
+  }
 
   parse_doubles(args.updateString, args.updateName, args.updateArgs);
   parse_doubles(args.regularizeString, args.regularizeName, args.regularizeArgs);

@@ -78,6 +78,9 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 #define DSGDPP_WRITE_STORE 1  /* store the new row/column (concurrent updates may be lost) */
 #define DSGDPP_WRITE_ATOMIC 2 /* add the update atomically: vector atomic add (FP32/FP64);
                                  BF16 adds the increment to the stochastically rounded value */
+/* the stratified method (DsgdPpRunner, DsgdRunner) */
+#define DSGDPP_METHOD_DSGDPP 0 /* d x 2d blocks, 2d sub-epochs (mf/sgd/dsgdpp_impl.h)        */
+#define DSGDPP_METHOD_DSGD 1   /* d x d blocks, d sub-epochs (mf/sgd/dsgd_impl.h:80-234,328-350) */
 /* order of the Hogwild training records inside each block */
 #define DSGDPP_LAYOUT_SHUFFLED 0 /* random order (hash of layout_seed and the record) */
 #define DSGDPP_LAYOUT_COL_RUNS 1 /* by column, random within a column: runs of one H row */
@@ -114,6 +117,7 @@ typedef struct dsgdpp_config {
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
   int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
   int32_t layout;         /* Hogwild record order in a block: DSGDPP_LAYOUT_* */
+  int32_t method;         /* DSGDPP_METHOD_*: d x 2d (default) or d x d blocking */
 } dsgdpp_config;
 
 /* One row of the run trace (SgdTraceEntry, mf/trace.h:84-116); times in ns. */
@@ -150,7 +154,7 @@ int dsgdpp_set_matrix(dsgdpp_ctx* ctx, int which, uint64_t nnz, const uint32_t* 
 int dsgdpp_set_factors(dsgdpp_ctx* ctx, const double* W, const double* H);
 /* replaces: unblock + the factor arrays read by writeMatrix (tools/mfdsgdpp.cc:145-159) */
 int dsgdpp_get_factors(dsgdpp_ctx* ctx, double* W, double* H);
-/* nnz per block (d x 2d row-major) of the blocked matrix */
+/* nnz per block of the blocked matrix: d x 2d row-major (DSGD++), d x d (DSGD) */
 int dsgdpp_block_nnz(dsgdpp_ctx* ctx, int which, uint64_t* out);
 /* per-row / per-column counts of the training matrix (nnz12) */
 int dsgdpp_nnz12(dsgdpp_ctx* ctx, uint64_t* nnz1, uint64_t* nnz2, uint64_t* nnz12max);

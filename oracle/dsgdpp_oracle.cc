@@ -216,6 +216,8 @@ struct Block {
 struct orc_problem {
   uint64_t m = 0, n = 0;
   uint32_t r = 0, d = 0;
+  uint32_t nb2 = 0;  // column blocks = sub-epochs: 2d (DSGD++) or d (DSGD)
+  int method = 0;    // 0 DSGD++, 1 DSGD
   std::vector<uint64_t> off1, off2;
   std::vector<Block> train, test;  // d x 2d row-major
   std::vector<double> W, H;        // W m x r row-major; H col-major (col j contiguous)
@@ -241,7 +243,7 @@ uint32_t blockOf(uint64_t i, const std::vector<uint64_t>& off) {
 // 162-164): block-local coordinates, (i, j) order, duplicates summed in file order.
 std::vector<Block> blockMatrix(const orc_problem& p, uint64_t nnz, const uint32_t* rows,
                                const uint32_t* cols, const double* vals) {
-  const uint32_t d = p.d, d2 = 2 * p.d;
+  const uint32_t d = p.d, d2 = p.nb2;
   std::vector<std::vector<uint64_t>> idx((size_t)d * d2);
   for (uint64_t k = 0; k < nnz; ++k) {
     uint32_t b1 = blockOf(rows[k], p.off1), b2 = blockOf(cols[k], p.off2);
@@ -396,10 +398,10 @@ struct TaskRunner {
 
 BlockJob makeJob(orc_problem& p, uint32_t b1, uint32_t b2) {
   BlockJob J;
-  J.v = &p.train[(size_t)b1 * 2 * p.d + b2];
+  J.v = &p.train[(size_t)b1 * p.nb2 + b2];
   J.r = p.r;
   J.mBlk = (b1 + 1 < p.d ? p.off1[b1 + 1] : p.m) - p.off1[b1];
-  J.nBlk = (b2 + 1 < 2 * p.d ? p.off2[b2 + 1] : p.n) - p.off2[b2];
+  J.nBlk = (b2 + 1 < p.nb2 ? p.off2[b2 + 1] : p.n) - p.off2[b2];
   J.w = p.W.data() + p.off1[b1] * p.r;
   J.h = p.H.data() + p.off2[b2] * p.r;
   J.nnz1 = p.nnz1.data() + p.off1[b1];
@@ -431,7 +433,7 @@ double epochExplicit(orc_problem& p, double eps, const uint32_t* sched, const ui
   for (uint32_t id = 0; id < d; ++id) tasks.emplace_back(seeds[id]);
   if (threads <= 1) {
     std::vector<uint32_t> scratch;
-    for (uint32_t s = 0; s < 2 * d; ++s)
+    for (uint32_t s = 0; s < p.nb2; ++s)
       for (uint32_t id = 0; id < d; ++id)
         runTaskSubepoch(p, tasks[id], id, sched[(size_t)s * d + id], eps, scratch);
   } else {
@@ -441,7 +443,7 @@ double epochExplicit(orc_problem& p, double eps, const uint32_t* sched, const ui
     for (int t = 0; t < T; ++t) {
       pool.emplace_back([&, t]() {
         std::vector<uint32_t> scratch;
-        for (uint32_t s = 0; s < 2 * d; ++s) {
+        for (uint32_t s = 0; s < p.nb2; ++s) {
           for (uint32_t id = (uint32_t)t; id < d; id += (uint32_t)T)
             runTaskSubepoch(p, tasks[id], id, sched[(size_t)s * d + id], eps, scratch);
           bar.arrive_and_wait();  // barrier(channels), dsgdpp_impl.h:259-263
@@ -506,12 +508,14 @@ void orc_dsgdpp_schedule(orc_random* r, uint32_t d, int order, uint32_t* schedul
 orc_problem* orc_create(uint64_t m, uint64_t n, uint32_t r, uint32_t d, uint64_t nnz,
                         const uint32_t* rows, const uint32_t* cols, const double* vals,
                         uint64_t nnz_test, const uint32_t* trows, const uint32_t* tcols,
-                        const double* tvals) {
-  if (d == 0 || r == 0) return nullptr;
+                        const double* tvals, int method) {
+  if (d == 0 || r == 0 || method < 0 || method > 1) return nullptr;
   auto* p = new orc_problem();
   p->m = m; p->n = n; p->r = r; p->d = d;
+  p->method = method;
+  p->nb2 = method == 1 ? d : 2 * d;  // DSGD: d x d blocks (mf/sgd/dsgd_impl.h:328-350)
   p->off1 = blockOffsets(m, d);
-  p->off2 = blockOffsets(n, 2 * d);
+  p->off2 = blockOffsets(n, p->nb2);
   p->train = blockMatrix(*p, nnz, rows, cols, vals);
   p->test = blockMatrix(*p, nnz_test, trows, tcols, tvals);
   p->W.assign(m * r, 0.0);
@@ -520,8 +524,8 @@ orc_problem* orc_create(uint64_t m, uint64_t n, uint32_t r, uint32_t d, uint64_t
   p->nnz1.assign(m, 0);
   p->nnz2.assign(n, 0);
   for (uint32_t b1 = 0; b1 < d; ++b1)
-    for (uint32_t b2 = 0; b2 < 2 * d; ++b2) {
-      const Block& B = p->train[(size_t)b1 * 2 * d + b2];
+    for (uint32_t b2 = 0; b2 < p->nb2; ++b2) {
+      const Block& B = p->train[(size_t)b1 * p->nb2 + b2];
       for (size_t q = 0; q < B.x.size(); ++q) {
         p->nnz1[B.i[q] + p->off1[b1]]++;
         p->nnz2[B.j[q] + p->off2[b2]]++;
@@ -572,7 +576,7 @@ void orc_block_nnz(const orc_problem* p, int which, uint64_t* out) {
 
 uint64_t orc_block_records(const orc_problem* p, int which, uint32_t b1, uint32_t b2,
                            uint32_t* i, uint32_t* j, double* x) {
-  const Block& B = (which ? p->test : p->train)[(size_t)b1 * 2 * p->d + b2];
+  const Block& B = (which ? p->test : p->train)[(size_t)b1 * p->nb2 + b2];
   if (i) std::copy(B.i.begin(), B.i.end(), i);
   if (j) std::copy(B.j.begin(), B.j.end(), j);
   if (x) std::copy(B.x.begin(), B.x.end(), x);
@@ -585,9 +589,15 @@ double orc_epoch_explicit(orc_problem* p, double eps, const uint32_t* schedule,
 }
 
 double orc_epoch(orc_problem* p, double eps, int threads) {
-  std::vector<uint32_t> sched((size_t)2 * p->d * p->d), seeds(p->d);
+  std::vector<uint32_t> sched((size_t)p->nb2 * p->d), seeds(p->d);
   auto t0 = std::chrono::steady_clock::now();
-  dsgdppSchedule(p->master, p->d, p->stratumOrder, sched.data(), seeds.data());
+  if (p->method == 1) {  // DsgdRunner::epoch (mf/sgd/dsgd_impl.h:328-350): schedule, then task seeds
+    const std::vector<uint32_t> S = computeDsgdSchedule(1, p->d, p->stratumOrder, p->master);
+    std::copy(S.begin(), S.end(), sched.begin());
+    for (uint32_t id = 0; id < p->d; ++id) seeds[id] = p->master.next();
+  } else {
+    dsgdppSchedule(p->master, p->d, p->stratumOrder, sched.data(), seeds.data());
+  }
   auto t1 = std::chrono::steady_clock::now();
   return epochExplicit(*p, eps, sched.data(), seeds.data(), threads) +
          (double)std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count();
@@ -599,9 +609,9 @@ uint64_t orc_positions(const orc_problem* p, const uint32_t* schedule, const uin
   std::vector<TaskRunner> tasks;
   for (uint32_t id = 0; id < d; ++id) tasks.emplace_back(seeds[id]);
   uint64_t at = 0;
-  for (uint32_t s = 0; s < 2 * d; ++s)
+  for (uint32_t s = 0; s < p->nb2; ++s)
     for (uint32_t id = 0; id < d; ++id) {
-      const Block& B = p->train[(size_t)id * 2 * d + schedule[(size_t)s * d + id]];
+      const Block& B = p->train[(size_t)id * p->nb2 + schedule[(size_t)s * d + id]];
       uint64_t n = B.x.size();
       if (out) tasks[id].positions(p->sgdOrder, n, out + at);
       else {
@@ -619,8 +629,8 @@ double orc_nzsl(const orc_problem* p, int which) {
   const auto& Bs = which ? p->test : p->train;
   double total = 0;
   for (uint32_t b1 = 0; b1 < p->d; ++b1)
-    for (uint32_t b2 = 0; b2 < 2 * p->d; ++b2)
-      total += nzslBlock(*p, Bs[(size_t)b1 * 2 * p->d + b2], b1, b2);
+    for (uint32_t b2 = 0; b2 < p->nb2; ++b2)
+      total += nzslBlock(*p, Bs[(size_t)b1 * p->nb2 + b2], b1, b2);
   return total;
 }
 
@@ -638,8 +648,8 @@ double orc_l2w(const orc_problem* p) {
 }
 double orc_l2h(const orc_problem* p) {
   double total = 0;
-  for (uint32_t b2 = 0; b2 < 2 * p->d; ++b2) {
-    uint64_t lo = p->off2[b2] * p->r, hi = (b2 + 1 < 2 * p->d ? p->off2[b2 + 1] : p->n) * p->r;
+  for (uint32_t b2 = 0; b2 < p->nb2; ++b2) {
+    uint64_t lo = p->off2[b2] * p->r, hi = (b2 + 1 < p->nb2 ? p->off2[b2 + 1] : p->n) * p->r;
     double s = 0;
     for (uint64_t q = lo; q < hi; ++q) s = s + p->H[q] * p->H[q];
     total += s;
@@ -664,8 +674,8 @@ double orc_nzl2w(const orc_problem* p) {
 }
 double orc_nzl2h(const orc_problem* p) {
   double total = 0;
-  for (uint32_t b2 = 0; b2 < 2 * p->d; ++b2) {
-    uint64_t lo = p->off2[b2], hi = (b2 + 1 < 2 * p->d ? p->off2[b2 + 1] : p->n);
+  for (uint32_t b2 = 0; b2 < p->nb2; ++b2) {
+    uint64_t lo = p->off2[b2], hi = (b2 + 1 < p->nb2 ? p->off2[b2 + 1] : p->n);
     double result = 0;
     for (uint64_t j = lo; j < hi; ++j) {
       double v = 0;

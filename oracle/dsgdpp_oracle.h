@@ -52,7 +52,8 @@ orc_problem* orc_create(uint64_t m, uint64_t n, uint32_t r, uint32_t d,
                         uint64_t nnz, const uint32_t* rows, const uint32_t* cols,
                         const double* vals,
                         uint64_t nnz_test, const uint32_t* trows,
-                        const uint32_t* tcols, const double* tvals);
+                        const uint32_t* tcols, const double* tvals,
+                        int method);
 void orc_destroy(orc_problem* p);
 
 /* update: 0 Nzsl, 1 Nzsl_L2, 2 Nzsl_Nzl2; regularize: 0 None, 1 L2;

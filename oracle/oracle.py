@@ -31,7 +31,7 @@ _SIGS = {
     "orc_compute_dsgd_schedule": (None, [_P, C.c_uint32, C.c_uint32, C.c_int, _u32p]),
     "orc_dsgdpp_schedule": (None, [_P, C.c_uint32, C.c_int, _u32p, _u32p]),
     "orc_create": (_P, [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _u32p,
-                        _u32p, _f64p, C.c_uint64, _u32p, _u32p, _f64p]),
+                        _u32p, _f64p, C.c_uint64, _u32p, _u32p, _f64p, C.c_int]),
     "orc_destroy": (None, [_P]),
     "orc_configure": (C.c_int, [_P, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int,
                                 C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]),
@@ -136,11 +136,17 @@ def bold_driver(eps, prev, cur, dec=0.5, inc=1.05):
     return lib.orc_bold_driver(eps, C.byref(pv), cur, dec, inc)
 
 
-class Problem:
-    """The CPU restatement of one DSGD++ job (d x 2d blocking)."""
+METHOD = {"dsgdpp": 0, "dsgd": 1}
 
-    def __init__(self, m, n, r, d, rows, cols, vals, trows=None, tcols=None, tvals=None):
+
+class Problem:
+    """The CPU restatement of one DSGD++ job (d x 2d blocking), or of one DSGD
+    job (d x d blocking, d sub-epochs; method="dsgd")."""
+
+    def __init__(self, m, n, r, d, rows, cols, vals, trows=None, tcols=None, tvals=None,
+                 method="dsgdpp"):
         self.m, self.n, self.r, self.d = m, n, r, d
+        self.nb2 = d if method == "dsgd" else 2 * d
         rows = np.ascontiguousarray(rows, np.uint32)
         cols = np.ascontiguousarray(cols, np.uint32)
         vals = np.ascontiguousarray(vals, np.float64)
@@ -154,7 +160,7 @@ class Problem:
         self._h = lib.orc_create(m, n, r, d, len(vals), _p(rows, C.c_uint32),
                                  _p(cols, C.c_uint32), _p(vals, C.c_double), len(tvals),
                                  _p(trows, C.c_uint32), _p(tcols, C.c_uint32),
-                                 _p(tvals, C.c_double))
+                                 _p(tvals, C.c_double), METHOD[method])
         if not self._h:
             raise ValueError("orc_create failed")
 
@@ -198,9 +204,9 @@ class Problem:
         return a, b, mx.value
 
     def block_nnz(self, which=0):
-        out = np.empty(2 * self.d * self.d, np.uint64)
+        out = np.empty(self.nb2 * self.d, np.uint64)
         lib.orc_block_nnz(self._h, which, _p(out, C.c_uint64))
-        return out.reshape(self.d, 2 * self.d)
+        return out.reshape(self.d, self.nb2)
 
     def block_records(self, b1, b2, which=0):
         n = lib.orc_block_records(self._h, which, b1, b2, None, None, None)

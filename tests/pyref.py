@@ -143,15 +143,16 @@ class Task:
 class Job:
     """Blocked problem with global factors as lists of rows."""
 
-    def __init__(self, m, n, r, d, rows, cols, vals):
+    def __init__(self, m, n, r, d, rows, cols, vals, nb2=None):
         self.m, self.n, self.r, self.d = m, n, r, d
+        self.nb2 = 2 * d if nb2 is None else nb2  # d x 2d (DSGD++) or d x d (DSGD)
         self.o1 = block_offsets(m, d) + [m]
-        self.o2 = block_offsets(n, 2 * d) + [n]
+        self.o2 = block_offsets(n, self.nb2) + [n]
         self.blocks = {}
         for i, j, x in sorted(zip(rows.tolist(), cols.tolist(), vals.tolist()),
                               key=lambda e: (e[0], e[1])):
             b1 = max(b for b in range(d) if self.o1[b] <= i)
-            b2 = max(b for b in range(2 * d) if self.o2[b] <= j)
+            b2 = max(b for b in range(self.nb2) if self.o2[b] <= j)
             self.blocks.setdefault((b1, b2), []).append((i, j, x))
         self.nnz1 = [0] * m
         self.nnz2 = [0] * n
@@ -194,7 +195,7 @@ class Job:
     def epoch(self, eps, sched, seeds, update="Nzsl_L2", lam=1.0, sgd_order="WOR"):
         d = self.d
         tasks = [Task(s) for s in seeds]
-        for s in range(2 * d):
+        for s in range(self.nb2):
             for tid in range(d):
                 recs = self.blocks.get((tid, sched[s][tid]), [])
                 for p in tasks[tid].order(sgd_order, len(recs)):
@@ -204,7 +205,7 @@ class Job:
     def nzsl(self):
         total = 0.0
         for b1 in range(self.d):
-            for b2 in range(2 * self.d):
+            for b2 in range(self.nb2):
                 res = 0.0
                 for i, j, x in self.blocks.get((b1, b2), []):
                     ip = 0.0

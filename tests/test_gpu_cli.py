@@ -22,16 +22,21 @@ def _write(tmp_path, p):
     P.write_mm_array(str(tmp_path / "H.mma"), p.H0.T)
 
 
+@pytest.mark.parametrize("tool", ["mfdsgdpp", "mfdsgd"])
 @pytest.mark.parametrize("blocked", [False, True])
-def test_cli_replay_matches_oracle(tmp_path, blocked):
+def test_cli_replay_matches_oracle(tmp_path, blocked, tool):
     p = synth.make(400, 300, 6000, 600, rank_true=4, r=5, noise=0.1, seed=4)
     _write(tmp_path, p)
     d = 3
+    dsgd = tool == "mfdsgd"  # d x d blocks, d sub-epochs (mf/sgd/dsgd_impl.h)
     train = str(tmp_path / "train.mmc")
     if blocked:
         train = str(tmp_path / "V.xml")
-        P.write_blocked(train, str(tmp_path), "V", p.m, p.n, d, 2 * d, p.rows, p.cols, p.vals)
-    r = subprocess.run([CLI, f"--input-file={train}", f"--input-test-file={tmp_path}/test.mmc",
+        P.write_blocked(train, str(tmp_path), "V", p.m, p.n, d, d if dsgd else 2 * d, p.rows,
+                        p.cols, p.vals)
+    extra = ["--map-reduce=1"] if dsgd else []
+    r = subprocess.run([os.path.join(os.path.dirname(CLI), tool), *extra,
+                        f"--input-file={train}", f"--input-test-file={tmp_path}/test.mmc",
                         f"--input-row-file={tmp_path}/W.mma", f"--input-col-file={tmp_path}/H.mma",
                         "--rank=5", f"--tasks-per-rank={d}", "--update=Nzsl_L2(1)",
                         "--regularize=None", "--loss=Nzsl_L2(1)", "--decay=BoldDriver(0.01)",
@@ -45,7 +50,8 @@ def test_cli_replay_matches_oracle(tmp_path, blocked):
     H0 = P.read_mm_array(str(tmp_path / "H.mma")).T
     _, _, tr, tc, tv = P.read_sparse(str(tmp_path / "train.mmc"))
     _, _, sr, sc, sv = P.read_sparse(str(tmp_path / "test.mmc"))
-    ref = O.Problem(p.m, p.n, 5, d, tr, tc, tv, sr, sc, sv).configure()
+    ref = O.Problem(p.m, p.n, 5, d, tr, tc, tv, sr, sc, sv,
+                    method="dsgd" if dsgd else "dsgdpp").configure()
     ref.set_factors(W0, H0)
     ref.seed(1499881717)
     trace = ref.run(4, "BoldDriver", 0.01)
@@ -59,3 +65,6 @@ def test_cli_replay_matches_oracle(tmp_path, blocked):
     assert text.startswith("trace <- list(trace=list(")
     assert "eps=NA" in text and 'update = "Nzsl_L2(1)"' in text and "rank = 5" in text
     assert "Step size: 0.01 " in r.stdout and "Finished epoch 4" in r.stdout
+    if dsgd:
+        assert "Starting DSGD on" in r.stdout and "DSGD options" in r.stdout
+        assert "Slow MapReduce implementation: 1" in r.stdout

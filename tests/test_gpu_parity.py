@@ -367,3 +367,93 @@ def test_small_cpu_workload_replay_run_matches_oracle():
         Wr, Hr = ref.get_factors()
         np.testing.assert_array_equal(W, Wr)
         np.testing.assert_array_equal(H, Hr)
+
+
+# ---- DSGD (d x d blocking, d sub-epochs; mf/sgd/dsgd_impl.h) -------------------
+@pytest.mark.parametrize("stratum_order", ["SEQ", "RSEQ", "WR", "WOR", "COWOR"])
+@pytest.mark.parametrize("sgd_order", ["SEQ", "WOR"])
+def test_dsgd_replay_master_rng_epochs_bit_exact(stratum_order, sgd_order):
+    p = _problem()
+    d = 3
+    ref = O.Problem(p.m, p.n, 10, d, p.rows, p.cols, p.vals, p.trows, p.tcols, p.tvals,
+                    method="dsgd")
+    ref.configure(sgd_order=sgd_order, stratum_order=stratum_order, update_lambda=0.5)
+    ref.set_factors(p.W0, p.H0)
+    cfg = P.Config(m=p.m, n=p.n, rank=10, d=d, precision="fp64", exec="replay", method="dsgd",
+                   sgd_order=sgd_order, stratum_order=stratum_order, update_lambda=0.5)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ctx.set_factors(p.W0, p.H0)
+        assert ctx.block_nnz(P.TRAIN).shape == (d, d)
+        np.testing.assert_array_equal(ctx.block_nnz(P.TRAIN), ref.block_nnz(0))
+        ctx.seed(5)
+        ref.seed(5)
+        for _ in range(3):
+            ctx.epoch(0.02)
+            ref.epoch(0.02)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+        assert ctx.loss() == pytest.approx(ref.loss(), rel=LOSS_RTOL)
+
+
+def test_dsgd_replay_l2_regularize_and_run_trace():
+    p = _problem(m=800, n=600, nnz=10000, ntest=1000)
+    ref = O.Problem(p.m, p.n, 10, 4, p.rows, p.cols, p.vals, p.trows, p.tcols, p.tvals,
+                    method="dsgd")
+    ref.configure(regularize="L2", regularize_lambda=0.05)
+    ref.set_factors(p.W0, p.H0)
+    cfg = P.Config(m=p.m, n=p.n, rank=10, d=4, precision="fp64", exec="replay", method="dsgd",
+                   regularize="L2", regularize_lambda=0.05)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ctx.set_factors(p.W0, p.H0)
+        ctx.seed(42)
+        ref.seed(42)
+        tr = ctx.run(5, "BoldDriver", 0.01)
+        rt = ref.run(5, "BoldDriver", 0.01)
+        for k, row in enumerate(tr):
+            assert row["loss"] == pytest.approx(rt[k, 0], rel=LOSS_RTOL)
+            assert row["test_loss"] == pytest.approx(rt[k, 1], rel=LOSS_RTOL)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 0.005), ("bf16", 0.01)])
+@pytest.mark.parametrize("launch", ["graph", "persistent"])
+def test_dsgd_hogwild_tracks_fp64_oracle(precision, tol, launch):
+    p = synth.make(20000, 20000, 400000, 40000, rank_true=10, r=10, noise=0.1, seed=3)
+    ref = O.Problem(p.m, p.n, 10, 4, p.rows, p.cols, p.vals, p.trows, p.tcols, p.tvals,
+                    method="dsgd")
+    ref.configure(regularize="L2", regularize_lambda=0.02)
+    ref.set_factors(p.W0, p.H0)
+    cfg = P.Config(m=p.m, n=p.n, rank=10, d=4, precision=precision, launch=launch,
+                   method="dsgd", regularize="L2", regularize_lambda=0.02)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ctx.set_factors(p.W0, p.H0)
+        ctx.seed(9)
+        ref.seed(9)
+        for _ in range(8):
+            ctx.epoch(0.01)
+            ref.epoch(0.01)
+        got = _rmse(ctx, len(p.tvals))
+        want = float(np.sqrt(ref.nzsl(1) / len(p.tvals)))
+        assert abs(got - want) <= tol * want, (got, want)
+
+
+def test_dsgd_blocking_limits_and_batch_rejection():
+    p = _problem(m=50, n=5, nnz=100, ntest=10)
+    P.Context(P.Config(m=p.m, n=p.n, rank=4, d=5, method="dsgd")).close()  # n >= d suffices
+    with pytest.raises(P.DsgdppError):
+        P.Context(P.Config(m=p.m, n=p.n, rank=4, d=5))  # DSGD++ needs n >= 2d
+    prob = dict(m=p.m, n=p.n, rank=4, rows=p.rows, cols=p.cols, vals=p.vals, W=p.W0[:, :4],
+                H=p.H0[:, :4])
+    with pytest.raises(P.DsgdppError):
+        P.Batch(P.Config(m=1, n=1, rank=1, d=1, method="dsgd"), [prob])

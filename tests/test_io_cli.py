@@ -152,3 +152,17 @@ def test_cli_fails_loudly_without_gpu(tmp_path):
     assert r.returncode == 1
     assert "dsgdpp_create" in r.stderr
     assert "    Update function: Nzsl_L2(1)" in r.stdout
+
+
+def test_dsgd_tool_name_and_map_reduce_option(tmp_path):
+    _files(tmp_path)
+    dsgd = os.path.join(os.path.dirname(CLI), "mfdsgd")
+    r = subprocess.run([dsgd, "--input-file=x.mmc"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1 and r.stdout.startswith("mfdsgd [options]")
+    common = [*_base(tmp_path), "--update=Nzsl", "--regularize=None", "--loss=Nzsl",
+              "--decay=BoldDriver(0.01)"]
+    r = _cli(*common, "--map-reduce=1")  # mfdsgdpp has no such option
+    assert r.returncode == 1 and "unrecognised option '--map-reduce'" in r.stderr
+    r = subprocess.run([dsgd, *common, "--map-reduce=maybe"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1 and "'--map-reduce' is invalid" in r.stderr

@@ -123,6 +123,32 @@ def test_oracle_epoch_matches_python_restatement(update, sgd_order):
     assert ref.nzsl() == py.nzsl()
 
 
+@pytest.mark.parametrize("stratum_order", ["SEQ", "RSEQ", "WR", "WOR", "COWOR"])
+@pytest.mark.parametrize("sgd_order", ["SEQ", "WR", "WOR"])
+def test_oracle_dsgd_epoch_matches_python_restatement(stratum_order, sgd_order):
+    # DsgdRunner::epoch (mf/sgd/dsgd_impl.h:328-350): the d x d schedule of
+    # computeDsgdSchedule(1, d), then one raw draw per task seed; d x d blocks
+    p = _tiny()
+    d = 3
+    ref = O.Problem(p.m, p.n, 3, d, p.rows, p.cols, p.vals, method="dsgd")
+    ref.configure(update="Nzsl_L2", update_lambda=0.7, loss="Nzsl", sgd_order=sgd_order,
+                  stratum_order=stratum_order)
+    ref.set_factors(p.W0, p.H0)
+    ref.seed(11)
+    py = pyref.Job(p.m, p.n, 3, d, p.rows, p.cols, p.vals, nb2=d)
+    py.set_factors(p.W0, p.H0)
+    R = pyref.Rand(11)
+    for e in range(3):
+        S = pyref.dsgd_schedule(1, d, stratum_order, R)
+        seeds = [R.raw() for _ in range(d)]
+        ref.epoch(0.05)
+        py.epoch(0.05, S, seeds, update="Nzsl_L2", lam=0.7, sgd_order=sgd_order)
+    W, H = ref.get_factors()
+    assert np.array_equal(W, np.array(py.W)) and np.array_equal(H, np.array(py.H))
+    assert ref.nzsl() == py.nzsl()
+    assert ref.block_nnz(0).shape == (d, d)
+
+
 def test_positions_are_permutations_and_persist():
     p = _tiny(nnz=200)
     d = 2
