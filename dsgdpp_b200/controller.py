@@ -55,16 +55,28 @@ def _context(prob, precision="fp32", d=16, device=0):
     return ctx
 
 
-KEEP_RISE = 0.01  # as kKeepRise, kMaxHalvings, kCapFrac in csrc/controller.cc
+KEEP_RISE = 0.01  # as the constants of the same meaning in csrc/controller.cc
 MAX_HALVINGS = 8
 CAP_FRAC = 0.9
 CAP_RELAX = 1.05
+BOMB_RATIO = 40.0
+BOMB_GROW = 4.0
 
 
-def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
+def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5, decision=1,
+                    kept_max=()):
     """One epoch under the controller with the BoldDriver fallback, exactly as
-    dsgdpp_run_controlled takes it; returns (training loss, next step, the
-    smallest step that raised the loss in this decision or 0)."""
+    dsgdpp_run_controlled takes it (`decision` = its index, 0 for the first;
+    `kept_max` = the largest row movement of every kept epoch so far);
+    returns (training loss, next step, the smallest step that raised the loss
+    in this decision or 0)."""
+    last3 = sorted(kept_max[-3:])
+    recent = last3[len(last3) // 2] if last3 else 0.0
+
+    def bomb():
+        mean, largest = ctx.update_norms()
+        return decision > 0 and largest > BOMB_RATIO * mean and largest > BOMB_GROW * recent
+
     m = float(net.forward(f[None, :])[0])
     proposed = eps * math.exp(m)
     if fail_eps > 0:
@@ -72,9 +84,10 @@ def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
     ctx.save_factors()
     ctx.epoch(proposed)
     cur = ctx.loss()
-    if cur <= prev_loss:
+    bad = bomb()
+    if cur <= prev_loss and not bad:
         return cur, proposed, 0.0
-    if cur <= prev_loss * (1.0 + KEEP_RISE):
+    if cur <= prev_loss * (1.0 + KEEP_RISE) and not bad:
         return cur, proposed * decrease, proposed
     step, failed = proposed, proposed
     for _ in range(MAX_HALVINGS):
@@ -82,7 +95,7 @@ def controlled_step(ctx, net, f, eps, prev_loss, fail_eps=0.0, decrease=0.5):
         ctx.restore_factors()
         ctx.epoch(step)
         cur = ctx.loss()
-        if cur <= prev_loss * (1.0 + KEEP_RISE):
+        if cur <= prev_loss * (1.0 + KEEP_RISE) and not bomb():
             break
         failed = step
     return cur, (step if cur <= prev_loss else step * decrease), failed
@@ -121,6 +134,7 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None
             eps = float(math.exp(rng.uniform(math.log(3e-4), math.log(3e-3))))
             tr, te = [ctx.loss()], [ctx.nzsl(TEST)]
             upd, last_m, fail_eps = (0.0, 0.0), 0.0, 0.0
+            kept_max = []
             for e in range(epochs):
                 f = controller_features(tr[::-1][:5], te[::-1][:5], eps, upd[0], upd[1],
                                         e / epochs, last_m, fail_eps)
@@ -152,7 +166,8 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None
                     nxt = eps * (0.5 if tr[-1] <= cur else 1.05)
                     failed = eps if not cur <= tr[-1] else 0.0
                 elif policy == "net":
-                    cur, nxt, failed = controlled_step(ctx, net, f, eps, tr[-1], fail_eps)
+                    cur, nxt, failed = controlled_step(ctx, net, f, eps, tr[-1], fail_eps,
+                                                       decision=e, kept_max=kept_max)
                     used_m = math.log(nxt / eps)
                 else:
                     used_m = float(rng.choice(CANDIDATES))
@@ -165,6 +180,7 @@ def generate_traces(count=2000, epochs=25, seed=0, device=0, log=print, net=None
                 elif fail_eps > 0:
                     fail_eps *= CAP_RELAX
                 upd = ctx.update_norms()
+                kept_max.append(upd[1])
                 tr.append(cur)
                 te.append(ctx.nzsl(TEST))
                 last_m = used_m

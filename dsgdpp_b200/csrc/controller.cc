@@ -14,12 +14,21 @@
 //      epoch re-runs with the proposal halved, again and again until the loss
 //      rises by at most kKeepRise (at most kMaxHalvings times; the last
 //      attempt is kept).
+//      An epoch in which one factor row moved more than kBombRatio times the
+//      mean row movement, and more than kBombGrow times the median largest
+//      movement of the last three kept epochs (after the first decision),
+//      counts as a large rise even when the loss fell: such a row makes the
+//      next epochs diverge at any step near the current one, so it is rolled
+//      back at once.  The second condition keeps small steps from a state
+//      that still pulls one row back (movement linear in the step, so the
+//      ratio alone does not fall) from being rejected without end.
 //      The smallest step that raised the loss (fail_eps) is a feature of later
 //      decisions and caps them: a proposal is at most kCapFrac * fail_eps,
 //      and fail_eps grows by kCapRelax (BoldDriver's increase) after every
 //      decision without a rise, so the edge is probed again slowly;
 //   4. the run stops early once the test loss reaches the target.
 // No reference counterpart (the reference's BoldDriver never rolls back).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <vector>
@@ -32,6 +41,8 @@ constexpr double kKeepRise = 0.01;  // relative training-loss rise kept without 
 constexpr int kMaxHalvings = 8;
 constexpr double kCapFrac = 0.9;    // proposals stay below this fraction of fail_eps
 constexpr double kCapRelax = 1.05;  // fail_eps growth per decision without a rise
+constexpr double kBombRatio = 40.0; // largest / mean row movement of an epoch that is kept ...
+constexpr double kBombGrow = 4.0;   // ... unless the largest also grew this much over recent epochs
 
 double since(std::chrono::steady_clock::time_point a) {
   return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(
@@ -61,7 +72,15 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
   if (trace) trace[0] = dsgdpp_trace_row{0, loss, test, NAN, 0, 0, tl, has_test ? since(t1) : 0.0};
   push(tr, loss);
   push(te, test);
+  // the factor snapshot is allocated by its first save: do that before the timed epochs
+  if ((rc = dsgdpp_save_factors(ctx)) != DSGDPP_OK) return rc;
   double eps = eps0, upd_mean = 0, upd_max = 0, last_m = 0, fail_eps = 0;
+  std::vector<double> kept_max;  // largest row movement of each kept epoch
+  auto recent_max = [&]() {       // median of the last three
+    std::vector<double> v(kept_max.end() - std::min<size_t>(3, kept_max.size()), kept_max.end());
+    std::sort(v.begin(), v.end());
+    return v.empty() ? 0.0 : v[v.size() / 2];
+  };
   auto failed = [&](double step) { fail_eps = fail_eps > 0 ? std::fmin(fail_eps, step) : step; };
   uint32_t fb = 0, e = 0;
   for (; e < epochs; ++e) {
@@ -78,11 +97,15 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
     if ((rc = dsgdpp_epoch(ctx, proposed)) != DSGDPP_OK) return rc;
     double cur = 0;
     if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
+    if ((rc = dsgdpp_update_norms(ctx, &upd_mean, &upd_max)) != DSGDPP_OK) return rc;
+    auto bomb = [&]() {
+      return e > 0 && upd_max > kBombRatio * upd_mean && upd_max > kBombGrow * recent_max();
+    };
     double used = proposed, next = proposed;
-    if (!(cur <= tr[0])) {  // the proposed step raised the training loss: fallback
+    if (!(cur <= tr[0]) || bomb()) {  // the proposed step raised the training loss: fallback
       ++fb;
       failed(proposed);
-      if (cur <= tr[0] * (1.0 + kKeepRise)) {
+      if (!bomb() && cur <= tr[0] * (1.0 + kKeepRise)) {
         next = proposed * decrease;  // kept, as BoldDriver keeps it
       } else {
         double step = proposed;
@@ -91,7 +114,8 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
           if ((rc = dsgdpp_restore_factors(ctx)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_epoch(ctx, step)) != DSGDPP_OK) return rc;
           if ((rc = dsgdpp_loss(ctx, &cur)) != DSGDPP_OK) return rc;
-          if (cur <= tr[0] * (1.0 + kKeepRise)) break;  // kept, as the first attempt
+          if ((rc = dsgdpp_update_norms(ctx, &upd_mean, &upd_max)) != DSGDPP_OK) return rc;
+          if (!bomb() && cur <= tr[0] * (1.0 + kKeepRise)) break;  // kept, as the first attempt
           failed(step);
         }
         used = step;
@@ -102,7 +126,7 @@ extern "C" int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t 
     }
     (void)increase;
     last_m = std::log(next / eps);
-    if ((rc = dsgdpp_update_norms(ctx, &upd_mean, &upd_max)) != DSGDPP_OK) return rc;
+    kept_max.push_back(upd_max);
     const double t_epoch = since(b);
     eps = next;
     auto c = std::chrono::steady_clock::now();

@@ -257,10 +257,14 @@ int dsgdpp_mlp_train_step(dsgdpp_mlp* mlp, const float* x, const float* y, int b
  * over (a fallback event): a rise of at most 1% is kept and the next step is
  * the proposal times `decrease`; a larger rise, or a non-finite loss, is
  * rolled back and the epoch re-run at the proposal times decrease^k
- * (k = 1..8) until the rise is at most 1%.  Once a step has raised the loss,
- * proposals are capped at 0.9 times the smallest such step, a cap that grows
- * by 5% with every decision that does not raise the loss.  Stops after `epochs` or once the
- * test loss is at most target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
+ * (k = 1..8) until the rise is at most 1%.  From the second decision on, an
+ * epoch in which one factor row moved more than 40 times the mean row
+ * movement and more than 4 times the median largest movement of the last
+ * three kept epochs is rolled back the same way, whatever the loss did.  Once a step
+ * has raised the loss, proposals are capped at 0.9 times the smallest such
+ * step, a cap that grows by 5% with every decision that does not raise the
+ * loss.  Stops after `epochs` or once the test loss is at most
+ * target_test_loss (> 0).  trace gets epochs_done + 1 rows (time_epoch
  * includes the training losses the decisions need). */
 int dsgdpp_run_controlled(dsgdpp_ctx* ctx, dsgdpp_mlp* mlp, uint32_t epochs, double eps0,
                           double decrease, double increase, double target_test_loss,
