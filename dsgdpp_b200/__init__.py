@@ -171,6 +171,18 @@ SIGNATURES = {
     "dsgdpp_write_blocked": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64,
                                        C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _u32p,
                                        _u32p, _f64p]),
+    "dsgdpp_rm_error": (C.c_char_p, []),
+    "dsgdpp_rm_load": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+    "dsgdpp_rm_create": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64,
+                                   C.c_uint64, C.c_uint32, C.c_char_p, C.c_char_p,
+                                   C.POINTER(_P)]),
+    "dsgdpp_rm_save": (C.c_int, [_P, C.c_char_p]),
+    "dsgdpp_rm_destroy": (None, [_P]),
+    "dsgdpp_rm_info": (C.c_int, [_P, _u64p]),
+    "dsgdpp_rm_generate": (C.c_int, [_P, C.c_int, C.c_int, _u32p, _u32p, _f64p]),
+    "dsgdpp_rm_generate_factors": (C.c_int, [_P, C.c_int, _f64p, _f64p]),
+    "dsgdpp_set_matrix_rm": (C.c_int, [_P, C.c_int, _P]),
+    "dsgdpp_set_factors_rm": (C.c_int, [_P, _P]),
 }
 
 
@@ -299,6 +311,15 @@ class Context:
         w, h = _f64(W), _f64(H)
         self._check(lib.dsgdpp_set_factors(self._h, _ptr(w, C.c_double), _ptr(h, C.c_double)),
                     "set_factors")
+
+    def set_matrix_rm(self, which: int, rm: "RandomMatrix"):
+        """The data (TRAIN) or test (TEST) matrix of a .rm descriptor, generated
+        on the device (getDataMatrices with a .rm file)."""
+        self._check(lib.dsgdpp_set_matrix_rm(self._h, which, rm._h), "set_matrix_rm")
+
+    def set_factors_rm(self, rm: "RandomMatrix"):
+        """Worig and Horig of a .rm descriptor as the factors (getFactors with .rm)."""
+        self._check(lib.dsgdpp_set_factors_rm(self._h, rm._h), "set_factors_rm")
 
     def get_factors(self):
         w = np.empty((self.config.m, self.config.rank), np.float64)
@@ -741,3 +762,68 @@ def philox4x32_10(ctr, key) -> np.ndarray:
     out = np.empty(4, np.uint32)
     lib.dsgdpp_philox4x32_10(_ptr(c, C.c_uint32), _ptr(k, C.c_uint32), _ptr(out, C.c_uint32))
     return out
+
+
+class RandomMatrix:
+    """A .rm random-matrix descriptor (RandomMatrixDescriptor): load one with
+    RandomMatrix(path), make one with RandomMatrix.create(...)."""
+
+    def __init__(self, path: Optional[str] = None, _handle=None):
+        self._h = _handle
+        if path is not None:
+            h = _P()
+            rc = lib.dsgdpp_rm_load(path.encode(), C.byref(h))
+            if rc != OK:
+                raise DsgdppError(rc, f"rm_load: {lib.dsgdpp_rm_error().decode()}")
+            self._h = h
+
+    @staticmethod
+    def create(size1, size2, blocks1, blocks2, nnz, nnz_test, rank, values, noise=""):
+        h = _P()
+        rc = lib.dsgdpp_rm_create(size1, size2, blocks1, blocks2, nnz, nnz_test, rank,
+                                  values.encode(), noise.encode(), C.byref(h))
+        if rc != OK:
+            raise DsgdppError(rc, f"rm_create: {lib.dsgdpp_rm_error().decode()}")
+        return RandomMatrix(_handle=h)
+
+    def _chk(self, rc, what):
+        if rc != OK:
+            raise DsgdppError(rc, f"{what}: {lib.dsgdpp_rm_error().decode()}")
+
+    def save(self, path: str):
+        self._chk(lib.dsgdpp_rm_save(self._h, path.encode()), "rm_save")
+
+    def info(self) -> dict:
+        out = np.zeros(9, np.uint64)
+        self._chk(lib.dsgdpp_rm_info(self._h, _ptr(out, C.c_uint64)), "rm_info")
+        keys = ("size1", "size2", "rank", "blocks1", "blocks2", "nnz", "nnz_test", "data_nnz",
+                "test_nnz")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def generate(self, which: int = TRAIN, device: int = 0):
+        """(rows, cols, vals) of the data or test matrix, generated on the GPU."""
+        n = self.info()["data_nnz" if which == TRAIN else "test_nnz"]
+        rows = np.empty(n, np.uint32)
+        cols = np.empty(n, np.uint32)
+        vals = np.empty(n, np.float64)
+        self._chk(lib.dsgdpp_rm_generate(self._h, which, device, _ptr(rows, C.c_uint32),
+                                         _ptr(cols, C.c_uint32), _ptr(vals, C.c_double)),
+                  "rm_generate")
+        return rows, cols, vals
+
+    def generate_factors(self, device: int = 0):
+        """(Worig: size1 x rank, Horig: size2 x rank), generated on the GPU."""
+        i = self.info()
+        W = np.empty((i["size1"], i["rank"]), np.float64)
+        H = np.empty((i["size2"], i["rank"]), np.float64)
+        self._chk(lib.dsgdpp_rm_generate_factors(self._h, device, _ptr(W, C.c_double),
+                                                 _ptr(H, C.c_double)), "rm_generate_factors")
+        return W, H
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_rm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -2,6 +2,8 @@
 // losses and the defaultRunner loop.
 #include <cub/cub.cuh>
 
+#include <functional>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -14,6 +16,7 @@
 
 #include "../../include/dsgdpp.h"
 #include "context.h"
+#include "rm_device.h"
 #include "kernels.cuh"
 #include "schedule.h"
 
@@ -279,10 +282,15 @@ void reserve_records(DevMatrix& M, uint64_t u, bool as_double) {
   M.cap = u;
 }
 
+// Fills the device input arrays (rows, cols, values) of the blocking: the
+// entries generated on the device instead of copied from the host.
+using DeviceFill = std::function<void(uint32_t*, uint32_t*, double*, cudaStream_t)>;
+
 void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* rows,
-                     const uint32_t* cols, const double* vals) {
+                     const uint32_t* cols, const double* vals,
+                     const DeviceFill* fill = nullptr) {
   if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
-  if (nnz > 0 && (!rows || !cols || !vals)) throw Error(DSGDPP_E_INVALID, "null input array");
+  if (nnz > 0 && !fill && (!rows || !cols || !vals)) throw Error(DSGDPP_E_INVALID, "null input array");
   if (nnz >= 0x7FFFFFFFull) throw Error(DSGDPP_E_UNSUPPORTED, "nnz must be below 2^31");
   check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
   check_cuda(cudaStreamSynchronize(c->stream), "sync");
@@ -361,9 +369,13 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   unsigned long long* d_bad = cv.take<unsigned long long>(1);
   void* tmp = cv.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
 
-  check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
-  check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
-  check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+  if (fill) {
+    (*fill)(t_rows, t_cols, t_vals, st);
+  } else {
+    check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
+    check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
+    check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+  }
   check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
   BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
   check_cuda(launch_make_keys(g, t_rows, t_cols, nnz, keys[0], idx[0], d_bad, st), "make_keys");
@@ -843,6 +855,55 @@ int dsgdpp_set_matrix(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* ro
                       const uint32_t* cols, const double* vals) {
   return guarded(c, [&]() {
     set_matrix_impl(c, which, nnz, rows, cols, vals);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_matrix_rm(dsgdpp_ctx* c, int which, const dsgdpp_rm* rm) {
+  return guarded(c, [&]() {
+    if (!rm) throw Error(DSGDPP_E_INVALID, "null descriptor");
+    const RmDesc& d = rm->d;
+    if (!d.has_data()) throw Error(DSGDPP_E_INVALID, "the descriptor holds no data matrix");
+    if (d.size1 != c->cfg.m || d.size2 != c->cfg.n)
+      throw Error(DSGDPP_E_INVALID, "descriptor size " + std::to_string(d.size1) + " x " +
+                                        std::to_string(d.size2) + " differs from the context's");
+    const uint64_t nnz = rm_count(d, which == DSGDPP_TEST ? 1 : 0);
+    const DeviceFill fill = [&](uint32_t* r, uint32_t* col, double* v, cudaStream_t st) {
+      try {
+        rm_data_device(d, which == DSGDPP_TEST ? 1 : 0, r, col, v, st);
+      } catch (const std::invalid_argument& e) {
+        throw Error(DSGDPP_E_INVALID, e.what());
+      } catch (const std::runtime_error& e) {
+        throw Error(DSGDPP_E_CUDA, e.what());
+      }
+    };
+    set_matrix_impl(c, which, nnz, nullptr, nullptr, nullptr, &fill);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_factors_rm(dsgdpp_ctx* c, const dsgdpp_rm* rm) {
+  return guarded(c, [&]() {
+    if (!rm) throw Error(DSGDPP_E_INVALID, "null descriptor");
+    const RmDesc& d = rm->d;
+    if (d.size1 != c->cfg.m || d.size2 != c->cfg.n || d.rank != c->r)
+      throw Error(DSGDPP_E_INVALID, "descriptor " + std::to_string(d.size1) + " x " +
+                                        std::to_string(d.size2) + ", rank " +
+                                        std::to_string(d.rank) + " does not fit the context");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    ensure_staging(c);
+    const uint64_t m = c->cfg.m, r = c->r;
+    cudaStream_t st = c->stream;
+    try {
+      rm_factors_device(d, c->staging, c->staging + m * r, st);
+    } catch (const std::runtime_error& e) {
+      throw Error(DSGDPP_E_CUDA, e.what());
+    }
+    check_cuda(launch_factor_to_device(c->cfg.precision, c->staging, m, c->r, c->rp, c->W, st), "W");
+    check_cuda(launch_factor_to_device(c->cfg.precision, c->staging + m * r, c->cfg.n, c->r, c->rp,
+                                       c->H, st), "H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    c->factors_set = true;
     return DSGDPP_OK;
   });
 }

@@ -10,6 +10,10 @@
 //                                order per block, FP64 only (default hogwild)
 //   --launch graph|stream        epoch as one CUDA graph or 2d launches
 //   --layout shuffled|col-runs|row-runs|runs   Hogwild record order in a block
+// A .rm random-matrix descriptor given as --input-file (data and, with any
+// --input-test-file, test matrix) or as --input-row-file (both factors) is
+// generated on the device, as the reference generates it on the fly
+// (mf/matrix/io/generateDistributedMatrix_impl.h:655-744).
 // Invoked as `mfdsgd` (the same binary under that name) it is the drop-in for
 // tools/mfdsgd.cc instead: DSGD with d x d blocks and d sub-epochs per epoch
 // (mf/sgd/dsgd_impl.h), plus the --map-reduce option (on one GPU the H blocks
@@ -23,6 +27,7 @@
 #include <fstream>
 #include <iostream>
 #include <map>
+#include <memory>
 #include <regex>
 #include <string>
 #include <vector>
@@ -308,40 +313,80 @@ int run(Args& args, const Job& job) {
     }
     return m;
   };
-  Coo V = load_sparse(args.inputMatrixFile);
-  Coo T;
+  // .rm descriptors: matrices generated on the device instead of read
+  // (getDataMatrices / getFactors, generateDistributedMatrix_impl.h:655-744)
+  using RmPtr = std::unique_ptr<dsgdpp_rm, void (*)(dsgdpp_rm*)>;
+  auto load_rm = [](const std::string& f) {
+    dsgdpp_rm* h = nullptr;
+    if (dsgdpp_rm_load(f.c_str(), &h) != DSGDPP_OK) throw std::invalid_argument(dsgdpp_rm_error());
+    RmPtr p(h, dsgdpp_rm_destroy);
+    return p;
+  };
+  RmPtr rmV(nullptr, dsgdpp_rm_destroy), rmF(nullptr, dsgdpp_rm_destroy);
+  uint64_t info_v[9] = {0}, info_f[9] = {0};
+  Coo V, T;
   const bool has_test = !args.inputTestMatrixFile.empty();
-  if (has_test) {
-    T = load_sparse(args.inputTestMatrixFile);
-    Log::info("mf", "Test matrix: " + std::to_string(T.size1) + " x " + std::to_string(T.size2) +
-                        ", " + std::to_string(T.vals.size()) + " nonzeros, " + std::to_string(d) +
-                        " x " + std::to_string(nb2) + " blocks");
+  uint64_t Vm, Vn, Vnnz, Tm = 0, Tn = 0, Tnnz = 0;
+  if (ends_with(args.inputMatrixFile, ".rm")) {
+    rmV = load_rm(args.inputMatrixFile);
+    dsgdpp_rm_info(rmV.get(), info_v);
+    Log::info("mf", "generating data matrices on the fly...");
+    if (info_v[7] == 0 && info_v[5] == 0)
+      throw std::invalid_argument(args.inputMatrixFile + " holds no data matrix (nnz or nnzTest is 0)");
+    Vm = Tm = info_v[0];
+    Vn = Tn = info_v[1];
+    Vnnz = info_v[7];
+    Tnnz = info_v[8];  // the test matrix comes from the same descriptor
+  } else {
+    V = load_sparse(args.inputMatrixFile);
+    Vm = V.size1; Vn = V.size2; Vnnz = V.vals.size();
+    if (has_test) {
+      T = load_sparse(args.inputTestMatrixFile);
+      Tm = T.size1; Tn = T.size2; Tnnz = T.vals.size();
+    }
   }
-  Log::info("mf", "Data matrix: " + std::to_string(V.size1) + " x " + std::to_string(V.size2) +
-                      ", " + std::to_string(V.vals.size()) + " nonzeros, " + std::to_string(d) +
-                      " x " + std::to_string(nb2) + " blocks");
-  Log::info("mf", "File '" + args.inputRowFacFile + "' is not blocked; it will be blocked automatically");
-  Dense Wf = read_mm_array(args.inputRowFacFile);
+  if (has_test)
+    Log::info("mf", "Test matrix: " + std::to_string(Tm) + " x " + std::to_string(Tn) + ", " +
+                        std::to_string(Tnnz) + " nonzeros, " + std::to_string(d) + " x " +
+                        std::to_string(nb2) + " blocks");
+  Log::info("mf", "Data matrix: " + std::to_string(Vm) + " x " + std::to_string(Vn) + ", " +
+                      std::to_string(Vnnz) + " nonzeros, " + std::to_string(d) + " x " +
+                      std::to_string(nb2) + " blocks");
+  Dense Wf, Hf;
+  if (ends_with(args.inputRowFacFile, ".rm")) {  // both factors from this one descriptor
+    Log::info("mf", "generating factors on the fly...");
+    rmF = load_rm(args.inputRowFacFile);
+    dsgdpp_rm_info(rmF.get(), info_f);
+    Wf.size1 = info_f[0]; Wf.size2 = info_f[2];
+    Hf.size1 = info_f[2]; Hf.size2 = info_f[1];
+  } else {
+    Log::info("mf", "File '" + args.inputRowFacFile + "' is not blocked; it will be blocked automatically");
+    Wf = read_mm_array(args.inputRowFacFile);
+    Log::info("mf", "File '" + args.inputColFacFile + "' is not blocked; it will be blocked automatically");
+    Hf = read_mm_array(args.inputColFacFile);
+  }
   Log::info("mf", "Row factor matrix: " + std::to_string(Wf.size1) + " x " +
                       std::to_string(Wf.size2) + ", " + std::to_string(d) + " x 1 blocks");
-  Log::info("mf", "File '" + args.inputColFacFile + "' is not blocked; it will be blocked automatically");
-  Dense Hf = read_mm_array(args.inputColFacFile);
   Log::info("mf", "Column factor matrix: " + std::to_string(Hf.size1) + " x " +
                       std::to_string(Hf.size2) + ", 1 x " + std::to_string(nb2) + " blocks");
   // conformity (mf/factorization.h:27-33)
-  if (Wf.size1 != V.size1 || Hf.size2 != V.size2 || Wf.size2 != Hf.size1 ||
-      (has_test && (T.size1 != V.size1 || T.size2 != V.size2)))
+  if (Wf.size1 != Vm || Hf.size2 != Vn || Wf.size2 != Hf.size1 ||
+      (has_test && (Tm != Vm || Tn != Vn)))
     throw std::invalid_argument("factor and data matrices do not conform");
   if (Wf.size2 != args.rank)
     Log::info("main", "Warning: --rank differs from the factor files; using " +
                           std::to_string(Wf.size2));
-  const uint64_t m = V.size1, n = V.size2, r = Wf.size2;
+  const uint64_t m = Vm, n = Vn, r = Wf.size2;
   // W: m x r column-major in the file -> row-major; H: r x n column-major = n x r rows
-  std::vector<double> W(m * r), H(n * r);
-  for (uint64_t i = 0; i < m; ++i)
-    for (uint64_t z = 0; z < r; ++z) W[i * r + z] = Wf.colmajor[z * m + i];
-  for (uint64_t j = 0; j < n; ++j)
-    for (uint64_t z = 0; z < r; ++z) H[j * r + z] = Hf.colmajor[j * r + z];
+  std::vector<double> W, H;
+  if (!rmF) {
+    W.resize(m * r);
+    H.resize(n * r);
+    for (uint64_t i = 0; i < m; ++i)
+      for (uint64_t z = 0; z < r; ++z) W[i * r + z] = Wf.colmajor[z * m + i];
+    for (uint64_t j = 0; j < n; ++j)
+      for (uint64_t z = 0; z < r; ++z) H[j * r + z] = Hf.colmajor[j * r + z];
+  }
   auto t1 = std::chrono::steady_clock::now();
   Log::info("main", "Total time for loading matrices: " +
                         fmt_secs((double)std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count()));
@@ -381,12 +426,20 @@ int run(Args& args, const Job& job) {
     dsgdpp_ctx* c;
     ~Guard() { dsgdpp_destroy(c); }
   } guard{ctx};
-  check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TRAIN, V.vals.size(), V.rows.data(), V.cols.data(),
-                               V.vals.data()), "set_matrix");
-  if (has_test)
-    check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TEST, T.vals.size(), T.rows.data(), T.cols.data(),
-                                 T.vals.data()), "set_matrix");
-  check(ctx, dsgdpp_set_factors(ctx, W.data(), H.data()), "set_factors");
+  if (rmV) {
+    check(ctx, dsgdpp_set_matrix_rm(ctx, DSGDPP_TRAIN, rmV.get()), "set_matrix_rm");
+    if (has_test) check(ctx, dsgdpp_set_matrix_rm(ctx, DSGDPP_TEST, rmV.get()), "set_matrix_rm");
+  } else {
+    check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TRAIN, V.vals.size(), V.rows.data(),
+                                 V.cols.data(), V.vals.data()), "set_matrix");
+    if (has_test)
+      check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TEST, T.vals.size(), T.rows.data(),
+                                   T.cols.data(), T.vals.data()), "set_matrix");
+  }
+  if (rmF)
+    check(ctx, dsgdpp_set_factors_rm(ctx, rmF.get()), "set_factors_rm");
+  else
+    check(ctx, dsgdpp_set_factors(ctx, W.data(), H.data()), "set_factors");
   check(ctx, dsgdpp_seed(ctx, args.seed), "seed");
 
   Trace trace;  // Args::createTraceFields (tools/detail/mfdsgd-args.h:53-63)
@@ -430,6 +483,8 @@ int run(Args& args, const Job& job) {
     f << trace.to_r(args.traceVar);
   }
   if (!args.outputRowFacFile.empty() || !args.outputColFacFile.empty()) {
+    W.resize(m * r);  // empty when the factors were generated from a descriptor
+    H.resize(n * r);
     check(ctx, dsgdpp_get_factors(ctx, W.data(), H.data()), "get_factors");
   }
   if (!args.outputRowFacFile.empty()) {

@@ -238,16 +238,6 @@ void write_mm_array(const std::string& path, const Dense& m) {
 // ---- minimal XML for the descriptor -------------------------------------------------
 namespace {
 
-struct XNode {
-  std::string name, text;
-  std::vector<XNode> kids;
-  const XNode* child(const std::string& n) const {
-    for (auto& k : kids)
-      if (k.name == n) return &k;
-    return nullptr;
-  }
-};
-
 struct XParser {
   const std::string& s;
   size_t p = 0;
@@ -284,11 +274,11 @@ struct XParser {
     }
     return o;
   }
-  XNode element() {
+  XmlNode element() {
     skip_misc();
     if (p >= s.size() || s[p] != '<') throw MmError("malformed XML descriptor");
     size_t e = s.find_first_of(" \t\r\n/>", p + 1);
-    XNode n;
+    XmlNode n;
     n.name = s.substr(p + 1, e - p - 1);
     size_t close = s.find('>', p);
     if (close == std::string::npos) throw MmError("malformed XML descriptor");
@@ -318,8 +308,8 @@ struct XParser {
   }
 };
 
-const XNode& need(const XNode& n, const std::string& name) {
-  const XNode* c = n.child(name);
+const XmlNode& need(const XmlNode& n, const std::string& name) {
+  const XmlNode* c = n.child(name);
   if (!c) throw MmError("XML descriptor lacks matrix." + name);
   return *c;
 }
@@ -345,10 +335,27 @@ std::string xml_escape(const std::string& t) {
 
 }  // namespace
 
+const XmlNode* XmlNode::child(const std::string& n) const {
+  for (auto& k : kids)
+    if (k.name == n) return &k;
+  return nullptr;
+}
+
+std::vector<XmlNode> parse_xml(const std::string& text) {
+  XParser P(text);
+  std::vector<XmlNode> out;
+  for (;;) {
+    P.skip_misc();
+    if (P.p >= text.size()) break;
+    out.push_back(P.element());
+  }
+  return out;
+}
+
 BlockedDescriptor read_descriptor(const std::string& path) {
   const std::string s = read_file(path);
   XParser P(s);
-  XNode root = P.element();
+  XmlNode root = P.element();
   if (root.name != "matrix") throw MmError("XML descriptor root is not <matrix>: " + path);
   BlockedDescriptor d;
   d.size1 = to_u64(need(root, "size1").text);

@@ -44,6 +44,16 @@ struct BlockedDescriptor {
 
 bool ends_with(const std::string& s, const std::string& suffix);
 
+// Element tree of the small XML files the reference writes with Boost's
+// property_tree (text trimmed, entities decoded, attributes ignored).
+struct XmlNode {
+  std::string name, text;
+  std::vector<XmlNode> kids;
+  const XmlNode* child(const std::string& n) const;
+};
+// top-level elements in file order (property_tree writes several roots)
+std::vector<XmlNode> parse_xml(const std::string& text);
+
 // Reads a coordinate file with several threads; entries keep file order.
 Coo read_mm_coord(const std::string& path, unsigned threads = 0);
 Dense read_mm_array(const std::string& path);

@@ -382,6 +382,42 @@ int dsgdpp_write_blocked(const char* xml_path, const char* dir, const char* base
 /* Philox4x32-10 of the BF16 stochastic rounding, for known-answer checks */
 void dsgdpp_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
+/* ---- random-matrix descriptors (.rm), generated on the device ----------------
+ * replaces: RandomMatrixDescriptor (mf/matrix/io/randomMatrixDescriptor.h:27-77,
+ * randomMatrixDescriptor_impl.cc:21-176), the .rm branches of getDataMatrices /
+ * getFactors (mf/matrix/io/generateDistributedMatrix_impl.h:655-744) and
+ * tools/mfcreateRandomMatrixFile.cc.  The file format, chunk grid, counts per
+ * chunk and value model (Worig * Horig + noise) are the reference's; the draws
+ * are this library's own counter-based ones (rm.h states them), so a
+ * descriptor gives the same matrices here on every run and device, not the
+ * reference's.  Failures return DSGDPP_E_IO (file, format) or
+ * DSGDPP_E_INVALID, message in dsgdpp_rm_error(). */
+typedef struct dsgdpp_rm dsgdpp_rm;
+const char* dsgdpp_rm_error(void);
+int dsgdpp_rm_load(const char* path, dsgdpp_rm** out);
+/* RandomMatrixDescriptor::create; values / noise: "Normal(mean,stddev)" (the
+ * mean is ignored, as tools/parse.h:80-88 ignores it) or "Uniform(min,max)" */
+int dsgdpp_rm_create(uint64_t size1, uint64_t size2, uint32_t blocks1, uint32_t blocks2,
+                     uint64_t nnz, uint64_t nnz_test, uint32_t rank, const char* values,
+                     const char* noise, dsgdpp_rm** out);
+int dsgdpp_rm_save(const dsgdpp_rm* rm, const char* path);
+void dsgdpp_rm_destroy(dsgdpp_rm* rm);
+/* out[9]: size1, size2, rank, blocks1, blocks2, nnz, nnzTest (as written), and
+ * the data and test nonzeros the chunk counts add up to (0 without a data part) */
+int dsgdpp_rm_info(const dsgdpp_rm* rm, uint64_t* out);
+/* the data (DSGDPP_TRAIN) or test (DSGDPP_TEST) matrix into host arrays of
+ * out[7] / out[8] entries, 0-based; chunk by chunk in row-major chunk order */
+int dsgdpp_rm_generate(const dsgdpp_rm* rm, int which, int device, uint32_t* rows,
+                       uint32_t* cols, double* vals);
+/* Worig (size1 x rank, row-major) and Horig (size2 x rank: column j of the
+ * rank x size2 factor contiguous) */
+int dsgdpp_rm_generate_factors(const dsgdpp_rm* rm, int device, double* W, double* H);
+/* generated straight into the context (no host copy): the data or test
+ * matrix of rm, which must be m x n */
+int dsgdpp_set_matrix_rm(dsgdpp_ctx* ctx, int which, const dsgdpp_rm* rm);
+/* the factors of getFactors(.rm): Worig and Horig of rm (m x n, rank r) */
+int dsgdpp_set_factors_rm(dsgdpp_ctx* ctx, const dsgdpp_rm* rm);
+
 #ifdef __cplusplus
 }
 #endif

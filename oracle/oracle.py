@@ -54,6 +54,11 @@ _SIGS = {
     "orc_run": (C.c_int, [_P, C.c_uint32, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                           _f64p]),
     "orc_bold_driver": (C.c_double, [C.c_double, _f64p, C.c_double, C.c_double, C.c_double]),
+    "orc_rm_factor": (None, [C.c_int, C.c_double, C.c_double, _u32p, C.c_uint64, C.c_uint64,
+                             C.c_uint32, C.c_uint32, _f64p]),
+    "orc_rm_data": (C.c_uint64, [C.c_int, C.c_double, C.c_double, _u32p, _u64p, C.c_uint64,
+                                 C.c_uint64, C.c_uint64, C.c_uint64, _f64p, _f64p, C.c_uint32,
+                                 _u32p, _u32p, _f64p]),
 }
 
 
@@ -250,3 +255,70 @@ class Problem:
         lib.orc_run(self._h, epochs, 1 if decay == "BoldDriver" else 0, eps0, dec, inc, threads,
                     _p(tr, C.c_double))
         return tr
+
+
+# ---- .rm descriptors (rm_oracle.cc) ------------------------------------------------
+def read_rm(path):
+    """The property_tree XML of a .rm descriptor (randomMatrixDescriptor_impl.cc:21-91),
+    read with Python's own XML parser: a dict of sizes, specs, seeds and counts."""
+    import re
+    import xml.etree.ElementTree as ET
+    text = open(path).read()
+    text = re.sub(r"<\?xml[^>]*\?>", "", text)
+    root = ET.fromstring("<root>" + text + "</root>")
+    num = lambda tag: int(root.find(tag).text.strip())
+    d = dict(size1=num("size1"), size2=num("size2"), blocks1=num("blocks1"),
+             blocks2=num("blocks2"), nnz=num("nnz"), nnzTest=num("nnzTest"), rank=num("rank"),
+             values=(root.find("values").text or "").strip(),
+             noise=(root.find("noise").text or "").strip())
+    d["Worig"] = [int(e.text) for e in root.find("Worig")]
+    d["Horig"] = [int(e.text) for e in root.find("Horig")]
+    if d["nnz"] and d["nnzTest"]:
+        for part in ("V", "Vtest"):
+            d[part + ".seeds"] = [int(e.text) for e in root.find(part).find("seeds")]
+            d[part + ".nnzs"] = [int(e.text) for e in root.find(part).find("nnzs")]
+    return d
+
+
+def parse_dist(spec):
+    """(kind, a, b): Normal -> 0, Uniform -> 1, empty -> -1 (tools/parse.h:75-110)."""
+    spec = (spec or "").strip()
+    if not spec:
+        return -1, 0.0, 0.0
+    name, args = spec.split("(", 1)
+    a, b = [float(x) for x in args.rstrip(")").split(",")]
+    return {"Normal": 0, "Uniform": 1}[name.strip()], a, b
+
+
+def rm_factors(d):
+    """Worig (size1 x rank) and Horig (size2 x rank), row-major."""
+    kind, a, b = parse_dist(d["values"])
+    out = []
+    for rows, key, tag, blocks in ((d["size1"], "Worig", 1, d["blocks1"]),
+                                   (d["size2"], "Horig", 2, d["blocks2"])):
+        seeds = np.ascontiguousarray(d[key], np.uint32)
+        X = np.empty((rows, d["rank"]), np.float64)
+        lib.orc_rm_factor(kind, a, b, _p(seeds, C.c_uint32), blocks, rows, d["rank"], tag,
+                          _p(X, C.c_double))
+        out.append(X)
+    return out[0], out[1]
+
+
+def rm_data(d, which, W, H):
+    """The data (which=0, with noise) or test (which=1) matrix: rows, cols, vals."""
+    part = "V" if which == 0 else "Vtest"
+    seeds = np.ascontiguousarray(d[part + ".seeds"], np.uint32)
+    counts = np.ascontiguousarray(d[part + ".nnzs"], np.uint64)
+    total = int(counts.sum())
+    kind, a, b = parse_dist(d["noise"]) if which == 0 else (-1, 0.0, 0.0)
+    rows = np.empty(total, np.uint32)
+    cols = np.empty(total, np.uint32)
+    vals = np.empty(total, np.float64)
+    W = np.ascontiguousarray(W, np.float64)
+    H = np.ascontiguousarray(H, np.float64)
+    n = lib.orc_rm_data(kind, a, b, _p(seeds, C.c_uint32), _p(counts, C.c_uint64), d["blocks1"],
+                        d["blocks2"], d["size1"], d["size2"], _p(W, C.c_double),
+                        _p(H, C.c_double), d["rank"], _p(rows, C.c_uint32), _p(cols, C.c_uint32),
+                        _p(vals, C.c_double))
+    assert n == total
+    return rows, cols, vals
