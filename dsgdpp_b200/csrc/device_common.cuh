@@ -81,13 +81,24 @@ __host__ __device__ inline Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
   return r;
 }
 
-// fp32 -> bf16 with stochastic rounding: add 16 random bits below the bf16
-// mantissa and truncate, so the magnitude rounds up with probability equal to
-// the discarded fraction.
-__device__ inline uint32_t bf16_sr_bits(float x, uint32_t rnd16) {
-  uint32_t b = __float_as_uint(x);
-  if ((b & 0x7f800000u) == 0x7f800000u) return b >> 16;  // inf / nan unchanged
-  return (b + (rnd16 & 0xffffu)) >> 16;
+// Two fp32 values -> packed bf16x2 with stochastic rounding, one sm_100a
+// instruction: each value gets 16 random bits added below the bf16 mantissa
+// and is truncated, so its magnitude rounds up with probability equal to the
+// discarded fraction.  The lower half comes from `lo` with the lower 16 bits
+// of `rbits`, the upper half from `hi` with the upper 16 (measured on B200:
+// identical, for finite values, to (bits(x) + r16) >> 16 per half).
+__device__ __forceinline__ uint32_t bf16x2_sr(float lo, float hi, uint32_t rbits) {
+  uint32_t d;
+  asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+  return d;
+}
+
+// a - b on packed bf16x2, rounded to nearest (the exact difference when the
+// two values lie a few ulps apart)
+__device__ __forceinline__ uint32_t bf16x2_sub(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("sub.rn.bf16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
 }
 
 // One sub-epoch segment: the records of block (id, schedule[s][id]).

@@ -49,11 +49,7 @@ __device__ __forceinline__ void store_vec<__nv_bfloat16>(__nv_bfloat16* p, const
                                                          const Philox4* rnd) {
   uint32_t w[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    uint32_t lo = bf16_sr_bits(f[2 * k], rnd->v[k]);
-    uint32_t hi = bf16_sr_bits(f[2 * k + 1], rnd->v[k] >> 16);
-    w[k] = (lo & 0xffffu) | (hi << 16);
-  }
+  for (int k = 0; k < 4; ++k) w[k] = bf16x2_sr(f[2 * k], f[2 * k + 1], rnd->v[k]);
   *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
@@ -67,18 +63,7 @@ __device__ __forceinline__ void red_bf16_increment(__nv_bfloat16* q, const uint4
   const uint32_t ow[4] = {old.x, old.y, old.z, old.w};
   uint32_t inc[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    uint32_t halves = 0;
-#pragma unroll
-    for (int hlf = 0; hlf < 2; ++hlf) {
-      const uint32_t rbits = (ow[k] >> (16 * hlf)) & 0xffffu;
-      const uint32_t tbits = bf16_sr_bits(nv[2 * k + hlf], rnd.v[k] >> (16 * hlf)) & 0xffffu;
-      const float d = __uint_as_float(tbits << 16) - __uint_as_float(rbits << 16);
-      const uint32_t dbits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(d));
-      halves |= dbits << (16 * hlf);
-    }
-    inc[k] = halves;
-  }
+  for (int k = 0; k < 4; ++k) inc[k] = bf16x2_sub(bf16x2_sr(nv[2 * k], nv[2 * k + 1], rnd.v[k]), ow[k]);
   asm volatile("red.relaxed.gpu.global.add.noftz.v4.bf16x2 [%0], {%1, %2, %3, %4};"
                ::"l"(q), "r"(inc[0]), "r"(inc[1]), "r"(inc[2]), "r"(inc[3]) : "memory");
 }
