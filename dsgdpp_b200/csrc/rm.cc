@@ -129,6 +129,8 @@ void rm_validate(const RmDesc& d) {
   if (d.rank == 0 || d.rank > 4096) throw MmError("random matrix descriptor: rank must lie in [1, 4096]");
   if (d.chunks1 == 0 || d.chunks2 == 0 || d.chunks1 > d.size1 || d.chunks2 > d.size2)
     throw MmError("random matrix descriptor: blocks1/blocks2 must lie in [1, size]");
+  if (d.chunks1 * d.chunks2 >= (1ull << 31))
+    throw MmError("random matrix descriptor: blocks1 x blocks2 must stay below 2^31");
   if (d.seeds_w.size() != d.chunks1 || d.seeds_h.size() != d.chunks2)
     throw MmError("random matrix descriptor: one Worig seed per row block and one Horig seed per column block are required");
   parse_dist("values", d.values);
