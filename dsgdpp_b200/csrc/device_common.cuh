@@ -81,6 +81,28 @@ __host__ __device__ inline Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
   return r;
 }
 
+// 32-bit finalizer of MurmurHash3 (Appleby): a bijection with full avalanche.
+__host__ __device__ inline uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Random bits of one stochastically rounded vector write: a Philox-4x32-10
+// block drawn once per chunk and lane (`base`) is expanded per write by
+// fmix32(word + tag * golden ratio), the tag distinct per record, vector and
+// side within the chunk -- 128 fresh bits per vector for two multiplies per
+// word instead of a 10-round Philox call.
+__host__ __device__ inline Philox4 sr_expand(const Philox4& base, uint32_t tag) {
+  Philox4 r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.v[k] = fmix32(base.v[k] + tag * 0x9E3779B9u);
+  return r;
+}
+
 // Two fp32 values -> packed bf16x2 with stochastic rounding, one sm_100a
 // instruction: each value gets 16 random bits added below the bf16 mantissa
 // and is truncated, so its magnitude rounds up with probability equal to the

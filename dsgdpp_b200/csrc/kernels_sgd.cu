@@ -75,7 +75,7 @@ template <typename T, bool ATOMIC>
 __device__ __forceinline__ void write_vec(T* p, const uint4& old,
                                           const typename Elem<T>::C (&was)[Elem<T>::VW],
                                           const typename Elem<T>::C (&now)[Elem<T>::VW],
-                                          uint64_t rec, uint32_t tag, const EpochParams& ep) {
+                                          const Philox4& base, uint32_t tag) {
   constexpr int VW = Elem<T>::VW;
   constexpr bool kSR = sizeof(T) == 2;
   if constexpr (ATOMIC && !kSR) {
@@ -88,8 +88,7 @@ __device__ __forceinline__ void write_vec(T* p, const uint4& old,
     }
   } else {
     Philox4 rnd;
-    if constexpr (kSR)
-      rnd = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, tag, ep.key0, ep.key1);
+    if constexpr (kSR) rnd = sr_expand(base, tag);
     if constexpr (ATOMIC && kSR)
       red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(p), old, now, rnd);
     else
@@ -118,7 +117,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
                                           typename Elem<T>::C my_b, typename Elem<T>::C eps,
                                           typename Elem<T>::C cwh, typename Elem<T>::C rw,
                                           typename Elem<T>::C rh, typename Elem<T>::C tmin,
-                                          typename Elem<T>::C tmax, const EpochParams& ep,
+                                          typename Elem<T>::C tmax, const Philox4& base,
                                           uint32_t grp, uint32_t gl) {
   using E = Elem<T>;
   using C = typename E::C;
@@ -129,7 +128,8 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   uint4 hv0[VPL];        // ... as loaded
   C h0[VPL][VW];         // ... unpacked as loaded
   C hf[VPL][VW];         // ... as updated so far
-  uint64_t last_rec = 0;
+  uint32_t last_t = 0;  // the run's last record in the group (its H write tag)
+  // write tags: record t of the group, vector v: 2 (t VPL + v) for W, + 1 for H
 #pragma unroll 1
   for (int t = 0; t < LPN; ++t) {
     const uint32_t ri = grp * LPN + t;
@@ -149,8 +149,8 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
       for (int v = 0; v < VPL; ++v) {
         const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
         if (e0 < a.rp)
-          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], last_rec,
-                               e0 | 0x80000000u, ep);
+          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
+                               2u * (last_t * VPL + v) + 1u);
       }
       cur = kNone;
     }
@@ -184,7 +184,6 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
     if (!valid) continue;
     const C f1 = (C)-2 * eps * (x - dot * cwh);
     const C fw = f1 * rw, fh = f1 * rh;
-    const uint64_t rec = rb + ri;
 #pragma unroll
     for (int v = 0; v < VPL; ++v) {
       const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
@@ -203,19 +202,19 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
             nh[e] = clampw(nh[e], tmin, tmax, eps);
           }
       }
-      write_vec<T, ATOMIC>(wp + e0, wv[v], wf[v], nw, rec, e0, ep);
+      write_vec<T, ATOMIC>(wp + e0, wv[v], wf[v], nw, base, 2u * ((uint32_t)t * VPL + v));
 #pragma unroll
       for (int e = 0; e < VW; ++e) hf[v][e] = nh[e];
     }
-    last_rec = rec;
+    last_t = (uint32_t)t;
   }
   if (cur != kNone) {
 #pragma unroll
     for (int v = 0; v < VPL; ++v) {
       const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
       if (e0 < a.rp)
-        write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], last_rec,
-                             e0 | 0x80000000u, ep);
+        write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
+                             2u * (last_t * VPL + v) + 1u);
     }
   }
 }
@@ -307,9 +306,14 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
       }
     }
 
+    // stochastic rounding: one Philox block per chunk and lane (counter:
+    // first record of the chunk, epoch, lane; key: the epoch's key)
+    Philox4 base{};
+    if constexpr (kSR)
+      base = philox4x32_10((uint32_t)rb, (uint32_t)(rb >> 32), ep.epoch, lane, ep.key0, ep.key1);
     if constexpr (RUNS) {
       run_chunk<T, LPN, VPL, ATOMIC>(a, W, H, rb, nrec, my_row, my_col, my_x, my_a, my_b, eps,
-                                     cwh, rw, rh, tmin, tmax, ep, grp, gl);
+                                     cwh, rw, rh, tmin, tmax, base, grp, gl);
     } else {
       for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
         const uint32_t ri = t0 + grp;
@@ -366,7 +370,6 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
                 nh[e] = clampw(nh[e], tmin, tmax, eps);
               }
           }
-          const uint64_t rec = rb + ri;
           if constexpr (ATOMIC && !kSR) {
             // add the update, so concurrent updates of one row are not lost
             if constexpr (sizeof(T) == 4) {
@@ -383,10 +386,10 @@ __global__ void __launch_bounds__(256) hogwild_subepoch_kernel(HogwildArgs a, ui
             }
           } else {
             Philox4 r1, r2;
-            if constexpr (kSR) {
-              r1 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0, ep.key0, ep.key1);
-              r2 = philox4x32_10((uint32_t)rec, (uint32_t)(rec >> 32), ep.epoch, e0 | 0x80000000u,
-                                 ep.key0, ep.key1);
+            if constexpr (kSR) {  // tags: iteration t0 / NG of this group, vector v, side
+              const uint32_t tg = 2u * ((t0 / NG) * VPL + v);
+              r1 = sr_expand(base, tg);
+              r2 = sr_expand(base, tg + 1u);
             }
             if constexpr (ATOMIC && kSR) {
               red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(wp + e0), wv[v], nw, r1);
@@ -524,8 +527,11 @@ __global__ void __launch_bounds__(256) hogwild_epoch_kernel(HogwildArgs a, Epoch
         my_b = f2;
       }
     }
+    Philox4 base{};
+    if constexpr (sizeof(T) == 2)
+      base = philox4x32_10((uint32_t)rb, (uint32_t)(rb >> 32), ep.epoch, lane, ep.key0, ep.key1);
     run_chunk<T, LPN, VPL, true, true>(a, W, H, rb, nrec, my_row, my_col, my_x, my_a, my_b, eps,
-                                       cwh, rw, rh, tmin, tmax, ep, grp, gl);
+                                       cwh, rw, rh, tmin, tmax, base, grp, gl);
     __threadfence();  // this lane's writes, before the chunk counts as done
     __syncwarp();
     if (lane == 0) atomicAdd(dp.done + me, 1u);
