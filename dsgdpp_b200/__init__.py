@@ -15,6 +15,27 @@ The classes mirror the reference's C++ entry points:
   :func:`point_orders`, :func:`block_offsets` -- host-side random draws and
   blocking (mf/sgd/dsgdpp_impl.h:282-349, mf/sgd/dsgd_impl.h:246-325,
   mf/sgd/sgd_impl.h:197-351, mf/matrix/distributed_matrix_impl.cc:24-40).
+* :class:`RandomMatrix` -- a ``.rm`` random-matrix descriptor
+  (mf/matrix/io/randomMatrixDescriptor.h); ``Context.set_matrix_rm`` and
+  ``Context.set_factors_rm`` generate its matrices on the device.
+* :class:`Batch` -- many small independent factorizations in one launch
+  sequence; :class:`Mlp` and ``Context.run_controlled`` -- the learned
+  step-size controller.
+* :func:`read_sparse`, :func:`read_mm_array`, :func:`write_mm_coord`,
+  :func:`write_mm_array`, :func:`write_blocked` -- the MatrixMarket and
+  blocked ``.xml`` files of mf/matrix/io.
+
+Example::
+
+    import dsgdpp_b200 as P
+    cfg = P.Config(m=m, n=n, rank=32, d=64, precision="fp32")
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, rows, cols, vals)      # 0-based coordinates
+        ctx.set_matrix(P.TEST, trows, tcols, tvals)
+        ctx.set_factors(W, H)                          # m x r and n x r, FP64
+        ctx.seed(1)
+        trace = ctx.run(50, "BoldDriver", 0.001)       # one dict per epoch
+        W, H = ctx.get_factors()
 """
 from __future__ import annotations
 
