@@ -246,6 +246,9 @@ void destroy_impl(dsgdpp_ctx* c) {
   if (c->ev_begin) cudaEventDestroy(c->ev_begin);
   if (c->ev_end) cudaEventDestroy(c->ev_end);
   if (c->ev_inputs) cudaEventDestroy(c->ev_inputs);
+  if (c->ev_coords) cudaEventDestroy(c->ev_coords);
+  if (c->ev_vals) cudaEventDestroy(c->ev_vals);
+  if (c->side) cudaStreamDestroy(c->side);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -369,12 +372,33 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   unsigned long long* d_bad = cv.take<unsigned long long>(1);
   void* tmp = cv.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
 
+  // The coordinates are copied first; the values (half the bytes) follow on
+  // a side stream while the keys are built and sorted, and are waited for
+  // only where the merge needs them.  The guard waits for that copy on every
+  // exit, so no copy outlives the call (the caller may free its arrays).
+  struct SideGuard {
+    cudaStream_t s = nullptr;
+    ~SideGuard() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } side_guard;
+  bool vals_on_side = false;
   if (fill) {
     (*fill)(t_rows, t_cols, t_vals, st);
   } else {
+    if (!c->side) {
+      check_cuda(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "side stream");
+      check_cuda(cudaEventCreateWithFlags(&c->ev_coords, cudaEventDisableTiming), "event");
+      check_cuda(cudaEventCreateWithFlags(&c->ev_vals, cudaEventDisableTiming), "event");
+    }
     check_cuda(cudaMemcpyAsync(t_rows, rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
     check_cuda(cudaMemcpyAsync(t_cols, cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
-    check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+    check_cuda(cudaEventRecord(c->ev_coords, st), "event");
+    check_cuda(cudaStreamWaitEvent(c->side, c->ev_coords, 0), "wait");
+    side_guard.s = c->side;
+    check_cuda(cudaMemcpyAsync(t_vals, vals, nnz * 8, cudaMemcpyHostToDevice, c->side), "H2D vals");
+    check_cuda(cudaEventRecord(c->ev_vals, c->side), "event");
+    vals_on_side = true;
   }
   check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
   BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
@@ -403,6 +427,7 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   check_cuda(cudaStreamSynchronize(st), "sync");
   const uint64_t u = (uint64_t)last_pos + last_flag;
 
+  if (vals_on_side) check_cuda(cudaStreamWaitEvent(st, c->ev_vals, 0), "wait values");
   check_cuda(launch_merge_runs(g, skeys, sidx, pos, nnz, t_vals, t_rows, t_cols, okeys, urow,
                                ucol, uval, st), "merge_runs");
   uint64_t* ukeys = okeys;

@@ -133,6 +133,9 @@ struct dsgdpp_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   // timing / ordering
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_inputs = nullptr;
+  // set_matrix: the values travel on a side stream while the keys are sorted
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_coords = nullptr, ev_vals = nullptr;
   bool epoch_timed = false;
   // per-kernel timing of the Hogwild sub-epoch kernels (stream launch only)
   bool profiling = false;
