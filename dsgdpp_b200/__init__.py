@@ -203,6 +203,8 @@ SIGNATURES = {
     "dsgdpp_rm_generate": (C.c_int, [_P, C.c_int, C.c_int, _u32p, _u32p, _f64p]),
     "dsgdpp_rm_generate_factors": (C.c_int, [_P, C.c_int, _f64p, _f64p]),
     "dsgdpp_set_matrix_rm": (C.c_int, [_P, C.c_int, _P]),
+    "dsgdpp_set_blocks": (C.c_int, [_P, C.c_int, _u64p, _u32p, _u32p, _f64p]),
+    "dsgdpp_set_counts": (C.c_int, [_P, _u64p, _u64p]),
     "dsgdpp_set_factors_rm": (C.c_int, [_P, _P]),
 }
 
@@ -332,6 +334,22 @@ class Context:
         w, h = _f64(W), _f64(H)
         self._check(lib.dsgdpp_set_factors(self._h, _ptr(w, C.c_double), _ptr(h, C.c_double)),
                     "set_factors")
+
+    def set_blocks(self, which: int, block_nnz, local_rows, local_cols, vals):
+        """Blocks one after another (row-major block order) with block-local
+        coordinates, as the reference's blocked matrix holds them."""
+        bn = np.ascontiguousarray(block_nnz, np.uint64)
+        r, c, v = _u32(local_rows), _u32(local_cols), _f64(vals)
+        self._check(lib.dsgdpp_set_blocks(self._h, which, _ptr(bn, C.c_uint64),
+                                          _ptr(r, C.c_uint32), _ptr(c, C.c_uint32),
+                                          _ptr(v, C.c_double)), "set_blocks")
+
+    def set_counts(self, nnz1, nnz2):
+        """Per-row and per-column training counts (weights of Nzsl_L2)."""
+        a = np.ascontiguousarray(nnz1, np.uint64)
+        b = np.ascontiguousarray(nnz2, np.uint64)
+        self._check(lib.dsgdpp_set_counts(self._h, _ptr(a, C.c_uint64), _ptr(b, C.c_uint64)),
+                    "set_counts")
 
     def set_matrix_rm(self, which: int, rm: "RandomMatrix"):
         """The data (TRAIN) or test (TEST) matrix of a .rm descriptor, generated

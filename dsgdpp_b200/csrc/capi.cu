@@ -884,6 +884,76 @@ int dsgdpp_set_matrix(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* ro
   });
 }
 
+// small device buffer freed on scope exit (set-up calls only)
+struct TempDev {
+  void* p = nullptr;
+  explicit TempDev(size_t bytes) { check_cuda(cudaMalloc(&p, bytes ? bytes : 1), "cudaMalloc"); }
+  ~TempDev() { cudaFree(p); }
+};
+
+int dsgdpp_set_blocks(dsgdpp_ctx* c, int which, const uint64_t* block_nnz,
+                      const uint32_t* local_rows, const uint32_t* local_cols,
+                      const double* vals) {
+  return guarded(c, [&]() {
+    if (!block_nnz) throw Error(DSGDPP_E_INVALID, "null block_nnz");
+    const uint32_t nblocks = c->d * c->nb2;
+    std::vector<uint64_t> start(nblocks + 1, 0);
+    for (uint32_t b = 0; b < nblocks; ++b) start[b + 1] = start[b] + block_nnz[b];
+    const uint64_t nnz = start[nblocks];
+    if (nnz > 0 && (!local_rows || !local_cols || !vals))
+      throw Error(DSGDPP_E_INVALID, "null input array");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    const DeviceFill fill = [&](uint32_t* r, uint32_t* col, double* v, cudaStream_t st) {
+      TempDev tmp((nblocks + 1) * 8 + 8);
+      uint64_t* d_start = static_cast<uint64_t*>(tmp.p);
+      unsigned long long* d_bad = reinterpret_cast<unsigned long long*>(d_start + nblocks + 1);
+      check_cuda(cudaMemcpyAsync(r, local_rows, nnz * 4, cudaMemcpyHostToDevice, st), "H2D rows");
+      check_cuda(cudaMemcpyAsync(col, local_cols, nnz * 4, cudaMemcpyHostToDevice, st), "H2D cols");
+      check_cuda(cudaMemcpyAsync(v, vals, nnz * 8, cudaMemcpyHostToDevice, st), "H2D vals");
+      check_cuda(cudaMemcpyAsync(d_start, start.data(), (nblocks + 1) * 8, cudaMemcpyHostToDevice,
+                                 st), "H2D block starts");
+      check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
+      check_cuda(launch_shift_blocks(d_start, nblocks, c->nb2, c->d_off1, c->d_off2, nnz, r, col,
+                                     d_bad, st), "shift_blocks");
+      unsigned long long bad = 0;
+      check_cuda(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st), "D2H");
+      check_cuda(cudaStreamSynchronize(st), "sync");
+      if (bad)
+        throw Error(DSGDPP_E_INVALID, std::to_string(bad) + " entries lie outside their block");
+    };
+    set_matrix_impl(c, which, nnz, nullptr, nullptr, nullptr, &fill);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_counts(dsgdpp_ctx* c, const uint64_t* nnz1, const uint64_t* nnz2) {
+  return guarded(c, [&]() {
+    if (!nnz1 || !nnz2) throw Error(DSGDPP_E_INVALID, "null count array");
+    if (!c->mat[DSGDPP_TRAIN].present) throw Error(DSGDPP_E_STATE, "no training matrix");
+    const uint64_t m = c->cfg.m, n = c->cfg.n;
+    for (uint64_t i = 0; i < m; ++i)
+      if (nnz1[i] >> 32) throw Error(DSGDPP_E_INVALID, "a row count exceeds 2^32 - 1");
+    for (uint64_t j = 0; j < n; ++j)
+      if (nnz2[j] >> 32) throw Error(DSGDPP_E_INVALID, "a column count exceeds 2^32 - 1");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    cudaStream_t st = c->stream;
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    TempDev tmp((m + n) * 8);
+    uint64_t* d = static_cast<uint64_t*>(tmp.p);
+    check_cuda(cudaMemcpyAsync(d, nnz1, m * 8, cudaMemcpyHostToDevice, st), "H2D nnz1");
+    check_cuda(cudaMemcpyAsync(d + m, nnz2, n * 8, cudaMemcpyHostToDevice, st), "H2D nnz2");
+    check_cuda(launch_counts_to_u32(d, m, c->cnt1, st), "nnz1");
+    check_cuda(launch_counts_to_u32(d + m, n, c->cnt2, st), "nnz2");
+    if (c->inv1) {
+      const bool as_double = c->cfg.precision == kFp64;
+      check_cuda(launch_inverse_counts(c->cnt1, m, c->inv1, as_double, st), "inv1");
+      check_cuda(launch_inverse_counts(c->cnt2, n, c->inv2, as_double, st), "inv2");
+    }
+    check_cuda(cudaStreamSynchronize(st), "sync");
+    return DSGDPP_OK;
+  });
+}
+
 int dsgdpp_set_matrix_rm(dsgdpp_ctx* c, int which, const dsgdpp_rm* rm) {
   return guarded(c, [&]() {
     if (!rm) throw Error(DSGDPP_E_INVALID, "null descriptor");

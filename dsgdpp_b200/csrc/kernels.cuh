@@ -197,6 +197,14 @@ cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_
 cudaError_t launch_offset_copy(const uint32_t* rows_in, const uint32_t* cols_in, uint64_t nnz,
                                uint32_t row0, uint32_t col0, uint32_t* rows_out,
                                uint32_t* cols_out, cudaStream_t st);
+// block-local -> global coordinates of concatenated blocks (start: nblocks+1
+// prefix of the block sizes, row-major blocks); counts entries outside their block
+cudaError_t launch_shift_blocks(const uint64_t* start, uint32_t nblocks, uint32_t nb2,
+                                const uint64_t* off1, const uint64_t* off2, uint64_t nnz,
+                                uint32_t* rows, uint32_t* cols, unsigned long long* bad,
+                                cudaStream_t st);
+cudaError_t launch_counts_to_u32(const uint64_t* in, uint64_t len, uint32_t* out,
+                                 cudaStream_t st);
 cudaError_t launch_count_nnz12(const uint32_t* row, const uint32_t* col, uint64_t nnz,
                                uint32_t* cnt1, uint32_t* cnt2, cudaStream_t st);
 cudaError_t launch_inverse_counts(const uint32_t* cnt, uint64_t len, void* inv,

@@ -136,6 +136,32 @@ __global__ void offset_copy_kernel(const uint32_t* rows_in, const uint32_t* cols
   }
 }
 
+// Block-local coordinates of blocks stored one after another (block b holds
+// entries [start[b], start[b+1])) -> global ones; entries outside their block
+// are counted in *bad and left as they are.
+__global__ void shift_blocks_kernel(const uint64_t* start, uint32_t nblocks, uint32_t nb2,
+                                    const uint64_t* off1, const uint64_t* off2, uint64_t nnz,
+                                    uint32_t* rows, uint32_t* cols, unsigned long long* bad) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    const uint32_t b = find_block(start, nblocks, k);
+    const uint32_t b1 = b / nb2, b2 = b - b1 * nb2;
+    const uint64_t i = rows[k], j = cols[k];
+    if (i >= off1[b1 + 1] - off1[b1] || j >= off2[b2 + 1] - off2[b2]) {
+      atomicAdd(bad, 1ull);
+      continue;
+    }
+    rows[k] = (uint32_t)(i + off1[b1]);
+    cols[k] = (uint32_t)(j + off2[b2]);
+  }
+}
+
+__global__ void counts_to_u32_kernel(const uint64_t* in, uint64_t len, uint32_t* out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < len; k += stride)
+    out[k] = (uint32_t)in[k];
+}
+
 __global__ void count_nnz12_kernel(const uint32_t* row, const uint32_t* col, uint64_t nnz,
                                    uint32_t* cnt1, uint32_t* cnt2) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -252,6 +278,22 @@ cudaError_t launch_offset_copy(const uint32_t* rows_in, const uint32_t* cols_in,
   const uint64_t blocks = std::min<uint64_t>((nnz + 255) / 256, 4096);
   offset_copy_kernel<<<(unsigned)blocks, 256, 0, st>>>(rows_in, cols_in, nnz, row0, col0,
                                                        rows_out, cols_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shift_blocks(const uint64_t* start, uint32_t nblocks, uint32_t nb2,
+                                const uint64_t* off1, const uint64_t* off2, uint64_t nnz,
+                                uint32_t* rows, uint32_t* cols, unsigned long long* bad,
+                                cudaStream_t st) {
+  if (nnz == 0) return cudaSuccess;
+  shift_blocks_kernel<<<kGrid, 256, 0, st>>>(start, nblocks, nb2, off1, off2, nnz, rows, cols, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_counts_to_u32(const uint64_t* in, uint64_t len, uint32_t* out,
+                                 cudaStream_t st) {
+  if (len == 0) return cudaSuccess;
+  counts_to_u32_kernel<<<kGrid, 256, 0, st>>>(in, len, out);
   return cudaGetLastError();
 }
 

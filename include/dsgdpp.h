@@ -150,6 +150,21 @@ int dsgdpp_abi_version(void);
  * matrix this also counts nnz1 / nnz2 (mf/matrix/op/nnz.h:124-163). */
 int dsgdpp_set_matrix(dsgdpp_ctx* ctx, int which, uint64_t nnz, const uint32_t* rows,
                       const uint32_t* cols, const double* vals);
+/* replaces: the blocked DistributedMatrix the runner works on (block-local
+ * coordinates, read_impl.h:421): the d x 2d (d x d for DSGD) blocks one after
+ * another in row-major block order, block b holding block_nnz[b] entries with
+ * 0-based coordinates inside the block.  The block extents must be the
+ * context's (computeDefaultBlockOffsets); an entry outside its block is an
+ * error (DSGDPP_E_INVALID).  Otherwise the same as dsgdpp_set_matrix. */
+int dsgdpp_set_blocks(dsgdpp_ctx* ctx, int which, const uint64_t* block_nnz,
+                      const uint32_t* local_rows, const uint32_t* local_cols,
+                      const double* vals);
+/* replaces: the nnz12 counts of DistributedFactorizationData::init
+ * (mf/factorization.h:202-208) with counts the caller holds (m and n
+ * entries, each below 2^32), e.g. counted over more data than this context
+ * holds.  Call after dsgdpp_set_matrix of the training matrix, which counts
+ * them itself and would replace them. */
+int dsgdpp_set_counts(dsgdpp_ctx* ctx, const uint64_t* nnz1, const uint64_t* nnz2);
 /* replaces: getFactors (generateDistributedMatrix_impl.h:655-690) */
 int dsgdpp_set_factors(dsgdpp_ctx* ctx, const double* W, const double* H);
 /* replaces: unblock + the factor arrays read by writeMatrix (tools/mfdsgdpp.cc:145-159) */

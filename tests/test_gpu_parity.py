@@ -457,3 +457,84 @@ def test_dsgd_blocking_limits_and_batch_rejection():
                 H=p.H0[:, :4])
     with pytest.raises(P.DsgdppError):
         P.Batch(P.Config(m=1, n=1, rank=1, d=1, method="dsgd"), [prob])
+
+
+# ---- blocked input and caller-held counts (the runner's own data form) ---------------
+def _oracle_blocks(ref, d, nb2, which=0):
+    parts = [ref.block_records(b1, b2, which) for b1 in range(d) for b2 in range(nb2)]
+    bn = np.array([len(x) for _, _, x in parts], np.uint64)
+    cat = lambda k: np.concatenate([p[k] for p in parts]) if len(parts) else np.empty(0)
+    return bn, cat(0), cat(1), cat(2)
+
+
+@pytest.mark.parametrize("method", ["dsgdpp", "dsgd"])
+def test_set_blocks_matches_set_matrix_and_oracle(method):
+    p = _problem()
+    d = 3
+    nb2 = d if method == "dsgd" else 2 * d
+    ref = O.Problem(p.m, p.n, 10, d, p.rows, p.cols, p.vals, p.trows, p.tcols, p.tvals,
+                    method=method)
+    ref.configure(update_lambda=0.5)
+    ref.set_factors(p.W0, p.H0)
+    cfg = P.Config(m=p.m, n=p.n, rank=10, d=d, precision="fp64", exec="replay", method=method,
+                   update_lambda=0.5)
+    bn, li, lj, lx = _oracle_blocks(ref, d, nb2)
+    tbn, ti, tj, tx = _oracle_blocks(ref, d, nb2, which=1)
+    with P.Context(cfg) as ctx:
+        ctx.set_blocks(P.TRAIN, bn, li, lj, lx)
+        ctx.set_blocks(P.TEST, tbn, ti, tj, tx)
+        ctx.set_factors(p.W0, p.H0)
+        np.testing.assert_array_equal(ctx.block_nnz(P.TRAIN).ravel(), bn)
+        a1, a2, _ = ctx.nnz12()
+        r1, r2, _ = ref.nnz12()
+        np.testing.assert_array_equal(a1, r1)
+        np.testing.assert_array_equal(a2, r2)
+        ctx.seed(11)
+        ref.seed(11)
+        for _ in range(2):
+            ctx.epoch(0.02)
+            ref.epoch(0.02)
+        W, H = ctx.get_factors()
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+        assert ctx.nzsl(P.TEST) == pytest.approx(ref.nzsl(1), rel=LOSS_RTOL)
+
+
+def test_set_blocks_rejects_entries_outside_their_block():
+    p = _problem(m=60, n=40, nnz=300, ntest=30)
+    d = 2
+    cfg = P.Config(m=p.m, n=p.n, rank=4, d=d)
+    bn = np.zeros(d * 2 * d, np.uint64)
+    bn[0] = 2
+    with P.Context(cfg) as ctx:
+        # block (0, 0) spans rows [0, 30) and columns [0, 10)
+        with pytest.raises(P.DsgdppError, match="outside their block"):
+            ctx.set_blocks(P.TRAIN, bn, [0, 30], [0, 1], [1.0, 2.0])
+        with pytest.raises(P.DsgdppError, match="outside their block"):
+            ctx.set_blocks(P.TRAIN, bn, [0, 1], [0, 10], [1.0, 2.0])
+        ctx.set_blocks(P.TRAIN, bn, [0, 29], [0, 9], [1.0, 2.0])
+        assert int(ctx.block_nnz(P.TRAIN).sum()) == 2
+
+
+def test_set_counts_replaces_the_update_weights():
+    p = _problem()
+    cfg = dict(m=p.m, n=p.n, rank=10, d=3, precision="fp64", exec="replay")
+    with P.Context(P.Config(**cfg)) as a, P.Context(P.Config(**cfg)) as b:
+        for ctx in (a, b):
+            ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+            ctx.set_factors(p.W0, p.H0)
+            ctx.seed(4)
+        n1, n2, _ = a.nnz12()
+        b.set_counts(n1, n2)  # the same counts: the same run, bit for bit
+        a.epoch(0.02)
+        b.epoch(0.02)
+        np.testing.assert_array_equal(a.get_factors()[0], b.get_factors()[0])
+        b.set_counts(n1 * 2, n2 * 2)  # doubled counts halve the regularization weights
+        a.epoch(0.02)
+        b.epoch(0.02)
+        assert not np.array_equal(a.get_factors()[0], b.get_factors()[0])
+        m1, m2, _ = b.nnz12()
+        np.testing.assert_array_equal(m1, n1 * 2)
+        with pytest.raises(P.DsgdppError):
+            b.set_counts(np.full(p.m, 1 << 33, np.uint64), n2)
