@@ -1,6 +1,6 @@
 """GPU parity tests: the CUDA path (through the C ABI) against the CPU oracle.
 
-Tolerances (BASELINE north star):
+Tolerances:
 * FP64 replay factors: bit-identical to the oracle (the bar is 1e-10 relative
   per entry; the replay repeats every operation in the reference order);
 * FP64 losses: 1e-12 relative (the terms are identical, only the summation
