@@ -247,7 +247,8 @@ def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
-    torch.cuda.set_device(local)
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
     pg = None
     if world > 1:
         import datetime
