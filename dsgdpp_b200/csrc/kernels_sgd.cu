@@ -226,11 +226,13 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
 // right before it is used.  (Prefetching the next chunk's rows into registers
 // or into shared memory with cp.async measured slower on B200: the extra
 // registers or shared memory cost more resident warps than the prefetch gains.)
-// BF16 with one vector per lane is held to 64 registers (4 CTAs per SM): it
-// needs 70 unconstrained, where 3 CTAs per SM left it latency-bound; up to 16
-// lanes per entry (rank 128) the cap costs no spills.
+// One vector per lane: BF16 is held to 64 registers (4 CTAs per SM; 70
+// unconstrained, where 3 CTAs per SM left it latency-bound; up to 16 lanes
+// per entry the cap costs no spills), FP32 to 48 (5 CTAs per SM; a few bytes
+// of spill, and the rank-128 FP32 epoch 23.4 -> 21.6 ms).  Two vectors per
+// lane stay unconstrained (5 CTAs per SM measured slower at rank 32).
 template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM, bool RUNS>
-__global__ void __launch_bounds__(256, (sizeof(T) == 2 && VPL == 1) ? 4 : 1)
+__global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeof(T) == 4 ? 5 : 1)
     hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
