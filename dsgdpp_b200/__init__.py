@@ -204,6 +204,9 @@ SIGNATURES = {
     "dsgdpp_rm_generate_factors": (C.c_int, [_P, C.c_int, _f64p, _f64p]),
     "dsgdpp_set_matrix_rm": (C.c_int, [_P, C.c_int, _P]),
     "dsgdpp_set_blocks": (C.c_int, [_P, C.c_int, _u64p, _u32p, _u32p, _f64p]),
+    "dsgdpp_epoch_part": (C.c_int, [_P, C.c_double, _u32p, _u32p, C.c_uint32, C.c_uint32]),
+    "dsgdpp_h_block_bytes": (C.c_int, [_P, C.c_uint32, _u64p]),
+    "dsgdpp_h_block_copy": (C.c_int, [_P, C.c_uint32, _P, C.c_int]),
     "dsgdpp_set_counts": (C.c_int, [_P, _u64p, _u64p]),
     "dsgdpp_set_factors_rm": (C.c_int, [_P, _P]),
 }
@@ -401,6 +404,24 @@ class Context:
         s, t = _u32(schedule), _u32(task_seeds)
         self._check(lib.dsgdpp_epoch_explicit(self._h, eps, _ptr(s, C.c_uint32),
                                               _ptr(t, C.c_uint32)), "epoch_explicit")
+
+    def epoch_part(self, eps: float, schedule, task_seeds, s_begin: int, s_end: int):
+        """Sub-epochs [s_begin, s_end) of the epoch (eps, schedule, seeds)."""
+        s = _u32(schedule)
+        t = _u32(task_seeds)
+        self._check(lib.dsgdpp_epoch_part(self._h, eps, _ptr(s, C.c_uint32), _ptr(t, C.c_uint32),
+                                          s_begin, s_end), "epoch_part")
+
+    def h_block_bytes(self, b2: int) -> int:
+        out = C.c_uint64()
+        self._check(lib.dsgdpp_h_block_bytes(self._h, b2, C.byref(out)), "h_block_bytes")
+        return out.value
+
+    def h_block_copy(self, b2: int, device_ptr: int, to_context: bool):
+        """Copies H column block b2 to (to_context False) or from a device buffer
+        (an address, e.g. a torch CUDA tensor's data_ptr())."""
+        self._check(lib.dsgdpp_h_block_copy(self._h, b2, C.c_void_p(device_ptr), int(to_context)),
+                    "h_block_copy")
 
     def last_epoch_ms(self) -> float:
         v = C.c_double()

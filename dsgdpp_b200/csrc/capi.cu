@@ -531,10 +531,15 @@ bool lazy_l2(const dsgdpp_ctx* c) {
   return c->cfg.regularize == DSGDPP_REGULARIZE_L2 && c->cfg.regularize_lambda != 0;
 }
 
-void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
+// Sub-epochs [s0, s1) of the epoch; the epoch's inputs are uploaded and its
+// segment tables built with the part that starts at 0, the end-of-epoch
+// normalization runs with the part that ends at nb2.
+void enqueue_hogwild_epoch(dsgdpp_ctx* c, uint32_t s0, uint32_t s1) {
   cudaStream_t st = c->stream;
   const uint32_t d = c->d, d2 = c->nb2;
   const bool l2 = lazy_l2(c);
+  const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
+  if (s0 == 0) {
   check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
                              cudaMemcpyHostToDevice, st), "H2D schedule");
   check_cuda(cudaMemcpyAsync(c->d_params, c->h_params, sizeof(EpochParams),
@@ -548,12 +553,12 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   SegBuildArgs sb{c->d_params, c->d_schedule, c->mat[0].block_ptr, l2 ? c->d_sigma : nullptr,
                   c->d_segs, c->d_counters, d, d2};
   check_cuda(launch_build_segments(sb, st), "build_segments");
-  const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
   if (persistent) {
     check_cuda(cudaMemcpyAsync(c->d_dep_col, c->h_dep_col, (size_t)d2 * d * 4,
                                cudaMemcpyHostToDevice, st), "H2D dependencies");
     check_cuda(cudaMemsetAsync(c->d_done, 0, (size_t)d2 * d * 4, st), "segment counters");
     check_cuda(cudaMemsetAsync(c->d_ticket, 0, 8, st), "ticket");
+  }
   }
   HogwildArgs a{};
   const DevMatrix& M = c->mat[0];
@@ -573,7 +578,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
   a.update = c->cfg.update; a.truncate = c->cfg.truncate; a.sgd_order = c->cfg.sgd_order;
   a.atomic = c->atomic_writes;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
-  const bool prof = c->profiling && c->prof_ev.size() == d2 + 1;
+  const bool prof = c->profiling && c->prof_ev.size() == d2 + 1 && s0 == 0 && s1 == d2;
   if (persistent) {
     EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d, d2};
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[0], st), "event");
@@ -583,13 +588,13 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c) {
     check_cuda(cudaMemcpyAsync(c->h_error, c->d_ticket + 1, 4, cudaMemcpyDeviceToHost, st),
                "D2H error flag");
   }
-  for (uint32_t s = 0; s < d2 && !persistent; ++s) {
+  for (uint32_t s = s0; s < s1 && !persistent; ++s) {
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[s], st), "event");
     check_cuda(launch_hogwild(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
                "hogwild_subepoch");
   }
   if (prof && !persistent) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
-  if (l2)
+  if (l2 && s1 == d2)
     check_cuda(launch_normalize(c->cfg.precision, c->W, c->H, c->cfg.m, c->cfg.n, c->rp,
                                 c->d_scales, c->d_off2, d2, st), "normalize");
 }
@@ -614,11 +619,24 @@ void collect_profile(dsgdpp_ctx* c) {
   c->prof_launches += d2;
 }
 
-void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
-  if (lazy_l2(c)) fill_sigma(c, eps);
+void run_hogwild_epoch(dsgdpp_ctx* c, double eps, uint32_t s0, uint32_t s1) {
+  const bool whole = s0 == 0 && s1 == c->nb2;
   const bool persistent = c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT;
-  if (persistent) fill_deps(c);
+  if (!whole && persistent)
+    throw Error(DSGDPP_E_UNSUPPORTED, "the persistent launch runs whole epochs only");
+  if (s0 == 0 && lazy_l2(c)) fill_sigma(c, eps);
   cudaStream_t st = c->stream;
+  if (!whole) {  // a part: stream launches, timed from its first to its last part
+    if (s0 == 0) check_cuda(cudaEventRecord(c->ev_begin, st), "event");
+    enqueue_hogwild_epoch(c, s0, s1);
+    if (s1 == c->nb2) {
+      check_cuda(cudaEventRecord(c->ev_end, st), "event");
+      c->epoch_timed = true;
+    }
+    check_cuda(cudaEventRecord(c->ev_inputs, st), "event");
+    return;
+  }
+  if (persistent) fill_deps(c);
   collect_profile(c);
   check_cuda(cudaEventRecord(c->ev_begin, st), "event");
   if ((c->cfg.launch == DSGDPP_LAUNCH_GRAPH || persistent) && !c->profiling) {
@@ -626,7 +644,7 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
       cudaGraph_t g = nullptr;
       check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
       try {
-        enqueue_hogwild_epoch(c);
+        enqueue_hogwild_epoch(c, 0, c->nb2);
       } catch (...) {
         cudaStreamEndCapture(st, &g);
         if (g) cudaGraphDestroy(g);
@@ -639,7 +657,7 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
     }
     check_cuda(cudaGraphLaunch(c->graph_exec, st), "graph launch");
   } else {
-    enqueue_hogwild_epoch(c);
+    enqueue_hogwild_epoch(c, 0, c->nb2);
     c->prof_pending = c->profiling;
   }
   check_cuda(cudaEventRecord(c->ev_end, st), "event");
@@ -654,9 +672,12 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps) {
   }
 }
 
-void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
+void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds, uint32_t s0, uint32_t s1) {
   const uint32_t d = c->d, d2 = c->nb2;
   const DevMatrix& M = c->mat[0];
+  const bool l2 = c->cfg.regularize == DSGDPP_REGULARIZE_L2;
+  cudaStream_t st = c->stream;
+  if (s0 == 0) {  // the epoch's inputs, with its first part
   // point orders, one generator per task (mf/sgd/dsgdpp_impl.h:79,112)
   uint64_t total = 0;
   for (uint32_t s = 0; s < d2; ++s)
@@ -691,13 +712,11 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
   } else {
     for (unsigned t = 0; t < hw; ++t) work(t);
   }
-  const bool l2 = c->cfg.regularize == DSGDPP_REGULARIZE_L2;
   if (l2) {
     std::memset(c->h_mask, 0, (size_t)d2 * d2);
     for (uint32_t s = 0; s < d2; ++s)
       for (uint32_t id = 0; id < d; ++id) c->h_mask[(size_t)s * d2 + c->h_schedule[(size_t)s * d + id]] = 1;
   }
-  cudaStream_t st = c->stream;
   check_cuda(cudaEventRecord(c->ev_begin, st), "event");
   check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
                              cudaMemcpyHostToDevice, st), "H2D schedule");
@@ -711,6 +730,7 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
   if (l2)
     check_cuda(cudaMemcpyAsync(c->d_mask, c->h_mask, (size_t)d2 * d2, cudaMemcpyHostToDevice, st),
                "H2D mask");
+  }
   ReplayArgs a{};
   a.row = M.row; a.col = M.col; a.val = static_cast<const double*>(M.val);
   a.cnt1 = c->cnt1; a.cnt2 = c->cnt2;
@@ -720,7 +740,7 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
   a.d = d; a.r = c->r; a.rp = c->rp; a.nb2 = d2;
   a.update = c->cfg.update; a.truncate = c->cfg.truncate;
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
-  for (uint32_t s = 0; s < d2; ++s) {
+  for (uint32_t s = s0; s < s1; ++s) {
     check_cuda(launch_replay_subepoch(a, s, st), "replay_subepoch");
     if (l2 && c->cfg.regularize_lambda != 0)
       check_cuda(launch_regularize_exact(a.W, a.H, c->cfg.m, c->cfg.n, c->rp, c->r, c->d_off2,
@@ -729,26 +749,55 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds) {
                                          c->cfg.truncate_min, c->cfg.truncate_max, st),
                  "regularize");
   }
-  check_cuda(cudaEventRecord(c->ev_end, st), "event");
+  if (s1 == d2) {
+    check_cuda(cudaEventRecord(c->ev_end, st), "event");
+    c->epoch_timed = true;
+  }
   check_cuda(cudaEventRecord(c->ev_inputs, st), "event");
-  c->epoch_timed = true;
 }
 
-void epoch_explicit_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
-                         const uint32_t* seeds) {
+// Sub-epochs [s0, s1) of the epoch given by (eps, schedule, seeds); the
+// whole epoch is the range [0, nb2).  Parts run in order: a part starting at
+// 0 begins an epoch, later parts must continue it with the same arguments.
+void epoch_part_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule, const uint32_t* seeds,
+                     uint32_t s0, uint32_t s1) {
   if (!schedule || !seeds) throw Error(DSGDPP_E_INVALID, "schedule and task seeds are required");
   if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
   if (!c->factors_set) throw Error(DSGDPP_E_STATE, "factors not set");
   if (!std::isfinite(eps)) throw Error(DSGDPP_E_INVALID, "step size is not finite");
   const uint32_t d = c->d, d2 = c->nb2;
-  for (size_t k = 0; k < (size_t)d2 * d; ++k)
-    if (schedule[k] >= d2) throw Error(DSGDPP_E_INVALID, "schedule entry out of range");
+  if (s0 >= s1 || s1 > d2) throw Error(DSGDPP_E_INVALID, "sub-epoch range out of order or bounds");
+  if (s0 != c->part_next)
+    throw Error(DSGDPP_E_STATE, s0 == 0 ? "the epoch given in parts is unfinished"
+                                        : "parts of an epoch must follow one another");
+  if (s0 == 0) {
+    for (size_t k = 0; k < (size_t)d2 * d; ++k)
+      if (schedule[k] >= d2) throw Error(DSGDPP_E_INVALID, "schedule entry out of range");
+  } else if (eps != c->h_params->eps ||
+             std::memcmp(schedule, c->h_schedule, (size_t)d2 * d * 4) != 0 ||
+             std::memcmp(seeds, c->part_seeds.data(), (size_t)d * 4) != 0) {
+    throw Error(DSGDPP_E_INVALID, "a later part of an epoch must repeat its step size, schedule and seeds");
+  }
   check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
-  wait_inputs_free(c);
-  std::memcpy(c->h_schedule, schedule, (size_t)d2 * d * 4);
-  fill_epoch_params(c, eps, seeds);
-  if (c->cfg.exec == DSGDPP_EXEC_REPLAY) run_replay_epoch(c, eps, seeds);
-  else run_hogwild_epoch(c, eps);
+  if (s0 == 0) {
+    wait_inputs_free(c);
+    std::memcpy(c->h_schedule, schedule, (size_t)d2 * d * 4);
+    fill_epoch_params(c, eps, seeds);
+    c->part_seeds.assign(seeds, seeds + d);
+  }
+  c->part_next = s1 == d2 ? 0 : s1;
+  try {
+    if (c->cfg.exec == DSGDPP_EXEC_REPLAY) run_replay_epoch(c, eps, seeds, s0, s1);
+    else run_hogwild_epoch(c, eps, s0, s1);
+  } catch (...) {
+    c->part_next = 0;  // a failed part abandons its epoch
+    throw;
+  }
+}
+
+void epoch_explicit_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
+                         const uint32_t* seeds) {
+  epoch_part_impl(c, eps, schedule, seeds, 0, c->nb2);
 }
 
 // ---- losses --------------------------------------------------------------------------
@@ -1092,6 +1141,39 @@ int dsgdpp_epoch_explicit(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
                           const uint32_t* task_seeds) {
   return guarded(c, [&]() {
     epoch_explicit_impl(c, eps, schedule, task_seeds);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_epoch_part(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
+                      const uint32_t* task_seeds, uint32_t s_begin, uint32_t s_end) {
+  return guarded(c, [&]() {
+    epoch_part_impl(c, eps, schedule, task_seeds, s_begin, s_end);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_h_block_bytes(dsgdpp_ctx* c, uint32_t b2, uint64_t* bytes) {
+  return guarded(c, [&]() {
+    if (!bytes || b2 >= c->nb2) throw Error(DSGDPP_E_INVALID, "column block out of range");
+    *bytes = (c->off2[b2 + 1] - c->off2[b2]) * c->rp * elem_size(c->cfg.precision);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_h_block_copy(dsgdpp_ctx* c, uint32_t b2, void* device_buf, int to_context) {
+  return guarded(c, [&]() {
+    if (!device_buf || b2 >= c->nb2) throw Error(DSGDPP_E_INVALID, "column block out of range");
+    check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
+    const size_t es = elem_size(c->cfg.precision);
+    const size_t bytes = (c->off2[b2 + 1] - c->off2[b2]) * c->rp * es;
+    char* blk = static_cast<char*>(c->H) + c->off2[b2] * c->rp * es;
+    cudaStream_t st = c->stream;
+    if (to_context)
+      check_cuda(cudaMemcpyAsync(blk, device_buf, bytes, cudaMemcpyDefault, st), "copy into H");
+    else
+      check_cuda(cudaMemcpyAsync(device_buf, blk, bytes, cudaMemcpyDefault, st), "copy from H");
+    check_cuda(cudaStreamSynchronize(st), "sync");
     return DSGDPP_OK;
   });
 }

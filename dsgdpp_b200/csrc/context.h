@@ -137,6 +137,10 @@ struct dsgdpp_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_coords = nullptr, ev_vals = nullptr;
   bool epoch_timed = false;
+  // an epoch given in parts: the next sub-epoch to run (0 = none pending) and
+  // the task seeds of its first part
+  uint32_t part_next = 0;
+  std::vector<uint32_t> part_seeds;
   // per-kernel timing of the Hogwild sub-epoch kernels (stream launch only)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 2d + 1 events around the sub-epoch kernels

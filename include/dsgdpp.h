@@ -185,6 +185,23 @@ int dsgdpp_epoch(dsgdpp_ctx* ctx, double eps);
  * task id, entry = column block) and task seeds (d). */
 int dsgdpp_epoch_explicit(dsgdpp_ctx* ctx, double eps, const uint32_t* schedule,
                           const uint32_t* task_seeds);
+/* Sub-epochs [s_begin, s_end) of the epoch given by eps, schedule and
+ * task_seeds, as dsgdpp_epoch_explicit runs all of them: the parts of one
+ * epoch follow one another from 0 to 2d (d for DSGD) with the same arguments,
+ * and an epoch is finished (end-of-epoch work done) by the part that reaches
+ * the end.  Between parts the caller may exchange H column blocks
+ * (dsgdpp_h_block_copy) -- the hand-off of DsgdPpTask::run between
+ * sub-epochs when the tasks live on several ranks (mf/sgd/dsgdpp_impl.h:
+ * 153-263).  Stream launches; not for the persistent launch form. */
+int dsgdpp_epoch_part(dsgdpp_ctx* ctx, double eps, const uint32_t* schedule,
+                      const uint32_t* task_seeds, uint32_t s_begin, uint32_t s_end);
+/* H column block b2 (columns off2[b2] .. off2[b2+1] of H, each rank-padded,
+ * in the factor precision) copied from the context into device_buf
+ * (to_context = 0) or from device_buf into the context (1); the caller's
+ * buffer holds dsgdpp_h_block_bytes bytes and may live on any device the
+ * context's device can reach.  Synchronous. */
+int dsgdpp_h_block_bytes(dsgdpp_ctx* ctx, uint32_t b2, uint64_t* bytes);
+int dsgdpp_h_block_copy(dsgdpp_ctx* ctx, uint32_t b2, void* device_buf, int to_context);
 /* Device time of the last epoch's kernels in milliseconds. */
 int dsgdpp_last_epoch_ms(dsgdpp_ctx* ctx, double* ms);
 /* Per-kernel timing of the Hogwild sub-epoch kernels: when on, epochs launch

@@ -1,0 +1,95 @@
+"""DSGD++ with its tasks spread over ranks (dsgdpp_b200/shard.py), emulated as
+several contexts on one GPU that run one after another and hand H blocks to
+each other between sub-epochs: the result must be the single-context epoch's
+(bit for bit in the FP64 replay)."""
+import numpy as np
+import pytest
+
+import dsgdpp_b200 as P
+from dsgdpp_b200 import shard, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _ranks_run(p, d, world, epochs, precision, exec_, regularize, seed=3, eps=0.02):
+    kw = dict(m=p.m, n=p.n, rank=8, d=d, precision=precision, exec=exec_, launch="stream",
+              regularize=regularize, regularize_lambda=0.05 if regularize == "L2" else 0.0)
+    off1 = list(P.block_offsets(p.m, d)) + [p.m]
+    ctxs = {}
+    ref = P.Context(P.Config(**kw))
+    try:
+        ref.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ref.set_factors(p.W0, p.H0)
+        for r in range(world):
+            lo, hi = shard.rank_rows(off1, d, world, r)
+            keep = (p.rows >= lo) & (p.rows < hi)
+            c = P.Context(P.Config(**kw))
+            c.set_matrix(P.TRAIN, p.rows[keep], p.cols[keep], p.vals[keep])
+            ctxs[r] = c
+        # the update weights are counts over the whole matrix, as the reference's
+        n1, n2, _ = ref.nnz12()
+        for c in ctxs.values():
+            c.set_counts(n1, n2)
+            c.set_factors(p.W0, p.H0)
+        holder = shard.new_holders(2 * d)
+        rng = P.Random32(seed)
+        for _ in range(epochs):
+            sched, seeds = P.draw_schedule(rng, d, "COWOR")
+            ref.epoch_explicit(eps, sched, seeds)
+            shard.run_epoch(eps, sched, seeds, d, world, holder, list(range(world)),
+                            lambda r, s: ctxs[r].epoch_part(eps, sched, seeds, s, s + 1),
+                            lambda moves: shard.local_exchange(ctxs, moves))
+        W = np.empty_like(p.W0[:, :8])
+        H = np.empty_like(p.H0[:, :8])
+        off2 = list(P.block_offsets(p.n, 2 * d)) + [p.n]
+        parts = {r: ctxs[r].get_factors() for r in range(world)}
+        for r in range(world):
+            lo, hi = shard.rank_rows(off1, d, world, r)
+            W[lo:hi] = parts[r][0][lo:hi]
+        for b in range(2 * d):
+            src = holder[b] if holder[b] != shard.EVERYONE else 0
+            H[off2[b]:off2[b + 1]] = parts[src][1][off2[b]:off2[b + 1]]
+        Wr, Hr = ref.get_factors()
+        return W, H, Wr, Hr
+    finally:
+        ref.close()
+        for c in ctxs.values():
+            c.close()
+
+
+@pytest.mark.parametrize("regularize", ["None", "L2"])
+@pytest.mark.parametrize("world", [2, 4])
+def test_replay_over_ranks_equals_one_context(world, regularize):
+    p = synth.make(900, 700, 20000, 100, rank_true=6, r=8, noise=0.1, seed=8)
+    W, H, Wr, Hr = _ranks_run(p, 4, world, 3, "fp64", "replay", regularize)
+    np.testing.assert_array_equal(W, Wr)
+    np.testing.assert_array_equal(H, Hr)
+
+
+@pytest.mark.parametrize("regularize", ["None", "L2"])
+def test_hogwild_over_ranks_tracks_one_context(regularize):
+    p = synth.make(4000, 3000, 200000, 100, rank_true=6, r=8, noise=0.1, seed=9)
+    W, H, Wr, Hr = _ranks_run(p, 4, 2, 3, "fp32", "hogwild", regularize)
+    # Hogwild runs differ run to run; the products on the training entries agree closely
+    got = np.einsum("kz,kz->k", W[p.rows], H[p.cols])
+    want = np.einsum("kz,kz->k", Wr[p.rows], Hr[p.cols])
+    rmse_got = np.sqrt(np.mean((p.vals - got) ** 2))
+    rmse_want = np.sqrt(np.mean((p.vals - want) ** 2))
+    assert abs(rmse_got - rmse_want) <= 0.005 * rmse_want, (rmse_got, rmse_want)
+
+
+def test_parts_must_follow_one_another():
+    p = synth.make(300, 200, 3000, 100, rank_true=4, r=8, noise=0.1, seed=1)
+    with P.Context(P.Config(m=p.m, n=p.n, rank=8, d=2, launch="stream")) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_factors(p.W0, p.H0)
+        sched, seeds = P.draw_schedule(P.Random32(1), 2, "COWOR")
+        with pytest.raises(P.DsgdppError):
+            ctx.epoch_part(0.01, sched, seeds, 1, 2)      # must start at 0
+        ctx.epoch_part(0.01, sched, seeds, 0, 1)
+        with pytest.raises(P.DsgdppError):
+            ctx.epoch(0.01)                              # the epoch in parts is unfinished
+        with pytest.raises(P.DsgdppError):
+            ctx.epoch_part(0.02, sched, seeds, 1, 4)      # another step size
+        ctx.epoch_part(0.01, sched, seeds, 1, 4)
+        ctx.epoch(0.01)                                   # whole epochs again

@@ -1,0 +1,114 @@
+"""CPU tests of the multi-rank DSGD++ hand-off (dsgdpp_b200/shard.py): the
+plan of H-block moves, and two gloo ranks moving blocks whose contents record
+every task that updated them, against one process running all tasks."""
+import ctypes
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from dsgdpp_b200 import shard
+
+
+def _schedules(d, epochs, seed):
+    import dsgdpp_b200 as P
+    rng = P.Random32(seed)
+    return [P.draw_schedule(rng, d, "COWOR") for _ in range(epochs)]
+
+
+def test_plan_puts_every_block_on_its_task_rank():
+    d, world = 6, 3
+    owner = shard.task_owner(d, world)
+    holder = shard.new_holders(2 * d)
+    for sched, _ in _schedules(d, 3, 5):
+        plan = shard.handoff_plan(sched, d, world, holder)
+        assert len(plan) == 2 * d
+        for s, moves in enumerate(plan):
+            dsts = [m[2] for m in moves]
+            assert len({m[0] for m in moves}) == len(moves)  # a block moves at most once
+            for b2, src, dst in moves:
+                assert src != dst and src != shard.EVERYONE
+            for task in range(d):
+                b2 = int(sched[s, task])
+                # after the moves before s the block sits with its task's rank
+                assert owner[task] == next((m[2] for m in moves if m[0] == b2),
+                                           owner[task])
+        for task in range(d):
+            assert holder[int(sched[-1, task])] == owner[task]
+
+
+def test_task_ranges_need_a_multiple():
+    with pytest.raises(ValueError):
+        shard.task_owner(5, 2)
+    assert list(shard.task_owner(4, 2)) == [0, 0, 1, 1]
+
+
+class _FakeCtx:
+    """Blocks of int64 whose contents fold in every (sub-epoch, task) visit."""
+
+    def __init__(self, nb2, tasks, d, width=4):
+        self.blocks = {b: np.zeros(width, np.int64) for b in range(nb2)}
+        self.tasks, self.d = tasks, d
+
+    def visit(self, sched, s, epoch):
+        for task in self.tasks:
+            b = int(sched[s, task])
+            self.blocks[b] = (self.blocks[b] * 31 + (epoch * 1000 + s * self.d + task + 1)) % (1 << 40)
+
+    def h_block_bytes(self, b2):
+        return self.blocks[b2].nbytes
+
+    def h_block_copy(self, b2, ptr, to_context):
+        a = self.blocks[b2]
+        if to_context:
+            ctypes.memmove(a.ctypes.data, ptr, a.nbytes)
+        else:
+            ctypes.memmove(ptr, a.ctypes.data, a.nbytes)
+
+
+def _rank(rank, world, port, d, epochs, out):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        owner = shard.task_owner(d, world)
+        ctx = _FakeCtx(2 * d, [t for t in range(d) if owner[t] == rank], d)
+        holder = shard.new_holders(2 * d)
+        for e, (sched, _) in enumerate(_schedules(d, epochs, 9)):
+            shard.run_epoch(0.0, sched, None, d, world, holder, [rank],
+                            lambda r, s: ctx.visit(sched, s, e),
+                            lambda moves: shard.torch_exchange(dist, rank, ctx, moves, "cpu"))
+        final = {}
+        for b in range(2 * d):
+            t = torch.from_numpy(ctx.blocks[b].copy())
+            dist.broadcast(t, src=holder[b] if holder[b] != shard.EVERYONE else 0)
+            final[b] = t.numpy().tolist()
+        out[rank] = final
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_hand_blocks_over_as_one_process_would():
+    d, world, epochs = 4, 2, 3
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctxm = mp.get_context("spawn")
+    out = ctxm.Manager().dict()
+    procs = [ctxm.Process(target=_rank, args=(r, world, port, d, epochs, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    ref = _FakeCtx(2 * d, list(range(d)), d)
+    for e, (sched, _) in enumerate(_schedules(d, epochs, 9)):
+        for s in range(2 * d):
+            ref.visit(sched, s, e)
+    want = {b: ref.blocks[b].tolist() for b in range(2 * d)}
+    assert out[0] == want and out[1] == want
