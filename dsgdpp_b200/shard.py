@@ -87,7 +87,8 @@ def torch_exchange(pg, rank: int, ctx, moves: List[Move], device: str = "cuda"):
         if rank not in (src, dst):
             continue
         nbytes = ctx.h_block_bytes(b2)
-        buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device)
+        pin = device == "cpu" and torch.cuda.is_available()  # host buffers the GPU copies into
+        buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device, pin_memory=pin)
         if rank == src:
             ctx.h_block_copy(b2, buf.data_ptr(), False)
             ops.append(pg.P2POp(pg.isend, buf, dst))

@@ -93,3 +93,72 @@ def test_parts_must_follow_one_another():
             ctx.epoch_part(0.02, sched, seeds, 1, 4)      # another step size
         ctx.epoch_part(0.01, sched, seeds, 1, 4)
         ctx.epoch(0.01)                                   # whole epochs again
+
+
+def _gloo_rank(rank, world, port, out):
+    import datetime
+    import os
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        d, eps = 4, 0.02
+        p = synth.make(900, 700, 20000, 100, rank_true=6, r=8, noise=0.1, seed=8)
+        kw = dict(m=p.m, n=p.n, rank=8, d=d, precision="fp64", exec="replay", launch="stream")
+        off1 = list(P.block_offsets(p.m, d)) + [p.m]
+        lo, hi = shard.rank_rows(off1, d, world, rank)
+        keep = (p.rows >= lo) & (p.rows < hi)
+        with P.Context(P.Config(**kw)) as full, P.Context(P.Config(**kw)) as ctx:
+            full.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+            n1, n2, _ = full.nnz12()
+            ctx.set_matrix(P.TRAIN, p.rows[keep], p.cols[keep], p.vals[keep])
+            ctx.set_counts(n1, n2)
+            ctx.set_factors(p.W0, p.H0)
+            holder = shard.new_holders(2 * d)
+            rng = P.Random32(5)  # every rank draws the same epochs here; a job would
+            for _ in range(2):   # draw them on rank 0 and broadcast them
+                sched, seeds = P.draw_schedule(rng, d, "COWOR")
+                shard.run_epoch(eps, sched, seeds, d, world, holder, [rank],
+                                lambda r, s: ctx.epoch_part(eps, sched, seeds, s, s + 1),
+                                lambda moves: shard.torch_exchange(dist, rank, ctx, moves, "cpu"))
+            W, H = ctx.get_factors()
+            out[rank] = (W[lo:hi].copy(), H.copy(), list(holder))
+            if rank == 0:
+                full.set_factors(p.W0, p.H0)
+                rng = P.Random32(5)
+                for _ in range(2):
+                    sched, seeds = P.draw_schedule(rng, d, "COWOR")
+                    full.epoch_explicit(eps, sched, seeds)
+                out["ref"] = full.get_factors()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_processes_hand_blocks_over_with_torch_distributed():
+    # two ranks as two processes sharing this GPU; they meet only on the host
+    # (gloo), never inside a kernel
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_gloo_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    Wr, Hr = out["ref"]
+    d = 4
+    off1 = list(P.block_offsets(900, d)) + [900]
+    off2 = list(P.block_offsets(700, 2 * d)) + [700]
+    holder = out[0][2]
+    for r in range(2):
+        lo, hi = shard.rank_rows(off1, d, 2, r)
+        np.testing.assert_array_equal(out[r][0], Wr[lo:hi])
+    for b in range(2 * d):
+        H = out[holder[b]][1]
+        np.testing.assert_array_equal(H[off2[b]:off2[b + 1]], Hr[off2[b]:off2[b + 1]])
