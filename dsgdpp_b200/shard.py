@@ -16,6 +16,10 @@ sub-epoch s every block that a task uses at s is moved to that task's rank
 from the rank that holds its latest version; ``handoff_plan`` lists these
 moves for a whole epoch, identically on every rank.
 
+After an epoch, ``share_local`` / ``share_torch`` give every rank every
+block's latest version; the training loss is then the sum of the ranks'
+losses over their own entries.
+
 Transports: ``torch_exchange`` moves blocks with torch.distributed
 point-to-point operations (NCCL between GPUs; gloo works for host buffers),
 ``local_exchange`` moves them between contexts of one process (several
@@ -102,6 +106,43 @@ def torch_exchange(pg, rank: int, ctx, moves: List[Move], device: str = "cuda"):
         torch.cuda.synchronize()
     for b2, buf in recvs:
         ctx.h_block_copy(b2, buf.data_ptr(), True)
+
+
+def share_local(ctxs: Dict[int, object], holder: List[int], device: int = 0):
+    """Every context gets every block's latest version (emulated ranks)."""
+    import torch
+    for b2, src in enumerate(holder):
+        if src == EVERYONE:
+            continue
+        nbytes = ctxs[src].h_block_bytes(b2)
+        buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=f"cuda:{device}")
+        ctxs[src].h_block_copy(b2, buf.data_ptr(), False)
+        for r, c in ctxs.items():
+            if r != src:
+                c.h_block_copy(b2, buf.data_ptr(), True)
+        holder[b2] = EVERYONE
+
+
+def share_torch(pg, rank: int, ctx, holder: List[int], device: str = "cuda"):
+    """Every rank gets every block's latest version: one broadcast per block
+    from its holder, in block order on every rank.  Needed before the training
+    loss (a rank's entries touch every column block) and makes the next
+    epoch's hand-off start from blocks that every rank holds."""
+    import torch
+    for b2, src in enumerate(holder):
+        if src == EVERYONE:
+            continue
+        nbytes = ctx.h_block_bytes(b2)
+        pin = device == "cpu" and torch.cuda.is_available()
+        buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=device, pin_memory=pin)
+        if rank == src:
+            ctx.h_block_copy(b2, buf.data_ptr(), False)
+        pg.broadcast(buf, src=src)
+        if device != "cpu":
+            torch.cuda.synchronize()
+        if rank != src:
+            ctx.h_block_copy(b2, buf.data_ptr(), True)
+        holder[b2] = EVERYONE
 
 
 def run_epoch(eps: float, schedule: np.ndarray, seeds: np.ndarray, d: int, world: int,

@@ -50,6 +50,14 @@ def _ranks_run(p, d, world, epochs, precision, exec_, regularize, seed=3, eps=0.
             src = holder[b] if holder[b] != shard.EVERYONE else 0
             H[off2[b]:off2[b + 1]] = parts[src][1][off2[b]:off2[b + 1]]
         Wr, Hr = ref.get_factors()
+        # with every block shared, the ranks' losses over their entries add up
+        # to the single context's
+        shard.share_local(ctxs, holder)
+        total = sum(ctxs[r].nzsl(P.TRAIN) for r in range(world))
+        pred = np.einsum("kz,kz->k", W[p.rows], H[p.cols])
+        assert total == pytest.approx(float(np.sum((p.vals - pred) ** 2)), rel=1e-9)
+        if precision == "fp64":
+            assert total == pytest.approx(ref.nzsl(P.TRAIN), rel=1e-12)
         return W, H, Wr, Hr
     finally:
         ref.close()
@@ -98,6 +106,7 @@ def test_parts_must_follow_one_another():
 def _gloo_rank(rank, world, port, out):
     import datetime
     import os
+    import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
@@ -124,6 +133,10 @@ def _gloo_rank(rank, world, port, out):
                                 lambda moves: shard.torch_exchange(dist, rank, ctx, moves, "cpu"))
             W, H = ctx.get_factors()
             out[rank] = (W[lo:hi].copy(), H.copy(), list(holder))
+            shard.share_torch(dist, rank, ctx, holder, "cpu")
+            loss = torch.tensor([ctx.nzsl(P.TRAIN)], dtype=torch.float64)
+            dist.all_reduce(loss)
+            out[f"loss{rank}"] = float(loss.item())
             if rank == 0:
                 full.set_factors(p.W0, p.H0)
                 rng = P.Random32(5)
@@ -131,6 +144,7 @@ def _gloo_rank(rank, world, port, out):
                     sched, seeds = P.draw_schedule(rng, d, "COWOR")
                     full.epoch_explicit(eps, sched, seeds)
                 out["ref"] = full.get_factors()
+                out["ref_loss"] = full.nzsl(P.TRAIN)
     finally:
         dist.destroy_process_group()
 
@@ -162,3 +176,5 @@ def test_two_processes_hand_blocks_over_with_torch_distributed():
     for b in range(2 * d):
         H = out[holder[b]][1]
         np.testing.assert_array_equal(H[off2[b]:off2[b + 1]], Hr[off2[b]:off2[b + 1]])
+    for r in range(2):
+        assert out[f"loss{r}"] == pytest.approx(out["ref_loss"], rel=1e-12)
