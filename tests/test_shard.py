@@ -22,21 +22,21 @@ def test_plan_puts_every_block_on_its_task_rank():
     d, world = 6, 3
     owner = shard.task_owner(d, world)
     holder = shard.new_holders(2 * d)
+    where = [shard.EVERYONE] * (2 * d)  # replayed independently of the plan's own bookkeeping
     for sched, _ in _schedules(d, 3, 5):
         plan = shard.handoff_plan(sched, d, world, holder)
         assert len(plan) == 2 * d
         for s, moves in enumerate(plan):
-            dsts = [m[2] for m in moves]
             assert len({m[0] for m in moves}) == len(moves)  # a block moves at most once
             for b2, src, dst in moves:
-                assert src != dst and src != shard.EVERYONE
+                assert src == where[b2] and src != dst
+                where[b2] = dst
             for task in range(d):
                 b2 = int(sched[s, task])
-                # after the moves before s the block sits with its task's rank
-                assert owner[task] == next((m[2] for m in moves if m[0] == b2),
-                                           owner[task])
-        for task in range(d):
-            assert holder[int(sched[-1, task])] == owner[task]
+                # the block is with its task's rank (or still with every rank)
+                assert where[b2] in (owner[task], shard.EVERYONE)
+                where[b2] = owner[task]
+        assert where == holder
 
 
 def test_task_ranges_need_a_multiple():
