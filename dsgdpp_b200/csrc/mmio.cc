@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cerrno>
+#include <charconv>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -189,50 +190,76 @@ Dense read_mm_array(const std::string& path) {
 
 namespace {
 // %.16g: std::numeric_limits<double>::digits10 + 1 significant digits, as the
-// reference's ostream precision (write_impl.h:51,98)
+// reference's ostream precision (write_impl.h:51,98); std::to_chars with a
+// precision formats exactly as printf's %.16g does
 void put_double(std::string& out, double x) {
   char buf[40];
-  int k = std::snprintf(buf, sizeof(buf), "%.16g", x);
-  out.append(buf, (size_t)k);
+  const auto r = std::to_chars(buf, buf + sizeof(buf), x, std::chars_format::general, 16);
+  out.append(buf, (size_t)(r.ptr - buf));
+}
+void put_u64(std::string& out, uint64_t v) {
+  char buf[24];
+  const auto r = std::to_chars(buf, buf + sizeof(buf), v);
+  out.append(buf, (size_t)(r.ptr - buf));
+}
+
+// Writes `header` and then lines 0..n-1, each made by line(out, k); the lines
+// are formatted by several threads, one contiguous range each, and written in
+// order.
+template <typename F>
+void write_lines(const std::string& path, const std::string& header, size_t n, size_t bytes_per,
+                 F line) {
+  unsigned T = std::max(1u, std::thread::hardware_concurrency());
+  if (n < (1u << 16)) T = 1;
+  std::vector<std::string> parts(T);
+  auto work = [&](unsigned t) {
+    const size_t a = n * t / T, b = n * (t + 1) / T;
+    parts[t].reserve((b - a) * bytes_per);
+    for (size_t k = a; k < b; ++k) line(parts[t], k);
+  };
+  if (T == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < T; ++t) pool.emplace_back(work, t);
+    for (auto& th : pool) th.join();
+  }
+  std::ofstream f(path, std::ios::binary);
+  if (!f.is_open()) throw MmError("Cannot open file " + path);
+  f.write(header.data(), (std::streamsize)header.size());
+  for (const auto& part : parts) f.write(part.data(), (std::streamsize)part.size());
+  if (!f) throw MmError("Cannot write file " + path);
 }
 }  // namespace
 
 void write_mm_coord(const std::string& path, const Coo& m) {
-  std::string out;
-  out.reserve(64 + m.vals.size() * 32);
-  out += "%%MatrixMarket matrix coordinate real general\n";
-  out += "%=================================================================================\n";
-  out += "%\n% Indices are 1-based, i.e. A(1,1) is the first element.\n%\n";
-  out += "%=================================================================================\n";
-  out += std::to_string(m.size1) + " " + std::to_string(m.size2) + " " +
-         std::to_string(m.vals.size()) + "\n";
-  for (size_t k = 0; k < m.vals.size(); ++k) {
-    out += std::to_string((uint64_t)m.rows[k] + 1);
+  std::string head;
+  head += "%%MatrixMarket matrix coordinate real general\n";
+  head += "%=================================================================================\n";
+  head += "%\n% Indices are 1-based, i.e. A(1,1) is the first element.\n%\n";
+  head += "%=================================================================================\n";
+  head += std::to_string(m.size1) + " " + std::to_string(m.size2) + " " +
+          std::to_string(m.vals.size()) + "\n";
+  write_lines(path, head, m.vals.size(), 40, [&](std::string& out, size_t k) {
+    put_u64(out, (uint64_t)m.rows[k] + 1);
     out += ' ';
-    out += std::to_string((uint64_t)m.cols[k] + 1);
+    put_u64(out, (uint64_t)m.cols[k] + 1);
     out += ' ';
     put_double(out, m.vals[k]);
     out += '\n';
-  }
-  std::ofstream f(path, std::ios::binary);
-  if (!f.is_open()) throw MmError("Cannot open file " + path);
-  f.write(out.data(), (std::streamsize)out.size());
+  });
 }
 
 void write_mm_array(const std::string& path, const Dense& m) {
-  std::string out;
-  out.reserve(64 + m.colmajor.size() * 24);
-  out += "%%MatrixMarket matrix array real general\n";
-  out += "% First line: ROWS COLUMNS\n";
-  out += "% Subsequent lines: entries in column-major order\n";
-  out += std::to_string(m.size1) + " " + std::to_string(m.size2) + "\n";
-  for (double x : m.colmajor) {
-    put_double(out, x);
+  std::string head;
+  head += "%%MatrixMarket matrix array real general\n";
+  head += "% First line: ROWS COLUMNS\n";
+  head += "% Subsequent lines: entries in column-major order\n";
+  head += std::to_string(m.size1) + " " + std::to_string(m.size2) + "\n";
+  write_lines(path, head, m.colmajor.size(), 24, [&](std::string& out, size_t k) {
+    put_double(out, m.colmajor[k]);
     out += '\n';
-  }
-  std::ofstream f(path, std::ios::binary);
-  if (!f.is_open()) throw MmError("Cannot open file " + path);
-  f.write(out.data(), (std::streamsize)out.size());
+  });
 }
 
 // ---- minimal XML for the descriptor -------------------------------------------------

@@ -166,3 +166,21 @@ def test_dsgd_tool_name_and_map_reduce_option(tmp_path):
     r = subprocess.run([dsgd, *common, "--map-reduce=maybe"], capture_output=True, text=True,
                        timeout=120)
     assert r.returncode == 1 and "'--map-reduce' is invalid" in r.stderr
+
+
+def test_writers_format_like_printf_16g(tmp_path):
+    # the reference writes with 16 significant digits (write_impl.h:51,98); the
+    # multi-threaded writers must give printf's %.16g text for every value
+    rng = np.random.default_rng(3)
+    vals = np.concatenate([rng.standard_normal(200_000) * 10.0 ** rng.integers(-300, 300, 200_000),
+                           [0.0, -0.0, 1e-310, 5e-324, 1.7976931348623157e308, np.inf, -np.inf,
+                            np.nan, 1.0, 0.1, 1e16, 1e15, 9.999999999999999e15]])
+    P.write_mm_array(str(tmp_path / "v.mma"), vals.reshape(-1, 1))
+    lines = open(tmp_path / "v.mma").read().splitlines()
+    assert lines[3] == f"{len(vals)} 1"
+    assert lines[4:] == ["%.16g" % x for x in vals]
+    rows = rng.integers(0, 1000, len(vals)).astype(np.uint32)
+    cols = rng.integers(0, 50, len(vals)).astype(np.uint32)
+    P.write_mm_coord(str(tmp_path / "v.mmc"), 1000, 50, rows, cols, vals)
+    body = open(tmp_path / "v.mmc").read().splitlines()[7:]
+    assert body == ["%d %d %s" % (i + 1, j + 1, "%.16g" % x) for i, j, x in zip(rows, cols, vals)]
