@@ -43,6 +43,51 @@ bool blank(const char* a, const char* b) {
   return true;
 }
 
+// Number fields of one line, parsed in place: std::from_chars for the usual
+// forms, and strtoul / strtod on a copy of the token for anything it does not
+// take (a leading '+', hexadecimal, out-of-range values), so every line reads
+// exactly as with strtoul / strtod.
+inline const char* skip_blanks(const char* p, const char* e) {
+  while (p < e && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
+  return p;
+}
+inline const char* token_end(const char* p, const char* e) {
+  while (p < e && !std::isspace((unsigned char)*p)) ++p;
+  return p;
+}
+bool field_u64(const char*& p, const char* e, unsigned long& v) {
+  p = skip_blanks(p, e);
+  const auto r = std::from_chars(p, e, v);
+  if (r.ec == std::errc() && r.ptr != p && (r.ptr == e || std::isspace((unsigned char)*r.ptr))) {
+    p = r.ptr;
+    return true;
+  }
+  const char* te = token_end(p, e);
+  if (te == p) return false;
+  const std::string tok(p, te);
+  char* q = nullptr;
+  v = std::strtoul(tok.c_str(), &q, 10);
+  if (q == tok.c_str()) return false;
+  p += q - tok.c_str();
+  return true;
+}
+bool field_f64(const char*& p, const char* e, double& x) {
+  p = skip_blanks(p, e);
+  const auto r = std::from_chars(p, e, x, std::chars_format::general);
+  if (r.ec == std::errc() && r.ptr != p && (r.ptr == e || std::isspace((unsigned char)*r.ptr))) {
+    p = r.ptr;
+    return true;
+  }
+  const char* te = token_end(p, e);
+  if (te == p) return false;
+  const std::string tok(p, te);
+  char* q = nullptr;
+  x = std::strtod(tok.c_str(), &q);
+  if (q == tok.c_str()) return false;
+  p += q - tok.c_str();
+  return true;
+}
+
 // Cursor over the lines of a text buffer.
 struct Lines {
   const std::string& s;
@@ -122,23 +167,17 @@ Coo read_mm_coord(const std::string& path, unsigned threads) {
     for (size_t k = lo; k < hi; ++k) {
       const char* p = s.data() + starts[k];
       const char* end = s.data() + (k + 1 < starts.size() ? starts[k + 1] : pos);
-      std::string line(p, end);
-      if (!line.empty() && line.back() == '\n') line.pop_back();
-      if (!line.empty() && line.back() == '\r') line.pop_back();
-      const char* c = line.c_str();
-      char* q = nullptr;
-      unsigned long i = std::strtoul(c, &q, 10);
-      bool bad = (q == c);
-      const char* c2 = q;
-      unsigned long j = bad ? 0 : std::strtoul(c2, &q, 10);
-      bad = bad || (q == c2);
-      const char* c3 = q;
-      double x = bad ? 0 : std::strtod(c3, &q);
-      bad = bad || (q == c3) || !blank(q, line.c_str() + line.size());
+      if (end > p && end[-1] == '\n') --end;
+      if (end > p && end[-1] == '\r') --end;
+      const char* q = p;
+      unsigned long i = 0, j = 0;
+      double x = 0;
+      const bool bad = !field_u64(q, end, i) || !field_u64(q, end, j) || !field_f64(q, end, x) ||
+                       !blank(q, end);
       if (bad || i == 0 || j == 0 || i > m.size1 || j > m.size2) {
         if (errors[t].empty())
           errors[t] = "Parse error at line " + std::to_string(first_line + k) + " of " + path +
-                      ": " + line;
+                      ": " + std::string(p, end);
         continue;
       }
       m.rows[k] = (uint32_t)(i - 1);
@@ -171,16 +210,48 @@ Dense read_mm_array(const std::string& path) {
   Dense m;
   m.size1 = (uint64_t)s1;
   m.size2 = (uint64_t)s2;
-  m.colmajor.resize(m.size1 * m.size2);
-  for (uint64_t k = 0; k < m.size1 * m.size2; ++k) {
-    if (!L.next(a, b)) throw MmError("Unexpected EOF in file " + path);
-    std::string line(a, b);
-    char* q = nullptr;
-    double x = std::strtod(line.c_str(), &q);
-    if (q == line.c_str() || !blank(q, line.c_str() + line.size()))
-      throw MmError("Parse error at line " + std::to_string(L.number) + " of " + path + ": " + line);
-    m.colmajor[k] = x;
+  const uint64_t count = m.size1 * m.size2;
+  m.colmajor.resize(count);
+  // line starts first, then the values in parallel (as read_mm_coord)
+  std::vector<size_t> starts;
+  starts.reserve(count + 1);
+  const uint64_t first_line = L.number + 1;
+  for (uint64_t k = 0; k < count; ++k) {
+    if (L.pos >= s.size()) throw MmError("Unexpected EOF in file " + path);
+    starts.push_back(L.pos);
+    L.next(a, b);
   }
+  starts.push_back(L.pos);
+  unsigned T = std::max(1u, std::thread::hardware_concurrency());
+  T = (unsigned)std::min<uint64_t>(T, std::max<uint64_t>(1, count / 100000));
+  std::vector<std::string> errors(T);
+  auto work = [&](unsigned t) {
+    const size_t lo = (size_t)(count * t / T), hi = (size_t)(count * (t + 1) / T);
+    for (size_t k = lo; k < hi; ++k) {
+      const char* p = s.data() + starts[k];
+      const char* end = s.data() + std::min(starts[k + 1], s.size());
+      if (end > p && end[-1] == '\n') --end;
+      if (end > p && end[-1] == '\r') --end;
+      const char* q = p;
+      double x = 0;
+      if (!field_f64(q, end, x) || !blank(q, end)) {
+        if (errors[t].empty())
+          errors[t] = "Parse error at line " + std::to_string(first_line + k) + " of " + path +
+                      ": " + std::string(p, end);
+        continue;
+      }
+      m.colmajor[k] = x;
+    }
+  };
+  if (T > 1) {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < T; ++t) pool.emplace_back(work, t);
+    for (auto& th : pool) th.join();
+  } else {
+    work(0);
+  }
+  for (auto& e : errors)
+    if (!e.empty()) throw MmError(e);
   while (L.next(a, b))
     if (!blank(a, b))
       throw MmError("Unexpected input at at line " + std::to_string(L.number) + " of " + path +

@@ -184,3 +184,28 @@ def test_writers_format_like_printf_16g(tmp_path):
     P.write_mm_coord(str(tmp_path / "v.mmc"), 1000, 50, rows, cols, vals)
     body = open(tmp_path / "v.mmc").read().splitlines()[7:]
     assert body == ["%d %d %s" % (i + 1, j + 1, "%.16g" % x) for i, j, x in zip(rows, cols, vals)]
+
+
+def test_readers_take_what_strtod_takes(tmp_path):
+    # values are parsed in place; anything unusual must still read as strtod reads it
+    import ctypes
+    libc = ctypes.CDLL(None)
+    libc.strtod.restype = ctypes.c_double
+    libc.strtod.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    vals = ["1", "+2.5", "-0", "1e-310", "1e400", "-1e400", "0x1p3", "inf", "-Infinity", "nan",
+            "  7.25  ", "3.", ".5", "1E+5", "1.7976931348623157e308", "4.9e-324"]
+    path = tmp_path / "s.mma"
+    path.write_text("%%MatrixMarket matrix array real general\n%c\n"
+                    + f"{len(vals)} 1\n" + "\n".join(vals) + "\n")
+    got = P.read_mm_array(str(path)).ravel()
+    want = np.array([libc.strtod(x.encode(), None) for x in vals])
+    np.testing.assert_array_equal(got, want)
+    assert np.array_equal(np.signbit(got), np.signbit(want))
+    coo = tmp_path / "s.mmc"
+    coo.write_text("%%MatrixMarket matrix coordinate real general\n3 3 2\n+1 2 0x1p-2\n3\t3  -1e400\n")
+    _, _, r, c, v = P.read_sparse(str(coo))
+    assert list(r) == [0, 2] and list(c) == [1, 2] and v[0] == 0.25 and v[1] == -np.inf
+    for bad in ("1.5x", "abc", ""):
+        path.write_text("%%MatrixMarket matrix array real general\n1 1\n" + bad + "\n")
+        with pytest.raises(P.DsgdppError, match="Parse error at line 3"):
+            P.read_mm_array(str(path))
