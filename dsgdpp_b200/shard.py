@@ -157,3 +157,114 @@ def run_epoch(eps: float, schedule: np.ndarray, seeds: np.ndarray, d: int, world
         exchange(plan[s])
         for r in ranks:
             epoch_part(r, s)
+
+
+# ---- a whole job over torchrun ranks ---------------------------------------------------
+def _bold_driver(eps: float, prev: float, cur: float, dec: float = 0.5, inc: float = 1.05) -> float:
+    """BoldDriver (mf/sgd/decay/decay_bolddriver.h:59-67)"""
+    return eps * (dec if prev <= cur else inc)
+
+
+def main(argv=None):
+    """DSGD++ over torchrun ranks with BoldDriver, one GPU per rank:
+
+        torchrun --nproc-per-node G -m dsgdpp_b200.shard --tasks D --epochs E \\
+            --input-file V.mmc --input-test-file T.mmc --input-row-file W.mma --input-col-file H.mma
+
+    or --synthetic M,N,NNZ,NTEST,RANK for seeded synthetic data.  Prints one
+    JSON line per epoch on rank 0 (training and test loss, step)."""
+    import argparse
+    import datetime
+    import json
+    import os
+    import torch
+    import torch.distributed as dist
+    from . import Config, Context, Random32, TEST, TRAIN, block_offsets, draw_schedule
+    from . import read_mm_array, read_sparse, synth
+
+    ap = argparse.ArgumentParser(prog="python -m dsgdpp_b200.shard")
+    ap.add_argument("--input-file"); ap.add_argument("--input-test-file")
+    ap.add_argument("--input-row-file"); ap.add_argument("--input-col-file")
+    ap.add_argument("--synthetic", help="M,N,NNZ,NTEST,RANK")
+    ap.add_argument("--tasks", type=int, required=True)
+    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--eps0", type=float, default=0.001)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--exec", default="hogwild")
+    ap.add_argument("--loss-lambda", type=float, default=1.0)
+    ap.add_argument("--backend", default="nccl")
+    args = ap.parse_args(argv)
+
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dev = local % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
+    xdev = "cuda" if args.backend == "nccl" else "cpu"
+    try:
+        if args.synthetic:
+            m, n, nnz, ntest, r = (int(x) for x in args.synthetic.split(","))
+            p = synth.make(m, n, nnz, ntest, rank_true=min(r, 8), r=r, noise=0.1, seed=args.seed)
+            rows, cols, vals = p.rows, p.cols, p.vals
+            trows, tcols, tvals = p.trows, p.tcols, p.tvals
+            W0, H0 = p.W0, p.H0
+        else:
+            m, n, rows, cols, vals = read_sparse(args.input_file)
+            _, _, trows, tcols, tvals = read_sparse(args.input_test_file)
+            W0 = read_mm_array(args.input_row_file)
+            H0 = np.ascontiguousarray(read_mm_array(args.input_col_file).T)
+            r = W0.shape[1]
+        d = args.tasks
+        off1 = list(block_offsets(m, d)) + [m]
+        lo, hi = rank_rows(off1, d, world, rank)
+        keep = (rows >= lo) & (rows < hi)
+        tkeep = (trows >= lo) & (trows < hi)
+        ctx = Context(Config(m=m, n=n, rank=r, d=d, precision=args.precision, exec=args.exec,
+                             launch="stream", device=dev, loss_lambda=args.loss_lambda))
+        ctx.set_matrix(TRAIN, rows[keep], cols[keep], vals[keep])
+        ctx.set_matrix(TEST, trows[tkeep], tcols[tkeep], tvals[tkeep])
+        ctx.set_counts(np.bincount(rows, minlength=m).astype(np.uint64),
+                       np.bincount(cols, minlength=n).astype(np.uint64))
+        Wz = np.zeros_like(W0)  # rows of other ranks stay zero: they add nothing to L2 here
+        Wz[lo:hi] = W0[lo:hi]
+        ctx.set_factors(Wz, H0)
+        holder = new_holders(2 * d)
+
+        def job_losses():
+            share_torch(dist, rank, ctx, holder, xdev)
+            w2, h2 = ctx.l2()
+            t = torch.tensor([ctx.nzsl(TRAIN), w2, ctx.nzsl(TEST)], dtype=torch.float64,
+                             device=xdev)
+            dist.all_reduce(t)
+            a = t.cpu().numpy()
+            return a[0] + args.loss_lambda * (a[1] + h2), a[2]
+
+        master = Random32(args.seed)
+        loss, test = job_losses()
+        if rank == 0:
+            print(json.dumps({"epoch": 0, "loss": loss, "test_loss": test}), flush=True)
+        eps, prev = args.eps0, None
+        for e in range(1, args.epochs + 1):
+            if prev is not None:
+                eps = _bold_driver(eps, prev, loss)
+            sched, seeds = draw_schedule(master, d)
+            t = torch.from_numpy(np.concatenate([sched.ravel(), seeds]).astype(np.int64)).to(xdev)
+            dist.broadcast(t, 0)  # rank 0's draws for every rank
+            a = t.cpu().numpy().astype(np.uint32)
+            sched, seeds = a[:2 * d * d].reshape(2 * d, d), a[2 * d * d:]
+            run_epoch(eps, sched, seeds, d, world, holder, [rank],
+                      lambda _r, s: ctx.epoch_part(eps, sched, seeds, s, s + 1),
+                      lambda moves: torch_exchange(dist, rank, ctx, moves, xdev))
+            prev = loss
+            loss, test = job_losses()
+            if rank == 0:
+                print(json.dumps({"epoch": e, "loss": loss, "test_loss": test, "eps": eps}),
+                      flush=True)
+        ctx.close()
+    finally:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -178,3 +178,39 @@ def test_two_processes_hand_blocks_over_with_torch_distributed():
         np.testing.assert_array_equal(H[off2[b]:off2[b + 1]], Hr[off2[b]:off2[b + 1]])
     for r in range(2):
         assert out[f"loss{r}"] == pytest.approx(out["ref_loss"], rel=1e-12)
+
+
+def test_torchrun_job_matches_the_single_context_run(tmp_path):
+    # the whole job (BoldDriver, losses over ranks) as two torchrun processes
+    # sharing this GPU and meeting over gloo; FP64 replay, so the per-epoch
+    # losses must be the single context's
+    import json
+    import os
+    import socket
+    import subprocess
+    import sys
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    m, n, nnz, ntest, r, d, epochs, seed = 900, 700, 20000, 2000, 8, 4, 4, 6
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr=127.0.0.1", f"--master-port={port}", "-m", "dsgdpp_b200.shard",
+           f"--synthetic={m},{n},{nnz},{ntest},{r}", f"--tasks={d}", f"--epochs={epochs}",
+           f"--seed={seed}", "--precision=fp64", "--exec=replay", "--backend=gloo"]
+    env = dict(os.environ, PYTHONPATH=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-3000:]
+    rows = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    assert [x["epoch"] for x in rows] == list(range(epochs + 1))
+    p = synth.make(m, n, nnz, ntest, rank_true=min(r, 8), r=r, noise=0.1, seed=seed)
+    with P.Context(P.Config(m=m, n=n, rank=r, d=d, precision="fp64", exec="replay")) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ctx.set_factors(p.W0, p.H0)
+        ctx.seed(seed)
+        trace = ctx.run(epochs, "BoldDriver", 0.001)
+    for got, want in zip(rows, trace):
+        assert got["loss"] == pytest.approx(want["loss"], rel=1e-11)
+        assert got["test_loss"] == pytest.approx(want["test_loss"], rel=1e-11)
+        if got["epoch"] > 0:
+            assert got["eps"] == pytest.approx(want["eps"], rel=1e-15)
