@@ -88,6 +88,67 @@ bool field_f64(const char*& p, const char* e, double& x) {
   return true;
 }
 
+// Starts of the first `count` lines from byte `pos` on, found by several
+// threads (each scans one byte range that begins right after a newline);
+// *end gets the position after the last of them.  False if the text has
+// fewer lines.
+bool line_starts(const std::string& s, size_t pos, uint64_t count, std::vector<size_t>& out,
+                 size_t* end) {
+  out.clear();
+  if (count == 0) {
+    *end = pos;
+    return true;
+  }
+  const size_t n = s.size() > pos ? s.size() - pos : 0;
+  unsigned T = std::max(1u, std::thread::hardware_concurrency());
+  if (n < (1u << 22)) T = 1;
+  std::vector<size_t> cut(T + 1);
+  cut[0] = pos;
+  cut[T] = s.size();
+  for (unsigned t = 1; t < T; ++t) {
+    size_t c = pos + n * t / T;
+    const void* nl = c < s.size() ? std::memchr(s.data() + c, '\n', s.size() - c) : nullptr;
+    c = nl ? (size_t)(static_cast<const char*>(nl) - s.data()) + 1 : s.size();
+    cut[t] = std::max(c, cut[t - 1]);
+  }
+  std::vector<std::vector<size_t>> parts(T);
+  auto work = [&](unsigned t) {
+    for (size_t p = cut[t]; p < cut[t + 1];) {
+      parts[t].push_back(p);
+      const void* nl = std::memchr(s.data() + p, '\n', cut[t + 1] - p);
+      p = nl ? (size_t)(static_cast<const char*>(nl) - s.data()) + 1 : cut[t + 1];
+    }
+  };
+  if (T == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < T; ++t) pool.emplace_back(work, t);
+    for (auto& th : pool) th.join();
+  }
+  size_t total = 0;
+  for (auto& p : parts) total += p.size();
+  if (total < count) return false;
+  out.reserve(count);
+  for (auto& p : parts)
+    for (size_t v : p) {
+      if (out.size() == count) break;
+      out.push_back(v);
+    }
+  if (total > count) {  // the start of the line after the last one taken
+    uint64_t k = 0;
+    for (auto& p : parts) {
+      if (k + p.size() > count) {
+        *end = p[count - k];
+        return true;
+      }
+      k += p.size();
+    }
+  }
+  *end = s.size();
+  return true;
+}
+
 // Cursor over the lines of a text buffer.
 struct Lines {
   const std::string& s;
@@ -140,15 +201,10 @@ Coo read_mm_coord(const std::string& path, unsigned threads) {
   m.vals.resize((size_t)nnz);
   // entry lines: find the start of each of the nnz lines, then parse in parallel
   std::vector<size_t> starts;
-  starts.reserve((size_t)nnz + 1);
-  size_t pos = L.pos;
+  size_t pos = 0;
   const uint64_t first_line = L.number + 1;
-  for (long long k = 0; k < nnz; ++k) {
-    if (pos >= s.size()) throw MmError("Unexpected EOF in file " + path);
-    starts.push_back(pos);
-    size_t e = s.find('\n', pos);
-    pos = (e == std::string::npos) ? s.size() : e + 1;
-  }
+  if (!line_starts(s, L.pos, (uint64_t)nnz, starts, &pos))
+    throw MmError("Unexpected EOF in file " + path);
   if (!blank(s.data() + std::min(pos, s.size()), s.data() + s.size())) {
     // locate the offending line for the message (read_impl.h:106-111)
     Lines R(s);
@@ -214,14 +270,13 @@ Dense read_mm_array(const std::string& path) {
   m.colmajor.resize(count);
   // line starts first, then the values in parallel (as read_mm_coord)
   std::vector<size_t> starts;
-  starts.reserve(count + 1);
   const uint64_t first_line = L.number + 1;
-  for (uint64_t k = 0; k < count; ++k) {
-    if (L.pos >= s.size()) throw MmError("Unexpected EOF in file " + path);
-    starts.push_back(L.pos);
-    L.next(a, b);
-  }
-  starts.push_back(L.pos);
+  size_t after = 0;
+  if (!line_starts(s, L.pos, count, starts, &after))
+    throw MmError("Unexpected EOF in file " + path);
+  starts.push_back(after);
+  L.pos = after;
+  L.number += count;
   unsigned T = std::max(1u, std::thread::hardware_concurrency());
   T = (unsigned)std::min<uint64_t>(T, std::max<uint64_t>(1, count / 100000));
   std::vector<std::string> errors(T);
