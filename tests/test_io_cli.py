@@ -209,3 +209,19 @@ def test_readers_take_what_strtod_takes(tmp_path):
         path.write_text("%%MatrixMarket matrix array real general\n1 1\n" + bad + "\n")
         with pytest.raises(P.DsgdppError, match="Parse error at line 3"):
             P.read_mm_array(str(path))
+
+
+def test_cli_rm_input_errors(tmp_path):
+    # .rm inputs are checked before any device work
+    base = ["--rank=3", "--tasks-per-rank=2", "--update=Nzsl", "--regularize=None", "--loss=Nzsl",
+            "--decay=BoldDriver(0.01)"]
+    missing = str(tmp_path / "none.rm")
+    r = _cli(f"--input-file={missing}", f"--input-row-file={missing}",
+             f"--input-col-file={missing}", *base)
+    assert r.returncode == 1 and "Cannot open file" in r.stderr
+    factors_only = str(tmp_path / "f.rm")
+    P.RandomMatrix.create(60, 40, 3, 4, 0, 0, 3, "Uniform(-1,1)").save(factors_only)
+    r = _cli(f"--input-file={factors_only}", f"--input-row-file={factors_only}",
+             f"--input-col-file={factors_only}", *base)
+    assert r.returncode == 1 and "holds no data matrix" in r.stderr
+    assert "generating data matrices on the fly" in r.stdout
