@@ -84,7 +84,10 @@ def local_exchange(ctxs: Dict[int, object], moves: List[Move], device: int = 0):
 
 def torch_exchange(pg, rank: int, ctx, moves: List[Move], device: str = "cuda"):
     """This rank's part of the moves, as one batch of torch.distributed
-    point-to-point operations (every rank calls it with the same moves)."""
+    point-to-point operations (every rank calls it with the same moves).
+    With NCCL, torch wants every rank in the group's first communication, so
+    a collective (the schedule broadcast of the job) must come first; ranks
+    without a move in a sub-epoch then simply skip the batch."""
     import torch
     ops, recvs = [], []
     for b2, src, dst in moves:
