@@ -14,7 +14,7 @@ One step = one DSGD++ epoch (2d sub-epochs over all training entries) of the
            (12 B entry + 4 r 4 B of factor rows/columns + 8 B inverse counts per
            update) over its event-timed average launch duration;
 * cpu_baseline: the CPU restatement of the reference (oracle, threaded mode,
-           one thread per task, d = threads) timed on a 10M-entry sample;
+           d = threads tasks, all host threads) timed on a 10M-entry sample;
            test_rmse_vs_fp64_oracle compares this implementation's test RMSE
            with the oracle's on that sample (same d, seed and steps);
 * time_to_target: plain FP32 BoldDriver runs 50 epochs; its final test RMSE
@@ -22,8 +22,9 @@ One step = one DSGD++ epoch (2d sub-epochs over all training entries) of the
            controller (FP32, BF16) race to, in wall time of every epoch, loss
            and step decision.
 
-`--impl reference` times only the CPU restatement of the reference path (all
-host cores) on the same sample and prints its own line.
+`--impl reference` times only the CPU restatement of the reference path on
+the whole workload (every training entry, d = 64, all host threads), without
+loading the CUDA library, and prints its own line with the same `config`.
 Under torchrun every rank runs an independent replica of the job (the path is
 one GPU per job); value is the sum over ranks / the max time over ranks.
 """
@@ -147,18 +148,22 @@ def algorithmic_bytes_per_update(r, precision, update):
     return 12 + 4 * r * s_f + (8 if update == "Nzsl_L2" else 0)
 
 
-def traffic_per_launch(name, d):
-    """DRAM bytes per launch of the Hogwild kernel from the committed ncu summary
-    (None unless the summary was taken at the same d)."""
+def traffic_per_launch(name, shape):
+    """DRAM bytes per launch of the Hogwild kernel from the committed ncu summary,
+    or None unless the summary profiled the same kernel instance: the same d,
+    lanes per entry, vectors per lane and grid (`shape`, a dict of those four)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         text = open(path).read()
     except OSError:
         return None
     m = re.search(r"dram_bytes_per_launch_scaled:\s*([0-9.eE+]+)", text)
-    md = re.search(r"profiled_d:\s*([0-9]+)", text)
-    if not m or not md or int(md.group(1)) != d:
+    if not m:
         return None
+    for key in ("d", "lanes", "vecs", "grid"):
+        mk = re.search(rf"profiled_{key}:\s*([0-9]+)", text)
+        if not mk or int(mk.group(1)) != int(shape[key]):
+            return None
     return float(m.group(1))
 
 
@@ -221,11 +226,23 @@ def gpu_sample_rmse(P, data, wl, precision, d, epochs, write_mode, device, layou
         return float(np.sqrt(ctx.nzsl(P.TEST) / len(data["tvals"])))
 
 
+def _synth_gpu():
+    """dsgdpp_b200/synth_gpu.py loaded as a module of its own: it needs only torch
+    and numpy, and importing it through the package would load the CUDA
+    library, which the reference arm must not do."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "dsgdpp_synth_gpu", os.path.join(ROOT, "dsgdpp_b200", "synth_gpu.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def generate(wl, seed):
     import torch
-    from dsgdpp_b200 import synth_gpu
+    synth_gpu = _synth_gpu()
     t0 = time.time()
-    dev = f"cuda:{torch.cuda.current_device()}"
+    dev = f"cuda:{torch.cuda.current_device()}" if torch.cuda.is_available() else "cpu"
     if wl.get("kind") == "ratings":
         data = synth_gpu.make_ratings(wl["m"], wl["n"], wl["nnz"], wl["nnz_test"], wl["rank"], seed,
                                       device=dev)
@@ -234,6 +251,29 @@ def generate(wl, seed):
                           r=wl["rank"], noise=wl["noise"], seed=seed, s_row=wl["s"],
                           s_col=wl["s"], device=dev)
     return data, time.time() - t0
+
+
+def workload_config(wl, precision):
+    """The `config` of both arms' lines: what defines the workload, nothing
+    that depends on the implementation (launch shapes go to `launch`)."""
+    entries_gb = 12 * wl["nnz"] / 1e9
+    factors_mb = 4 * (wl["m"] + wl["n"]) * wl["rank"] / 1e6
+    tuned = wl in (WORKLOADS["c2"], WORKLOADS["c2s"])
+    return {"workload": wl["text"], "m": wl["m"], "n": wl["n"], "nnz": wl["nnz"],
+            "nnz_test": wl["nnz_test"], "rank": wl["rank"], "precision": precision,
+            "blocking": ("d x 2d, d autotuned in 64..512" if tuned else f"d x 2d, d = {wl['d']}"),
+            "l2_flush": (f"inputs larger than L2 ({entries_gb:.1f} GB entries + "
+                         f"{factors_mb:.0f} MB factors)")}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def pinned(a):
@@ -289,21 +329,52 @@ def barrier(pg):
         pg.barrier()
 
 
-def run_reference(args, world, rank, pg):
+def run_reference(args):
+    """The reference's CPU path (the oracle restatement of the DSGD++ epoch; the
+    reference binary cannot be built here) on the whole workload: every
+    training entry, FP64, d = 64 tasks (64 x 128 blocks) run by all host
+    threads with a barrier per sub-epoch; the epoch time excludes losses, as
+    the reference reports it.  Rank 0 only; the CUDA library is never loaded."""
+    import torch
+    from oracle import oracle as O
     wl = WORKLOADS[args.workload]
-    if rank != 0:
-        return 0
-    data, _ = generate(wl, args.seed)
-    ref = time_cpu_reference(data, wl, args.steps, args.warmup)
-    line = {"metric": "SGD updates/s (DSGD++ epoch)", "value": ref["value"], "unit": "updates/s",
+    d = args.d or wl["d"]
+    data, gen_s = generate(wl, args.seed)
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    prob = O.Problem(wl["m"], wl["n"], wl["rank"], d, data["rows"], data["cols"], data["vals"],
+                     data["trows"], data["tcols"], data["tvals"])
+    l2 = wl["s"] is not None and wl.get("kind") != "ratings"
+    prob.configure(update="Nzsl_L2", update_lambda=1.0, regularize="L2" if l2 else "None",
+                   regularize_lambda=0.05 if l2 else 0.0, loss="Nzsl_L2", loss_lambda=1.0)
+    prob.set_factors(data["W0"], data["H0"])
+    prob.seed(args.seed)
+    setup_s = time.time() - t0
+    nnz = len(data["vals"])
+    for _ in range(args.warmup):
+        prob.epoch(0.001, threads=threads)
+    times = [prob.epoch(0.001, threads=threads) * 1e-9 for _ in range(args.steps)]
+    t = sum(times)
+    value = nnz * args.steps / t
+    sample = (f"the whole workload: {nnz:,} training entries per epoch, FP64, d={d} tasks x "
+              f"{2 * d} column blocks on {threads} threads, {args.steps} epochs after "
+              f"{args.warmup} warm-up epochs")
+    line = {"metric": "SGD updates/s (DSGD++ epoch)", "value": value, "unit": "updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ref["epoch_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": wl["text"] + f"; CPU sample of {CPU_SAMPLE:,} entries"},
+            "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded; no public dataset)",
+            "config": workload_config(wl, args.precision),
             "impl": "reference",
-            "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": ref["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads,
+                             "cpu_model": cpu_model(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "epoch_s": {"median": statistics.median(times), "min": min(times),
+                        "max": max(times)},
+            "final_test_rmse": float(np.sqrt(prob.nzsl(1) / len(data["tvals"]))),
+            "generate_s": gen_s, "setup_s": setup_s}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -335,12 +406,17 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    world, rank, local, pg = dist_setup()
     if args.impl == "reference":
-        rc = run_reference(args, world, rank, pg)
-        if pg is not None:
-            pg.destroy_process_group()
-        return rc
+        # rank 0 alone times the CPU path; other ranks exit without work and
+        # without joining a process group
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return run_reference(args)
+
+    world, rank, local, pg = dist_setup()
 
     import dsgdpp_b200 as P
     wl = WORKLOADS[args.workload]
@@ -408,7 +484,8 @@ def main():
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
     suffix = "" if args.precision == "fp32" else "_" + args.precision
-    traffic = (traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", d)
+    shape = {"d": d, "lanes": lanes, "vecs": vecs, "grid": grid}
+    traffic = (traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", shape)
                if args.launch != "persistent" else None)
 
     # ---- end to end through the C ABI from pinned host buffers ----
@@ -446,6 +523,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref = time_cpu_reference(data, wl, steps=2, warmup=0, with_test=True)
         cpu = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu["cpu_model"] = cpu_model()
         # the same sample, d, seed and steps on the GPU: test RMSE against the FP64 oracle
         got = gpu_sample_rmse(P, data, wl, args.precision, ref["d"], ref["epochs"],
                               args.write_mode, local, args.layout)
@@ -476,19 +554,20 @@ def main():
             "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
             "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": wl["text"], "d": d, "blocks": f"{d} x {2 * d}",
-                       "nnz": nnz, "precision": args.precision, "exec": "hogwild",
+            "config": workload_config(wl, args.precision),
+            "launch": {"d": d, "blocks": f"{d} x {2 * d}", "exec": "hogwild",
                        "launch": args.launch, "lanes_per_nnz": lanes, "vecs_per_lane": vecs,
-                       "write_mode": args.write_mode, "layout": args.layout,
-                       "grid": grid, "parallelism": f"replicas x{world}", "autotune": tune,
-                       "l2_flush": "inputs larger than L2 (1.2 GB entries + 320 MB factors)"},
+                       "write_mode": args.write_mode, "layout": args.layout, "grid": grid,
+                       "parallelism": f"replicas x{world}", "autotune": tune},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": peak_kind,
                          "bytes_per_update": bpu,
                          "kernel": ("hogwild_epoch_kernel" if args.launch == "persistent"
                                     else "hogwild_subepoch_kernel"),
-                         "avg_launch_us": avg_launch_s * 1e6},
+                         "avg_launch_us": avg_launch_s * 1e6,
+                         "timing": "CUDA events around each sub-epoch launch of 2 epochs "
+                                   "launched on the library stream (not from the graph)"},
             "cpu_baseline": cpu,
             "test_rmse_vs_fp64_oracle": vs_oracle,
             "time_to_target": ttt,

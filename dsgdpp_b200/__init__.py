@@ -208,6 +208,7 @@ SIGNATURES = {
     "dsgdpp_h_block_bytes": (C.c_int, [_P, C.c_uint32, _u64p]),
     "dsgdpp_h_block_copy": (C.c_int, [_P, C.c_uint32, _P, C.c_int]),
     "dsgdpp_set_counts": (C.c_int, [_P, _u64p, _u64p]),
+    "dsgdpp_set_wait_limit": (C.c_int, [_P, C.c_double]),
     "dsgdpp_set_factors_rm": (C.c_int, [_P, _P]),
 }
 
@@ -427,6 +428,10 @@ class Context:
         v = C.c_double()
         self._check(lib.dsgdpp_last_epoch_ms(self._h, C.byref(v)), "last_epoch_ms")
         return v.value
+
+    def set_wait_limit(self, seconds: float):
+        """How long a dependency wait of the persistent epoch may last."""
+        self._check(lib.dsgdpp_set_wait_limit(self._h, float(seconds)), "set_wait_limit")
 
     def set_kernel_timing(self, on: bool):
         self._check(lib.dsgdpp_set_kernel_timing(self._h, int(on)), "set_kernel_timing")

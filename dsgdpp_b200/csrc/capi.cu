@@ -580,7 +580,7 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c, uint32_t s0, uint32_t s1) {
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   const bool prof = c->profiling && c->prof_ev.size() == d2 + 1 && s0 == 0 && s1 == d2;
   if (persistent) {
-    EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d, d2};
+    EpochDeps dp{c->d_dep_col, c->d_done, c->d_ticket, c->d_ticket + 1, d, d2, c->wait_ns};
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[0], st), "event");
     check_cuda(launch_hogwild_epoch(c->cfg.precision, c->lanes, c->vecs, a, dp, c->grid, st),
                "hogwild_epoch");
@@ -667,7 +667,9 @@ void run_hogwild_epoch(dsgdpp_ctx* c, double eps, uint32_t s0, uint32_t s1) {
     check_cuda(cudaEventSynchronize(c->ev_end), "event sync");
     if (*c->h_error) {
       *c->h_error = 0;
-      throw Error(DSGDPP_E_CUDA, "persistent epoch: a dependency wait gave up");
+      throw Error(DSGDPP_E_CUDA, "persistent epoch: a dependency wait gave up after " +
+                                     std::to_string(c->wait_ns / 1000) +
+                                     " us; the epoch is incomplete");
     }
   }
 }
@@ -1186,6 +1188,19 @@ int dsgdpp_last_epoch_ms(dsgdpp_ctx* c, double* ms) {
     float f = 0;
     check_cuda(cudaEventElapsedTime(&f, c->ev_begin, c->ev_end), "elapsed");
     *ms = f;
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_wait_limit(dsgdpp_ctx* c, double seconds) {
+  return guarded(c, [&]() {
+    if (!(seconds >= 0) || seconds > 3600)
+      throw Error(DSGDPP_E_INVALID, "the wait limit must be in [0, 3600] seconds");
+    const uint64_t ns = (uint64_t)(seconds * 1e9);
+    if (ns != c->wait_ns) {
+      c->wait_ns = ns;
+      release_graph(c);  // the limit is a launch argument: capture the epoch again
+    }
     return DSGDPP_OK;
   });
 }

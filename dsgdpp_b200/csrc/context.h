@@ -112,6 +112,7 @@ struct dsgdpp_ctx {
   int32_t* h_dep_col = nullptr;
   uint32_t* d_ticket = nullptr;   // [0] chunk ticket, [1] error flag
   uint32_t* h_error = nullptr;    // error flag read back after each epoch
+  uint64_t wait_ns = 1000000000ull;  // dependency wait limit (dsgdpp_set_wait_limit)
   // replay
   uint32_t* h_positions = nullptr;
   uint32_t* d_positions = nullptr;

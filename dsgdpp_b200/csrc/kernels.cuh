@@ -88,6 +88,7 @@ struct EpochDeps {
   uint32_t* error;         // set when a dependency wait gave up
   uint32_t d;
   uint32_t nsub;           // sub-epochs (2d for DSGD++, d for DSGD)
+  uint64_t wait_ns;        // a dependency wait gives up after this long
 };
 
 // ---- launchers (return cudaError_t) -------------------------------------------

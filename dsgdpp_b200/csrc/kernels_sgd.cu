@@ -411,21 +411,30 @@ __global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeo
   }
 }
 
-// A dependency wait polls for about 8 s at most, then the epoch gives up (error
-// flag) instead of waiting for ever.
-constexpr uint32_t kWaitLimit = 1u << 23;
-
 __device__ __forceinline__ uint32_t load_acquire(const uint32_t* p) {
   uint32_t v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
-// polls until *done >= need; false if it gave up (or another warp did)
-__device__ __forceinline__ bool wait_done(const uint32_t* done, uint32_t need, uint32_t* error) {
-  uint32_t it = 0;
-  while (load_acquire(done) < need) {
-    if (++it >= kWaitLimit || *reinterpret_cast<volatile uint32_t*>(error)) {
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Polls until *done >= need; false if it gave up (or another warp did).  A
+// wait gives up after limit_ns of the global timer (the epoch then reports an
+// error instead of waiting for ever); a poll count of limit_ns / 16 + 1024 --
+// more than the timer allows, since every poll is an L2 round trip plus a
+// sleep -- bounds it should the timer not advance.
+__device__ __forceinline__ bool wait_done(const uint32_t* done, uint32_t need, uint32_t* error,
+                                          uint64_t limit_ns) {
+  if (load_acquire(done) >= need) return true;
+  const uint64_t t0 = global_ns(), max_polls = limit_ns / 16 + 1024;
+  for (uint64_t it = 0; load_acquire(done) < need; ++it) {
+    if (global_ns() - t0 > limit_ns || it >= max_polls ||
+        *reinterpret_cast<volatile uint32_t*>(error)) {
       atomicExch(error, 1u);
       return false;
     }
@@ -438,7 +447,9 @@ __device__ __forceinline__ bool wait_done(const uint32_t* done, uint32_t need, u
 // chunks of sub-epoch s in the same order as the launch-per-sub-epoch form); a
 // chunk of segment (s, i) first waits for segment (s-1, i) and for
 // dep_col[s][i].  Every chunk waited for holds a smaller ticket, and tickets
-// go to running warps only, so the waits end; each is bounded anyway.  A
+// go to running warps only, so the waits end; each is bounded anyway (a wait
+// that runs out sets the error flag, and every warp then stops taking
+// tickets and returns).  A
 // finished chunk publishes its writes (fence) before it counts itself done.
 template <typename T, int LPN, int VPL>
 __global__ void __launch_bounds__(256) hogwild_epoch_kernel(HogwildArgs a, EpochDeps dp) {
@@ -499,12 +510,14 @@ __global__ void __launch_bounds__(256) hogwild_epoch_kernel(HogwildArgs a, Epoch
       uint32_t ok = 1;
       if (lane == 0 && s > 0) {
         const Segment* ps = a.segs + a.launches[s - 1].seg_begin;
-        ok = wait_done(dp.done + (me - d), ps[lo + 1].chunk_begin - ps[lo].chunk_begin, dp.error);
+        ok = wait_done(dp.done + (me - d), ps[lo + 1].chunk_begin - ps[lo].chunk_begin, dp.error,
+                       dp.wait_ns);
         const int32_t dc = dp.dep_col[me];
         if (ok && dc >= 0) {
           const uint32_t ds = (uint32_t)dc / d, dj = (uint32_t)dc % d;
           const Segment* qs = a.segs + a.launches[ds].seg_begin;
-          ok = wait_done(dp.done + dc, qs[dj + 1].chunk_begin - qs[dj].chunk_begin, dp.error);
+          ok = wait_done(dp.done + dc, qs[dj + 1].chunk_begin - qs[dj].chunk_begin, dp.error,
+                         dp.wait_ns);
         }
       }
       if (!__shfl_sync(kFullMask, ok, 0)) break;

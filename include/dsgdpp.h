@@ -202,6 +202,14 @@ int dsgdpp_epoch_part(dsgdpp_ctx* ctx, double eps, const uint32_t* schedule,
  * context's device can reach.  Synchronous. */
 int dsgdpp_h_block_bytes(dsgdpp_ctx* ctx, uint32_t b2, uint64_t* bytes);
 int dsgdpp_h_block_copy(dsgdpp_ctx* ctx, uint32_t b2, void* device_buf, int to_context);
+/* How long one dependency wait of the persistent epoch (DSGDPP_LAUNCH_PERSISTENT)
+ * may last before the epoch gives up, in seconds (default 1; 0 gives up at the
+ * first unmet dependency).  A wait that runs out sets an error flag; every
+ * warp then stops, dsgdpp_epoch returns DSGDPP_E_CUDA with a message, the
+ * epoch is left incomplete, and the context stays usable.  Replaces the
+ * unbounded barrier(channels) that ends a sub-epoch in the reference
+ * (mf/sgd/dsgdpp_impl.h:259-263); the other launch forms do not wait. */
+int dsgdpp_set_wait_limit(dsgdpp_ctx* ctx, double seconds);
 /* Device time of the last epoch's kernels in milliseconds. */
 int dsgdpp_last_epoch_ms(dsgdpp_ctx* ctx, double* ms);
 /* Per-kernel timing of the Hogwild sub-epoch kernels: when on, epochs launch
@@ -228,22 +236,30 @@ int dsgdpp_nzl2(dsgdpp_ctx* ctx, double* w, double* h);
 /* Capacity of the fixed scratch of dsgdpp_nzsl_fp32_noalloc, in partial sums
  * (4096 doubles = 32 KiB of device memory per GPU that loads this library). */
 #define DSGDPP_NOALLOC_MAX_PARTIALS 4096
+/* Widest factor row dsgdpp_nzsl_fp32_noalloc takes, in floats (128 vectors:
+ * the widest lane mapping of the loss kernel). */
+#define DSGDPP_NOALLOC_MAX_LD 512
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory -- code running inside another framework's memory pool, or under an
  * allocator it does not own -- this computes the same sum of squared errors
  * as dsgdpp_nzsl, sum over k < nnz of (vals[k] - W[rows[k]] . H[cols[k]])^2
  * accumulated in FP64, from caller-owned device buffers: FP32 values, W and H
- * as FP32 rows of `ld` floats (ld a multiple of 4 and >= rank rounded up to
- * 4; W and H 16-byte aligned; only the first `rank` entries of a row count).
- * The result is written to the device double *out, ordered on `stream` (a
- * cudaStream_t; NULL is the default stream).  The call allocates and frees
- * nothing: its scratch is a fixed device array of DSGDPP_NOALLOC_MAX_PARTIALS
- * doubles, one per CTA; `partials` sets the CTA count (0 = 4 per SM) and a
- * count above the capacity returns DSGDPP_E_INVALID with a message on stderr.
- * The first call on a device looks up the scratch address (device set-up);
- * make that first call before any stream capture.  All calls on a device share
- * the scratch, which keeps the last call's contents; calls that overlap on the
- * GPU race on it. */
+ * as FP32 rows of `ld` floats (ld a multiple of 4, >= rank rounded up to 4
+ * and <= DSGDPP_NOALLOC_MAX_LD; W and H 16-byte aligned; only the first
+ * `rank` entries of a row count).  The call takes no matrix shape, so it
+ * cannot check the indices: every rows[k] must name a row of W and every
+ * cols[k] a row of H -- that is the caller's contract.  The result is written
+ * to the device double *out, ordered on `stream` (a cudaStream_t; NULL is the
+ * default stream).  The call allocates and frees nothing: its scratch is a
+ * fixed device array of DSGDPP_NOALLOC_MAX_PARTIALS doubles, one per CTA;
+ * `partials` sets the CTA count (0 = 4 per SM).  A CTA count above the
+ * capacity, or an ld outside the limits above, returns DSGDPP_E_INVALID with
+ * a message on stderr.  The first call in a CUDA context (per device, the
+ * runtime's primary context unless the caller made another current) looks up
+ * the scratch address there (set-up); make that first call before any stream
+ * capture.  A cudaDeviceReset ends the library's use of that device, as for
+ * every other entry point.  All calls in a context share the scratch, which
+ * keeps the last call's contents; calls that overlap on the GPU race on it. */
 int dsgdpp_nzsl_fp32_noalloc(const uint32_t* rows, const uint32_t* cols, const float* vals,
                              uint64_t nnz, const float* W, const float* H, uint32_t rank,
                              uint32_t ld, uint32_t partials, double* out, void* stream);

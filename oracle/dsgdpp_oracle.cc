@@ -31,6 +31,7 @@
 #include "dsgdpp_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <barrier>
 #include <chrono>
 #include <cmath>
@@ -244,20 +245,61 @@ uint32_t blockOf(uint64_t i, const std::vector<uint64_t>& off) {
 std::vector<Block> blockMatrix(const orc_problem& p, uint64_t nnz, const uint32_t* rows,
                                const uint32_t* cols, const double* vals) {
   const uint32_t d = p.d, d2 = p.nb2;
-  std::vector<std::vector<uint64_t>> idx((size_t)d * d2);
-  for (uint64_t k = 0; k < nnz; ++k) {
-    uint32_t b1 = blockOf(rows[k], p.off1), b2 = blockOf(cols[k], p.off2);
-    idx[(size_t)b1 * d2 + b2].push_back(k);
+  const size_t nblk = (size_t)d * d2;
+  // route entries to blocks on all host threads; thread t takes a contiguous
+  // range of entries, so each block lists its entries in input order
+  const unsigned T = nnz > (1u << 20) ? std::max(1u, std::thread::hardware_concurrency()) : 1u;
+  std::vector<uint32_t> bid(nnz);
+  std::vector<std::vector<uint64_t>> cnt(T, std::vector<uint64_t>(nblk + 1, 0));
+  auto range = [&](unsigned t) { return std::make_pair(nnz * t / T, nnz * (t + 1) / T); };
+  auto par = [&](auto&& fn) {
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < T; ++t) pool.emplace_back(fn, t);
+    fn(0u);
+    for (auto& th : pool) th.join();
+  };
+  par([&](unsigned t) {
+    auto [a, b] = range(t);
+    for (uint64_t k = a; k < b; ++k) {
+      const uint32_t blk = blockOf(rows[k], p.off1) * d2 + blockOf(cols[k], p.off2);
+      bid[k] = blk;
+      cnt[t][blk]++;
+    }
+  });
+  std::vector<uint64_t> start(nblk + 1, 0);
+  for (size_t blk = 0; blk < nblk; ++blk) {
+    uint64_t acc = start[blk];
+    for (unsigned t = 0; t < T; ++t) {
+      const uint64_t c = cnt[t][blk];
+      cnt[t][blk] = acc;
+      acc += c;
+    }
+    start[blk + 1] = acc;
   }
-  std::vector<Block> out((size_t)d * d2);
-  for (uint32_t b1 = 0; b1 < d; ++b1)
-    for (uint32_t b2 = 0; b2 < d2; ++b2) {
-      auto& ix = idx[(size_t)b1 * d2 + b2];
-      std::stable_sort(ix.begin(), ix.end(), [&](uint64_t a, uint64_t b) {
-        return rows[a] != rows[b] ? rows[a] < rows[b] : cols[a] < cols[b];
+  std::vector<uint64_t> idx(nnz);
+  par([&](unsigned t) {
+    auto [a, b] = range(t);
+    for (uint64_t k = a; k < b; ++k) idx[cnt[t][bid[k]]++] = k;
+  });
+  std::vector<uint32_t>().swap(bid);
+  std::vector<Block> out(nblk);
+  // blocks are independent: sort (row-major (i, j), mf/matrix/io/read_impl.h:
+  // 162-164) and merge duplicates on all host threads
+  std::atomic<size_t> next{0};
+  par([&](unsigned) {
+    for (size_t blk = next++; blk < nblk; blk = next++) {
+      const uint32_t b1 = (uint32_t)(blk / d2), b2 = (uint32_t)(blk % d2);
+      uint64_t* ib = idx.data() + start[blk];
+      uint64_t* ie = idx.data() + start[blk + 1];
+      std::stable_sort(ib, ie, [&](uint64_t a, uint64_t c) {
+        return rows[a] != rows[c] ? rows[a] < rows[c] : cols[a] < cols[c];
       });
-      Block& B = out[(size_t)b1 * d2 + b2];
-      for (uint64_t k : ix) {
+      Block& B = out[blk];
+      B.i.reserve(ie - ib);
+      B.j.reserve(ie - ib);
+      B.x.reserve(ie - ib);
+      for (const uint64_t* q = ib; q != ie; ++q) {
+        const uint64_t k = *q;
         uint32_t li = (uint32_t)(rows[k] - p.off1[b1]), lj = (uint32_t)(cols[k] - p.off2[b2]);
         if (!B.i.empty() && B.i.back() == li && B.j.back() == lj) {
           B.x.back() += vals[k];
@@ -268,6 +310,7 @@ std::vector<Block> blockMatrix(const orc_problem& p, uint64_t nnz, const uint32_
         }
       }
     }
+  });
   return out;
 }
 
@@ -437,14 +480,20 @@ double epochExplicit(orc_problem& p, double eps, const uint32_t* sched, const ui
       for (uint32_t id = 0; id < d; ++id)
         runTaskSubepoch(p, tasks[id], id, sched[(size_t)s * d + id], eps, scratch);
   } else {
+    // T threads run the d tasks of each sub-epoch, a task to whichever thread
+    // claims it next (the tasks of a sub-epoch are row- and column-disjoint, and
+    // each keeps its own generator and permutation, so the result does not
+    // depend on which thread runs it); a barrier ends every sub-epoch.
     const int T = std::min<int>(threads, (int)d);
     std::barrier<> bar(T);
+    std::vector<std::atomic<uint32_t>> claim(p.nb2);
+    for (auto& c : claim) c.store(0);
     std::vector<std::thread> pool;
     for (int t = 0; t < T; ++t) {
-      pool.emplace_back([&, t]() {
+      pool.emplace_back([&]() {
         std::vector<uint32_t> scratch;
         for (uint32_t s = 0; s < p.nb2; ++s) {
-          for (uint32_t id = (uint32_t)t; id < d; id += (uint32_t)T)
+          for (uint32_t id = claim[s]++; id < d; id = claim[s]++)
             runTaskSubepoch(p, tasks[id], id, sched[(size_t)s * d + id], eps, scratch);
           bar.arrive_and_wait();  // barrier(channels), dsgdpp_impl.h:259-263
         }

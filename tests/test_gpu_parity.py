@@ -349,6 +349,38 @@ def test_persistent_epoch_kernel_timing_and_unsupported_forms():
                                **dict(dict(layout="col_runs"), **bad)))
 
 
+def test_persistent_epoch_wait_limit_gives_up_and_the_context_recovers():
+    # the bounded dependency wait of the one-launch epoch (in place of the
+    # reference's unbounded sub-epoch barrier, mf/sgd/dsgdpp_impl.h:259-263):
+    # with a zero limit the first unmet dependency ends the epoch with an error
+    # status, and the next epoch on the same context runs normally.  Every
+    # sub-epoch here has ~120 chunks against thousands of resident warps, so
+    # warps holding later sub-epochs' tickets meet unfinished dependencies.
+    p = _problem(m=3000, n=2000, nnz=60000, ntest=600, r=12)
+    cfg = P.Config(m=p.m, n=p.n, rank=12, d=8, launch="persistent", layout="col_runs")
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ctx.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ctx.set_factors(p.W0, p.H0)
+        ctx.seed(1)
+        ctx.epoch(0.01)
+        ctx.set_wait_limit(0.0)
+        with pytest.raises(P.DsgdppError) as err:
+            ctx.epoch(0.01)
+        assert err.value.status == P.E_CUDA and "gave up" in str(err.value)
+        ctx.set_wait_limit(1.0)
+        before = ctx.nzsl(P.TEST)
+        for _ in range(3):
+            ctx.epoch(0.01)
+        after = ctx.nzsl(P.TEST)
+        W, H = ctx.get_factors()
+        assert np.isfinite(W).all() and np.isfinite(H).all()
+        assert after < before
+    with pytest.raises(P.DsgdppError):
+        with P.Context(cfg) as ctx:
+            ctx.set_wait_limit(-1.0)
+
+
 def test_small_cpu_workload_replay_run_matches_oracle():
     # the reference's CPU-runnable case at full size: 100,000 x 100,000, 1M
     # uniform entries (+100k test), rank 10, FP64, Nzsl_L2(1), d = 4 (4 x 8

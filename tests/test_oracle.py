@@ -183,6 +183,43 @@ def test_blocking_sorted_and_duplicates_summed():
     assert a.tolist() == [2, 0, 0, 1, 0, 1] and mx == 2
 
 
+def test_blocking_of_a_large_matrix_on_all_threads_matches_numpy():
+    # above 2^20 entries the oracle routes and sorts blocks on all host threads;
+    # each block must still hold its entries in (i, j) order with duplicates
+    # summed in input order (mf/matrix/io/read_impl.h:162-164, 421)
+    rng = np.random.default_rng(4)
+    m, n, d, k = 5000, 3000, 4, 1_200_000
+    rows = rng.integers(0, m, k).astype(np.uint32)
+    cols = rng.integers(0, n, k).astype(np.uint32)
+    vals = rng.standard_normal(k)
+    ref = O.Problem(m, n, 2, d, rows, cols, vals)
+    off1, off2 = O.block_offsets(m, d), O.block_offsets(n, 2 * d)
+    key = rows.astype(np.int64) * n + cols
+    order = np.argsort(key, kind="stable")
+    skey = key[order]
+    first = np.flatnonzero(np.r_[True, skey[1:] != skey[:-1]])
+    ukey = skey[first]
+    sv = vals[order]
+    usum = sv[first].copy()
+    ends = np.r_[first[1:], k]
+    for g in np.flatnonzero(ends - first > 1):  # duplicates: summed one after another
+        for q in range(first[g] + 1, ends[g]):
+            usum[g] += sv[q]
+    ur, uc = ukey // n, ukey % n
+    b1 = np.searchsorted(off1, ur, side="right") - 1
+    b2 = np.searchsorted(off2, uc, side="right") - 1
+    total = 0
+    for a in range(d):
+        for b in range(2 * d):
+            sel = (b1 == a) & (b2 == b)
+            i, j, x = ref.block_records(a, b)
+            np.testing.assert_array_equal(i, ur[sel] - off1[a])
+            np.testing.assert_array_equal(j, uc[sel] - off2[b])
+            np.testing.assert_array_equal(x, usum[sel])
+            total += len(x)
+    assert total == len(ukey) < k
+
+
 def test_losses_against_numpy():
     p = _tiny(nnz=120, r=4)
     ref = O.Problem(p.m, p.n, 4, 2, p.rows, p.cols, p.vals)

@@ -81,5 +81,10 @@ def test_noalloc_rejects_requests_beyond_capacity():
     assert P.lib.dsgdpp_nzsl_fp32_noalloc(idx.data_ptr(), idx.data_ptr(), v.data_ptr(), 1,
                                           W.data_ptr(), W.data_ptr(), 3, 3, 0, out.data_ptr(),
                                           None) == P.E_INVALID
+    # a row wider than the widest loss kernel (512 floats) is refused, not failed
+    wide = torch.zeros((2, 516), dtype=torch.float32, device="cuda")
+    assert P.lib.dsgdpp_nzsl_fp32_noalloc(idx.data_ptr(), idx.data_ptr(), v.data_ptr(), 1,
+                                          wide.data_ptr(), wide.data_ptr(), 516, 516, 0,
+                                          out.data_ptr(), None) == P.E_INVALID
     assert P.lib.dsgdpp_nzsl_fp32_noalloc(*args, 1, out.data_ptr(), None) == P.OK
     torch.cuda.synchronize()
