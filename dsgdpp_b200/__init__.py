@@ -209,6 +209,22 @@ SIGNATURES = {
     "dsgdpp_h_block_copy": (C.c_int, [_P, C.c_uint32, _P, C.c_int]),
     "dsgdpp_set_counts": (C.c_int, [_P, _u64p, _u64p]),
     "dsgdpp_set_wait_limit": (C.c_int, [_P, C.c_double]),
+    "dsgdpp_set_tasks": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
+    "dsgdpp_shard_unique_id": (C.c_int, [_P]),
+    "dsgdpp_shard_create_nccl": (C.c_int, [_P, C.c_int, C.c_int, _P, C.POINTER(_P)]),
+    "dsgdpp_shard_create_local": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
+    "dsgdpp_shard_destroy": (None, [_P]),
+    "dsgdpp_shard_last_error": (C.c_char_p, [_P]),
+    "dsgdpp_shard_set_wait_limit": (C.c_int, [_P, C.c_double]),
+    "dsgdpp_shard_epoch": (C.c_int, [_P, C.c_double, _u32p, _u32p]),
+    "dsgdpp_shard_share": (C.c_int, [_P]),
+    "dsgdpp_shard_gather_w": (C.c_int, [_P]),
+    "dsgdpp_shard_losses": (C.c_int, [_P, _f64p, _f64p]),
+    "dsgdpp_shard_moved": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "dsgdpp_shard_set_timeline": (C.c_int, [_P, C.c_int]),
+    "dsgdpp_shard_timeline": (C.c_int, [_P, C.c_uint32, _f64p, _f64p]),
+    "dsgdpp_shard_plan": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_int, _u32p,
+                                       C.POINTER(C.c_int32), _u32p]),
     "dsgdpp_set_factors_rm": (C.c_int, [_P, _P]),
 }
 
@@ -413,6 +429,10 @@ class Context:
         self._check(lib.dsgdpp_epoch_part(self._h, eps, _ptr(s, C.c_uint32), _ptr(t, C.c_uint32),
                                           s_begin, s_end), "epoch_part")
 
+    def set_tasks(self, first: int, count: int):
+        """Run tasks first .. first+count-1 only (one rank's share of the job)."""
+        self._check(lib.dsgdpp_set_tasks(self._h, first, count), "set_tasks")
+
     def h_block_bytes(self, b2: int) -> int:
         out = C.c_uint64()
         self._check(lib.dsgdpp_h_block_bytes(self._h, b2, C.byref(out)), "h_block_bytes")
@@ -502,6 +522,122 @@ class Context:
         return [dict(epoch=r.epoch, loss=r.loss, test_loss=r.test_loss, eps=r.eps,
                      time_eps=r.time_eps, time_epoch=r.time_epoch, time_loss=r.time_loss,
                      time_test_loss=r.time_test_loss) for r in rows]
+
+
+SHARD_ID_BYTES = 128
+
+
+def shard_unique_id() -> bytes:
+    """A new NCCL unique id for :meth:`Shard.nccl` (made on rank 0)."""
+    buf = C.create_string_buffer(SHARD_ID_BYTES)
+    rc = lib.dsgdpp_shard_unique_id(C.cast(buf, C.c_void_p))
+    if rc != OK:
+        raise DsgdppError(rc, "shard_unique_id: NCCL is not available")
+    return buf.raw
+
+
+def shard_plan(d: int, nb2: int, world: int, schedule, holder):
+    """The hand-off plan of one epoch (no GPU): an array of (group, block,
+    from rank, to rank) rows (group 0 = before the epoch, s + 1 = after
+    sub-epoch s) and the block holders after it (-1 = every rank)."""
+    sch = _u32(schedule)
+    h = np.ascontiguousarray(holder, np.int32).copy()
+    hp = h.ctypes.data_as(C.POINTER(C.c_int32))
+    n = lib.dsgdpp_shard_plan(d, nb2, world, _ptr(sch, C.c_uint32), hp, None)
+    out = np.zeros((n, 4), np.uint32)
+    h = np.ascontiguousarray(holder, np.int32).copy()
+    hp = h.ctypes.data_as(C.POINTER(C.c_int32))
+    lib.dsgdpp_shard_plan(d, nb2, world, _ptr(sch, C.c_uint32), hp, _ptr(out, C.c_uint32))
+    return out, h
+
+
+class Shard:
+    """One DSGD++ job over several ranks (the hand-off of DsgdPpTask::run,
+    mf/sgd/dsgdpp_impl.h:141-263): :meth:`nccl` for one rank per GPU and
+    process, :meth:`local` for emulated ranks (contexts of this process)."""
+
+    def __init__(self, handle, keep):
+        self._h = handle
+        self._keep = keep
+
+    @classmethod
+    def nccl(cls, ctx: "Context", rank: int, world: int, unique_id: bytes) -> "Shard":
+        h = _P()
+        buf = C.create_string_buffer(bytes(unique_id), SHARD_ID_BYTES)
+        rc = lib.dsgdpp_shard_create_nccl(ctx._h, rank, world, C.cast(buf, C.c_void_p),
+                                          C.byref(h))
+        if rc != OK:
+            raise DsgdppError(rc, "shard_create_nccl: " + lib.dsgdpp_last_error(ctx._h).decode())
+        return cls(h, [ctx])
+
+    @classmethod
+    def local(cls, ctxs) -> "Shard":
+        arr = (_P * len(ctxs))(*[c._h for c in ctxs])
+        h = _P()
+        rc = lib.dsgdpp_shard_create_local(arr, len(ctxs), C.byref(h))
+        if rc != OK:
+            raise DsgdppError(rc, "shard_create_local: " +
+                              lib.dsgdpp_last_error(ctxs[0]._h).decode())
+        return cls(h, list(ctxs))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.dsgdpp_shard_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise DsgdppError(rc, f"{what}: {lib.dsgdpp_shard_last_error(self._h).decode()}")
+
+    def set_wait_limit(self, seconds: float):
+        self._check(lib.dsgdpp_shard_set_wait_limit(self._h, float(seconds)), "set_wait_limit")
+
+    def epoch(self, eps: float, schedule=None, task_seeds=None):
+        """One epoch on every rank: the given draws, or the master generator's."""
+        if schedule is None:
+            self._check(lib.dsgdpp_shard_epoch(self._h, eps, None, None), "shard_epoch")
+            return
+        s, t = _u32(schedule), _u32(task_seeds)
+        self._check(lib.dsgdpp_shard_epoch(self._h, eps, _ptr(s, C.c_uint32),
+                                           _ptr(t, C.c_uint32)), "shard_epoch")
+
+    def share(self):
+        self._check(lib.dsgdpp_shard_share(self._h), "shard_share")
+
+    def gather_w(self):
+        """Every rank's W rows to every rank (to read the result; ends the job)."""
+        self._check(lib.dsgdpp_shard_gather_w(self._h), "shard_gather_w")
+
+    def losses(self):
+        """(training loss, test loss) of the whole job, after :meth:`share`."""
+        a, b = C.c_double(), C.c_double()
+        self._check(lib.dsgdpp_shard_losses(self._h, C.byref(a), C.byref(b)), "shard_losses")
+        return a.value, b.value
+
+    def moved(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(lib.dsgdpp_shard_moved(self._h, C.byref(a), C.byref(b)), "shard_moved")
+        return a.value, b.value
+
+    def set_timeline(self, on: bool):
+        self._check(lib.dsgdpp_shard_set_timeline(self._h, int(on)), "set_timeline")
+
+    def timeline(self, index: int, nb2: int):
+        """([nb2, 2] compute, [nb2, 2] transfer) begin/end in ms of the last epoch."""
+        comp = np.zeros((nb2, 2))
+        xfer = np.zeros((nb2, 2))
+        self._check(lib.dsgdpp_shard_timeline(self._h, index, _ptr(comp, C.c_double),
+                                              _ptr(xfer, C.c_double)), "shard_timeline")
+        return comp, xfer
 
 
 def _problem_array(problems):

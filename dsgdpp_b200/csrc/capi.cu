@@ -22,6 +22,19 @@
 
 using namespace dsgdpp;
 
+// The master generator's draws of one epoch: DsgdPpRunner::epoch
+// (mf/sgd/dsgdpp_impl.h:289-344) or DsgdRunner::epoch (mf/sgd/dsgd_impl.h:
+// 328-350: the d x d schedule of computeDsgdSchedule, then one seed per task).
+void dsgdpp::draw_epoch(dsgdpp_ctx* c, uint32_t* sched, uint32_t* seeds) {
+  if (c->cfg.method == DSGDPP_METHOD_DSGD) {
+    const std::vector<uint32_t> S = dsgd_schedule(1, c->d, c->cfg.stratum_order, c->master);
+    std::copy(S.begin(), S.end(), sched);
+    for (uint32_t id = 0; id < c->d; ++id) seeds[id] = c->master.next();
+  } else {
+    dsgdpp_schedule(c->master, c->d, c->cfg.stratum_order, sched, seeds);
+  }
+}
+
 
 namespace {
 
@@ -51,19 +64,6 @@ int resolve_layout(int layout, uint64_t m, uint64_t n) {
     case DSGDPP_LAYOUT_ROW_RUNS: return kLayoutRowRuns;
     case DSGDPP_LAYOUT_RUNS: return n <= m ? kLayoutColRuns : kLayoutRowRuns;
     default: return kLayoutShuffled;
-  }
-}
-
-// The master generator's draws of one epoch: DsgdPpRunner::epoch
-// (mf/sgd/dsgdpp_impl.h:289-344) or DsgdRunner::epoch (mf/sgd/dsgd_impl.h:
-// 328-350: the d x d schedule of computeDsgdSchedule, then one seed per task).
-void draw_epoch(dsgdpp_ctx* c, uint32_t* sched, uint32_t* seeds) {
-  if (c->cfg.method == DSGDPP_METHOD_DSGD) {
-    const std::vector<uint32_t> S = dsgd_schedule(1, c->d, c->cfg.stratum_order, c->master);
-    std::copy(S.begin(), S.end(), sched);
-    for (uint32_t id = 0; id < c->d; ++id) seeds[id] = c->master.next();
-  } else {
-    dsgdpp_schedule(c->master, c->d, c->cfg.stratum_order, sched, seeds);
   }
 }
 
@@ -143,6 +143,8 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
              "cudaDeviceGetAttribute");
   c->d = cfg->d;
   c->nb2 = cfg->method == DSGDPP_METHOD_DSGD ? cfg->d : 2 * cfg->d;
+  c->task_lo = 0;
+  c->task_hi = cfg->d;
   c->r = cfg->rank;
   const uint32_t vw = vec_width(cfg->precision);
   c->rp = (c->r + vw - 1) / vw * vw;
@@ -714,10 +716,11 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds, uint32_t
   } else {
     for (unsigned t = 0; t < hw; ++t) work(t);
   }
-  if (l2) {
+  if (l2) {  // the H blocks each sub-epoch's tasks (those run here) regularize
     std::memset(c->h_mask, 0, (size_t)d2 * d2);
     for (uint32_t s = 0; s < d2; ++s)
-      for (uint32_t id = 0; id < d; ++id) c->h_mask[(size_t)s * d2 + c->h_schedule[(size_t)s * d + id]] = 1;
+      for (uint32_t id = c->task_lo; id < c->task_hi; ++id)
+        c->h_mask[(size_t)s * d2 + c->h_schedule[(size_t)s * d + id]] = 1;
   }
   check_cuda(cudaEventRecord(c->ev_begin, st), "event");
   check_cuda(cudaMemcpyAsync(c->d_schedule, c->h_schedule, (size_t)d2 * d * 4,
@@ -744,8 +747,11 @@ void run_replay_epoch(dsgdpp_ctx* c, double eps, const uint32_t* seeds, uint32_t
   a.lambda = c->cfg.update_lambda; a.tmin = c->cfg.truncate_min; a.tmax = c->cfg.truncate_max;
   for (uint32_t s = s0; s < s1; ++s) {
     check_cuda(launch_replay_subepoch(a, s, st), "replay_subepoch");
+    // the W row blocks of the tasks run here
+    double* w0 = a.W + c->off1[c->task_lo] * c->rp;
+    const uint64_t wrows = c->off1[c->task_hi] - c->off1[c->task_lo];
     if (l2 && c->cfg.regularize_lambda != 0)
-      check_cuda(launch_regularize_exact(a.W, a.H, c->cfg.m, c->cfg.n, c->rp, c->r, c->d_off2,
+      check_cuda(launch_regularize_exact(w0, a.H, wrows, c->cfg.n, c->rp, c->r, c->d_off2,
                                          c->d_mask + (size_t)s * d2, d, d2, c->d_params,
                                          c->cfg.regularize_lambda, c->cfg.truncate,
                                          c->cfg.truncate_min, c->cfg.truncate_max, st),
@@ -779,6 +785,18 @@ void epoch_part_impl(dsgdpp_ctx* c, double eps, const uint32_t* schedule, const 
              std::memcmp(schedule, c->h_schedule, (size_t)d2 * d * 4) != 0 ||
              std::memcmp(seeds, c->part_seeds.data(), (size_t)d * 4) != 0) {
     throw Error(DSGDPP_E_INVALID, "a later part of an epoch must repeat its step size, schedule and seeds");
+  }
+  if (s0 == 0 && (c->task_lo != 0 || c->task_hi != d)) {
+    for (int which = 0; which < 2; ++which) {
+      const DevMatrix& M = c->mat[which];
+      if (!M.present) continue;
+      for (uint32_t b1 = 0; b1 < d; ++b1)
+        if ((b1 < c->task_lo || b1 >= c->task_hi) &&
+            M.h_block_ptr[(size_t)(b1 + 1) * d2] != M.h_block_ptr[(size_t)b1 * d2])
+          throw Error(DSGDPP_E_STATE, std::string(which ? "test" : "training") +
+                                          " entries in row block " + std::to_string(b1) +
+                                          ", whose task does not run here (dsgdpp_set_tasks)");
+    }
   }
   check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
   if (s0 == 0) {
@@ -1151,6 +1169,17 @@ int dsgdpp_epoch_part(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
                       const uint32_t* task_seeds, uint32_t s_begin, uint32_t s_end) {
   return guarded(c, [&]() {
     epoch_part_impl(c, eps, schedule, task_seeds, s_begin, s_end);
+    return DSGDPP_OK;
+  });
+}
+
+int dsgdpp_set_tasks(dsgdpp_ctx* c, uint32_t first, uint32_t count) {
+  return guarded(c, [&]() {
+    if (count == 0 || first >= c->d || count > c->d - first)
+      throw Error(DSGDPP_E_INVALID, "task range out of bounds");
+    if (c->part_next != 0) throw Error(DSGDPP_E_STATE, "an epoch given in parts is unfinished");
+    c->task_lo = first;
+    c->task_hi = first + count;
     return DSGDPP_OK;
   });
 }

@@ -150,5 +150,12 @@ struct dsgdpp_ctx {
   bool prof_pending = false;
   Random32 master{0};
   uint32_t epoch_counter = 0;
+  // tasks [task_lo, task_hi) run here (dsgdpp_set_tasks; all d by default)
+  uint32_t task_lo = 0, task_hi = 0;
 };
+
+namespace dsgdpp {
+// The master generator's draws of one epoch (schedule [nb2][d], d task seeds).
+void draw_epoch(dsgdpp_ctx* c, uint32_t* sched, uint32_t* seeds);
+}  // namespace dsgdpp
 

@@ -20,6 +20,15 @@
 // stay in device memory either way, so it changes no result).
 // Extension: --regularize L2(l) is accepted (the reference rejects every
 // regularizer other than None, tools/mfdsgdpp.cc:165-258).
+// Several ranks: started by a launcher that sets WORLD_SIZE, RANK and
+// LOCAL_RANK (torchrun, for one), one process per GPU, the tool runs one job
+// over the ranks as the reference does over MPI ranks: d = ranks x
+// --tasks-per-rank (tools/mfdsgdpp.cc:41-42,76-77), rank r runs tasks
+// r t .. (r+1) t - 1 on GPU LOCAL_RANK (unless --device is given) and the H
+// blocks move between the ranks over NCCL (dsgdpp_shard_*).  Rank 0 makes the
+// NCCL id and hands it over through --shard-id-file (default
+// /tmp/dsgdpp-shard-<MASTER_PORT>.id); rank 0 logs and writes the outputs.
+// Given --shard-id-file, a single process runs the same path (one rank).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -30,6 +39,7 @@
 #include <memory>
 #include <regex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dsgdpp.h"
@@ -57,7 +67,11 @@ struct Args {
   int sgdOrder = DSGDPP_SGD_WOR, stratumOrder = DSGDPP_STRATUM_COWOR;
   // added options
   int device = 0;
+  bool deviceGiven = false;
   std::string precision = "fp32", exec = "hogwild", launch = "graph", layout = "runs";
+  // several ranks (WORLD_SIZE > 1)
+  int world = 1, worldRank = 0, localRank = 0;
+  std::string shardIdFile;
 };
 
 bool g_dsgd = false;  // running as mfdsgd
@@ -67,7 +81,7 @@ const char* kOptions[] = {
     "output-row-file", "output-col-file", "trace", "trace-var", "epochs", "tasks-per-rank",
     "sgd-order", "stratum-order", "seed", "rank", "update", "regularize", "loss", "abs",
     "truncate", "decay", "balance", "device", "precision", "exec", "launch", "layout",
-    "map-reduce"};
+    "map-reduce", "shard-id-file"};
 
 void usage() {
   std::cout << (g_dsgd ? "mfdsgd" : "mfsgdpp") << " [options]\n\nOptions:\n"
@@ -103,7 +117,9 @@ void usage() {
             << "  --exec arg             hogwild|replay [hogwild]\n"
             << "  --launch arg           graph|stream [graph]\n"
             << "  --layout arg           Hogwild record order in a block:\n"
-            << "                         shuffled|col-runs|row-runs|runs [runs]\n";
+            << "                         shuffled|col-runs|row-runs|runs [runs]\n"
+            << "  --shard-id-file arg    several ranks: file through which rank 0 hands the\n"
+            << "                         NCCL id to the others [/tmp/dsgdpp-shard-<MASTER_PORT>.id]\n";
 }
 
 // parse::parseArg (tools/parse.h:38-61): "Name(a,b,...)" -> name + doubles
@@ -285,8 +301,40 @@ std::string blocks_list(uint64_t b1, uint64_t b2) {
   return s;
 }
 
+// Rank 0 makes the NCCL id and publishes it in `path` (written under another
+// name, then renamed); the other ranks wait for the file, at most `limit_s`.
+std::vector<char> exchange_shard_id(const Args& args, double limit_s = 300) {
+  std::vector<char> id(DSGDPP_SHARD_ID_BYTES);
+  const std::string& path = args.shardIdFile;
+  if (args.worldRank == 0) {
+    const int rc = dsgdpp_shard_unique_id(id.data());
+    if (rc != DSGDPP_OK) throw CallError(rc, "dsgdpp_shard_unique_id: NCCL is not available");
+    const std::string tmp = path + ".tmp";
+    {
+      std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+      f.write(id.data(), (std::streamsize)id.size());
+      if (!f) throw std::runtime_error("cannot write " + tmp);
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0)
+      throw std::runtime_error("cannot rename " + tmp + " to " + path);
+    return id;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    std::ifstream f(path, std::ios::binary);
+    if (f && f.read(id.data(), (std::streamsize)id.size()) && f.gcount() == (std::streamsize)id.size())
+      return id;
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit_s)
+      throw std::runtime_error("no NCCL id from rank 0 in " + path + " within " +
+                               std::to_string((int)limit_s) + " s");
+    std::this_thread::sleep_for(std::chrono::milliseconds(20));
+  }
+}
+
 int run(Args& args, const Job& job) {
-  const uint32_t d = (uint32_t)args.tasksPerRank;
+  // d = ranks x tasks per rank (tools/mfdsgdpp.cc:41-42,76-77)
+  const uint32_t d = (uint32_t)(args.tasksPerRank * args.world);
+  const bool sharded = args.world > 1 || !args.shardIdFile.empty();
   const uint32_t nb2 = g_dsgd ? d : 2 * d;  // column blocks: d x d (DSGD) or d x 2d (DSGD++)
   if (args.decayName != "BoldDriver" && args.decayName != "Const") {
     std::cerr << "not implemented: decay" << std::endl;  // rg::NotImplementedException
@@ -419,6 +467,8 @@ int run(Args& args, const Job& job) {
   cfg.sgd_order = args.sgdOrder;
   cfg.stratum_order = args.stratumOrder;
   cfg.device = args.device;
+  if (sharded && cfg.launch == DSGDPP_LAUNCH_GRAPH)
+    cfg.launch = DSGDPP_LAUNCH_STREAM;  // a sharded epoch runs one sub-epoch at a time
   dsgdpp_ctx* ctx = nullptr;
   int rc = dsgdpp_create(&cfg, &ctx);
   if (rc != DSGDPP_OK) throw CallError(rc, std::string("dsgdpp_create: ") + dsgdpp_create_error());
@@ -426,7 +476,63 @@ int run(Args& args, const Job& job) {
     dsgdpp_ctx* c;
     ~Guard() { dsgdpp_destroy(c); }
   } guard{ctx};
-  if (rmV) {
+  if (sharded) {
+    // this rank's tasks' rows of V and of the test matrix; the update weights
+    // count the whole matrix; W is zero outside this rank's rows
+    if (rmV) {
+      for (int which : {DSGDPP_TRAIN, DSGDPP_TEST}) {
+        if (which == DSGDPP_TEST && !has_test) continue;
+        Coo& M = which == DSGDPP_TRAIN ? V : T;
+        const uint64_t cnt = info_v[which == DSGDPP_TRAIN ? 7 : 8];
+        M.size1 = m;
+        M.size2 = n;
+        M.rows.resize(cnt);
+        M.cols.resize(cnt);
+        M.vals.resize(cnt);
+        check(ctx, dsgdpp_rm_generate(rmV.get(), which, cfg.device, M.rows.data(),
+                                      M.cols.data(), M.vals.data()), "rm_generate");
+      }
+    }
+    if (rmF) {
+      W.resize(m * r);
+      H.resize(n * r);
+      check(ctx, dsgdpp_rm_generate_factors(rmF.get(), cfg.device, W.data(), H.data()),
+            "rm_generate_factors");
+    }
+    std::vector<uint64_t> off1(d + 1);
+    dsgdpp_block_offsets(m, d, off1.data());
+    off1[d] = m;
+    const uint32_t t = (uint32_t)args.tasksPerRank, first = (uint32_t)args.worldRank * t;
+    const uint64_t lo = off1[first], hi = off1[first + t];
+    std::vector<uint64_t> n1(m, 0), n2(n, 0);
+    for (size_t k = 0; k < V.vals.size(); ++k) {
+      n1[V.rows[k]]++;
+      n2[V.cols[k]]++;
+    }
+    auto own = [&](const Coo& M) {
+      Coo o;
+      for (size_t k = 0; k < M.vals.size(); ++k)
+        if (M.rows[k] >= lo && M.rows[k] < hi) {
+          o.rows.push_back(M.rows[k]);
+          o.cols.push_back(M.cols[k]);
+          o.vals.push_back(M.vals[k]);
+        }
+      return o;
+    };
+    check(ctx, dsgdpp_set_tasks(ctx, first, t), "set_tasks");
+    const Coo Vr = own(V);
+    check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TRAIN, Vr.vals.size(), Vr.rows.data(),
+                                 Vr.cols.data(), Vr.vals.data()), "set_matrix");
+    if (has_test) {
+      const Coo Tr = own(T);
+      check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TEST, Tr.vals.size(), Tr.rows.data(),
+                                   Tr.cols.data(), Tr.vals.data()), "set_matrix");
+    }
+    check(ctx, dsgdpp_set_counts(ctx, n1.data(), n2.data()), "set_counts");
+    std::vector<double> Wr(m * r, 0.0);
+    std::copy(W.begin() + lo * r, W.begin() + hi * r, Wr.begin() + lo * r);
+    check(ctx, dsgdpp_set_factors(ctx, Wr.data(), H.data()), "set_factors");
+  } else if (rmV) {
     check(ctx, dsgdpp_set_matrix_rm(ctx, DSGDPP_TRAIN, rmV.get()), "set_matrix_rm");
     if (has_test) check(ctx, dsgdpp_set_matrix_rm(ctx, DSGDPP_TEST, rmV.get()), "set_matrix_rm");
   } else {
@@ -436,11 +542,22 @@ int run(Args& args, const Job& job) {
       check(ctx, dsgdpp_set_matrix(ctx, DSGDPP_TEST, T.vals.size(), T.rows.data(),
                                    T.cols.data(), T.vals.data()), "set_matrix");
   }
-  if (rmF)
+  if (sharded) {
+  } else if (rmF) {
     check(ctx, dsgdpp_set_factors_rm(ctx, rmF.get()), "set_factors_rm");
-  else
+  } else {
     check(ctx, dsgdpp_set_factors(ctx, W.data(), H.data()), "set_factors");
+  }
   check(ctx, dsgdpp_seed(ctx, args.seed), "seed");
+  std::unique_ptr<dsgdpp_shard, void (*)(dsgdpp_shard*)> shard(nullptr, dsgdpp_shard_destroy);
+  if (sharded) {
+    const std::vector<char> id = exchange_shard_id(args);
+    dsgdpp_shard* sh = nullptr;
+    check(ctx, dsgdpp_shard_create_nccl(ctx, args.worldRank, args.world, id.data(), &sh),
+          "dsgdpp_shard_create_nccl");
+    shard.reset(sh);
+    if (args.worldRank == 0) std::remove(args.shardIdFile.c_str());  // every rank has joined
+  }
 
   Trace trace;  // Args::createTraceFields (tools/detail/mfdsgd-args.h:53-63)
   trace.add_field("update", args.updateString);
@@ -448,7 +565,7 @@ int run(Args& args, const Job& job) {
   trace.add_field("rank", (double)args.rank);
   trace.add_field("input_file", args.inputMatrixFile);
   trace.add_field("sample_matrix", "");
-  trace.add_field("nodes", 1.0);
+  trace.add_field("nodes", (double)args.world);
   trace.add_field("threads", (double)args.tasksPerRank);
   trace.add_field("barrier", "false");
 
@@ -461,7 +578,9 @@ int run(Args& args, const Job& job) {
   }
   if (has_test) Log::info("main", "Using NzslLoss for test data");
   Log::info("mf", std::string(g_dsgd ? "Starting DSGD" : "Starting DSGD++") + " on " +
-                      std::string(args.exec) + " " + args.precision + " (B200, one GPU)");
+                      std::string(args.exec) + " " + args.precision +
+                      (sharded ? " (B200, " + std::to_string(args.world) + " ranks, one GPU each)"
+                               : std::string(" (B200, one GPU)")));
   if (g_dsgd)  // mf/sgd/dsgd_impl.h:56-60
     Log::info("mf", args.mapReduce ? "Using slow MapReduce-style implementation"
                                    : "Using fast DSGD+ implementation");
@@ -471,12 +590,19 @@ int run(Args& args, const Job& job) {
   Log::info("mf", std::string("Using ") + kPoints[args.sgdOrder] +
                       " order for selecting training points");
   auto r0 = std::chrono::steady_clock::now();
-  default_runner(ctx, args.epochs, decay, trace, has_test);
+  if (shard)
+    shard_runner(shard.get(), args.epochs, decay, trace, has_test);
+  else
+    default_runner(ctx, args.epochs, decay, trace, has_test);
   auto r1 = std::chrono::steady_clock::now();
   Log::info("mf", g_dsgd ? "Finished DSGD" : "Finished DSGD++");
   Log::info("main", "Total time: " +
                         fmt_secs((double)std::chrono::duration_cast<std::chrono::nanoseconds>(r1 - r0).count()));
 
+  const bool writer = args.worldRank == 0;  // rank 0 writes the outputs
+  if (shard && (!args.outputRowFacFile.empty() || !args.outputColFacFile.empty()))
+    check_shard(shard.get(), dsgdpp_shard_gather_w(shard.get()), "shard gather W");
+  if (!writer) return 0;
   if (!args.traceFile.empty()) {
     Log::info("main", "Writing trace to " + args.traceFile);
     std::ofstream f(args.traceFile);
@@ -575,7 +701,15 @@ int main(int argc, char** argv) {
     args.epochs = vm.count("epochs") ? std::stoull(vm["epochs"]) : 10;
     args.tasksPerRank = vm.count("tasks-per-rank") ? std::stoi(vm["tasks-per-rank"]) : 1;
     args.rank = std::stoull(vm["rank"]);
-    args.device = vm.count("device") ? std::stoi(vm["device"]) : 0;
+    args.deviceGiven = vm.count("device") > 0;
+    args.device = args.deviceGiven ? std::stoi(vm["device"]) : 0;
+    auto env_int = [](const char* k, int dflt) {
+      const char* v = std::getenv(k);
+      return v && *v ? std::stoi(v) : dflt;
+    };
+    args.world = env_int("WORLD_SIZE", 1);
+    args.worldRank = env_int("RANK", 0);
+    args.localRank = env_int("LOCAL_RANK", 0);
   } catch (const std::exception&) {
     std::cerr << "invalid numeric option value" << std::endl;
     return 1;
@@ -587,6 +721,17 @@ int main(int argc, char** argv) {
   args.lossString = vm["loss"];
   args.decayString = vm["decay"];
   args.balanceString = get("balance", "None");
+  if (args.world < 1 || args.worldRank < 0 || args.worldRank >= args.world) {
+    std::cerr << "invalid WORLD_SIZE / RANK" << std::endl;
+    return 1;
+  }
+  if (args.world > 1 || vm.count("shard-id-file")) {
+    if (!args.deviceGiven) args.device = args.localRank;
+    const char* port = std::getenv("MASTER_PORT");
+    args.shardIdFile = get("shard-id-file", std::string("/tmp/dsgdpp-shard-") +
+                                                (port && *port ? port : "0") + ".id");
+    Log::quiet() = args.worldRank != 0;
+  }
   args.precision = get("precision", "fp32");
   args.exec = get("exec", "hogwild");
   args.launch = get("launch", "graph");
@@ -611,7 +756,7 @@ int main(int argc, char** argv) {
   Log::info("main", args.traceFile.empty() ? std::string("    Trace: Disabled")
                                            : "    Trace: " + args.traceFile + " (" + args.traceVar + ")");
   Log::info("main", "Parallelization");
-  Log::info("main", "    MPI ranks: 1");
+  Log::info("main", "    MPI ranks: " + std::to_string(args.world));
   Log::info("main", "    Tasks per rank: " + std::to_string(args.tasksPerRank));
   Log::info("main", g_dsgd ? "DSGD options" : "DSGD++ options");
   Log::info("main", "    Seed: " + std::to_string(args.seed));

@@ -28,8 +28,13 @@ namespace dsgdpp {
 // log4cxx-like lines: "<ms since start> <logger> | <message>"
 class Log {
  public:
+  static bool& quiet() {  // ranks other than 0 of a job over several ranks stay quiet
+    static bool q = false;
+    return q;
+  }
   static void info(const char* logger, const std::string& msg) {
     static const auto t0 = std::chrono::steady_clock::now();
+    if (quiet()) return;
     long long ms = std::chrono::duration_cast<std::chrono::milliseconds>(
                        std::chrono::steady_clock::now() - t0).count();
     std::printf("%8lld %-4s | %s\n", ms, logger, msg.c_str());
@@ -125,16 +130,23 @@ inline void check(dsgdpp_ctx* ctx, int rc, const char* what) {
                             dsgdpp_status_string(rc) + ")");
 }
 
+// What the runner drives: one context, or one job over several ranks.
+struct RunOps {
+  std::function<void(double)> epoch;  // one epoch at this step size, finished on return
+  std::function<double()> loss;       // the training loss
+  std::function<double()> test_loss;  // the test loss (after loss())
+};
+
 // detail::defaultRunner over the C ABI.
-inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace& trace,
-                           bool has_test) {
+inline void run_epochs(const RunOps& ops, uint64_t epochs, Decay decay, Trace& trace,
+                       bool has_test) {
   using clock = std::chrono::steady_clock;
   auto ns = [](clock::time_point a, clock::time_point b) {
     return (double)std::chrono::duration_cast<std::chrono::nanoseconds>(b - a).count();
   };
   double previous = 0, current = 0, test = NAN;
   auto t0 = clock::now();
-  check(ctx, dsgdpp_loss(ctx, &current), "loss");
+  current = ops.loss();
   auto t1 = clock::now();
   trace.clear();
   Log::info("mf", "Loss: " + fmt_g(current) + " (" + fmt_secs(ns(t0, t1)) + ")");
@@ -143,7 +155,7 @@ inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace&
   first.time_loss = ns(t0, t1);
   if (has_test) {
     auto a = clock::now();
-    check(ctx, dsgdpp_nzsl(ctx, DSGDPP_TEST, &test), "test loss");
+    test = ops.test_loss();
     auto b = clock::now();
     Log::info("mf", "Test loss: " + fmt_g(test) + " (" + fmt_secs(ns(a, b)) + ")");
     first.test_loss = test;
@@ -157,13 +169,12 @@ inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace&
     Log::info("mf", "Step size: " + fmt_g(eps) + " (" + fmt_secs(ns(a, b)) + ")");
     Log::info("mf", "Starting epoch " + std::to_string(e + 1));
     auto c = clock::now();
-    check(ctx, dsgdpp_epoch(ctx, eps), "epoch");
-    check(ctx, dsgdpp_sync(ctx), "sync");
+    ops.epoch(eps);
     auto dd = clock::now();
     Log::info("mf", "Finished epoch " + std::to_string(e + 1) + " (" + fmt_secs(ns(c, dd)) + ")");
     previous = current;
     auto f = clock::now();
-    check(ctx, dsgdpp_loss(ctx, &current), "loss");
+    current = ops.loss();
     auto g = clock::now();
     Log::info("mf", "Loss: " + fmt_g(current) + " (" + fmt_secs(ns(f, g)) + ")");
     TraceRow row;
@@ -175,7 +186,7 @@ inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace&
     row.time_loss = ns(f, g);
     if (has_test) {
       auto h = clock::now();
-      check(ctx, dsgdpp_nzsl(ctx, DSGDPP_TEST, &test), "test loss");
+      test = ops.test_loss();
       auto k = clock::now();
       Log::info("mf", "Test loss: " + fmt_g(test) + " (" + fmt_secs(ns(h, k)) + ")");
       row.test_loss = test;
@@ -183,6 +194,52 @@ inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace&
     }
     trace.add(row);
   }
+}
+
+inline void default_runner(dsgdpp_ctx* ctx, uint64_t epochs, Decay decay, Trace& trace,
+                           bool has_test) {
+  RunOps ops;
+  ops.epoch = [ctx](double eps) {
+    check(ctx, dsgdpp_epoch(ctx, eps), "epoch");
+    check(ctx, dsgdpp_sync(ctx), "sync");
+  };
+  ops.loss = [ctx]() {
+    double v = 0;
+    check(ctx, dsgdpp_loss(ctx, &v), "loss");
+    return v;
+  };
+  ops.test_loss = [ctx]() {
+    double v = 0;
+    check(ctx, dsgdpp_nzsl(ctx, DSGDPP_TEST, &v), "test loss");
+    return v;
+  };
+  run_epochs(ops, epochs, decay, trace, has_test);
+}
+
+inline void check_shard(dsgdpp_shard* sh, int rc, const char* what) {
+  if (rc != DSGDPP_OK)
+    throw CallError(rc, std::string(what) + ": " + dsgdpp_shard_last_error(sh) + " (" +
+                            dsgdpp_status_string(rc) + ")");
+}
+
+// The same loop over a job on several ranks: an epoch is the shard's epoch
+// (schedule drawn by every rank's master generator, seeded alike) followed by
+// the broadcast of every H block from its holder; the losses are the job's.
+inline void shard_runner(dsgdpp_shard* sh, uint64_t epochs, Decay decay, Trace& trace,
+                         bool has_test) {
+  double test = NAN;
+  RunOps ops;
+  ops.epoch = [sh](double eps) {
+    check_shard(sh, dsgdpp_shard_epoch(sh, eps, nullptr, nullptr), "shard epoch");
+    check_shard(sh, dsgdpp_shard_share(sh), "shard share");
+  };
+  ops.loss = [sh, &test]() {
+    double v = 0;
+    check_shard(sh, dsgdpp_shard_losses(sh, &v, &test), "shard losses");
+    return v;
+  };
+  ops.test_loss = [&test]() { return test; };
+  run_epochs(ops, epochs, decay, trace, has_test);
 }
 
 }  // namespace dsgdpp

@@ -202,6 +202,76 @@ int dsgdpp_epoch_part(dsgdpp_ctx* ctx, double eps, const uint32_t* schedule,
  * context's device can reach.  Synchronous. */
 int dsgdpp_h_block_bytes(dsgdpp_ctx* ctx, uint32_t b2, uint64_t* bytes);
 int dsgdpp_h_block_copy(dsgdpp_ctx* ctx, uint32_t b2, void* device_buf, int to_context);
+/* The context runs tasks first .. first+count-1 of the d tasks: one rank's
+ * share of a job whose tasks are spread over several ranks, as an MPI rank of
+ * the reference runs its tasksPerRank tasks (tools/mfdsgdpp.cc:41-42,76-77).
+ * The entries of the other tasks' row blocks must be absent (an epoch with
+ * such entries returns DSGDPP_E_STATE); the replay's per-sub-epoch
+ * RegularizeL2 scales only these tasks' W row blocks and H blocks, as each
+ * task of DsgdPpTask::run regularizes its own pair (mf/sgd/dsgdpp_impl.h:
+ * 241-243).  Default: all d tasks. */
+int dsgdpp_set_tasks(dsgdpp_ctx* ctx, uint32_t first, uint32_t count);
+
+/* ---- one job over several ranks --------------------------------------------
+ * replaces: the H-block hand-off of DsgdPpTask::run between sub-epochs over MPI
+ * (mf/sgd/dsgdpp_impl.h:141-263: igetCopy / irecv / isend of the next
+ * block, red/blue double buffering, a barrier per sub-epoch).  Rank r of G
+ * drives a context holding its tasks' rows (dsgdpp_set_tasks(ctx, r d/G, d/G),
+ * the nnz12 weights of the whole matrix given with dsgdpp_set_counts, the W
+ * rows of other ranks zero).  A block that another rank needs next is sent
+ * from H to H right after the sub-epoch that last used it, on a transfer
+ * stream, while the next sub-epoch (the other colour) computes; only the
+ * sub-epoch that uses it waits for it.  Transports: NCCL (one rank per GPU and
+ * process, NCCL loaded at run time) or device copies between the contexts of
+ * one process (emulated ranks on one GPU).  Not for the persistent launch. */
+typedef struct dsgdpp_shard dsgdpp_shard;
+#define DSGDPP_SHARD_ID_BYTES 128
+/* A new NCCL unique id (rank 0 makes it and hands the bytes to every rank). */
+int dsgdpp_shard_unique_id(void* id);
+/* Rank `rank` of `world` over NCCL; every rank calls it with the same id. */
+int dsgdpp_shard_create_nccl(dsgdpp_ctx* ctx, int rank, int world, const void* id,
+                             dsgdpp_shard** out);
+/* `world` emulated ranks in this process: ctxs[r] is rank r's context. */
+int dsgdpp_shard_create_local(dsgdpp_ctx* const* ctxs, int world, dsgdpp_shard** out);
+void dsgdpp_shard_destroy(dsgdpp_shard* sh);
+const char* dsgdpp_shard_last_error(const dsgdpp_shard* sh);
+/* Bound on a host wait for NCCL work (default 300 s); a wait that runs out
+ * aborts the communicator and returns DSGDPP_E_CUDA (a rank left or hung). */
+int dsgdpp_shard_set_wait_limit(dsgdpp_shard* sh, double seconds);
+/* One epoch on every rank (DsgdPpRunner::epoch, mf/sgd/dsgdpp_impl.h:282-349):
+ * the given schedule and task seeds, or (both null) the draws of the master
+ * generator of the (first) context, the same on every rank seeded alike. */
+int dsgdpp_shard_epoch(dsgdpp_shard* sh, double eps, const uint32_t* schedule,
+                       const uint32_t* task_seeds);
+/* Every H block's latest version to every rank (broadcast from its holder);
+ * needed before losses or dsgdpp_get_factors of H. */
+int dsgdpp_shard_share(dsgdpp_shard* sh);
+/* The job's training loss (the configured loss over all ranks' entries, the
+ * regularizer over all of W and H) and test loss (NaN without test entries);
+ * after dsgdpp_shard_share. */
+int dsgdpp_shard_losses(dsgdpp_shard* sh, double* loss, double* test_loss);
+/* Every rank's W rows to every rank, so that dsgdpp_get_factors returns the
+ * whole W (with NCCL a sum over the ranks: each rank's W is zero outside its
+ * own rows).  For reading the result: afterwards the contexts hold all of W,
+ * so no further epoch or loss of this shard is valid. */
+int dsgdpp_shard_gather_w(dsgdpp_shard* sh);
+/* Blocks (and bytes) the ranks driven here received in the last epoch. */
+int dsgdpp_shard_moved(dsgdpp_shard* sh, uint64_t* moves, uint64_t* bytes);
+/* Timeline of the next epochs: when on, events around every sub-epoch and
+ * every transfer group; dsgdpp_shard_timeline gives, for the driven rank at
+ * `index`, [begin, end] in ms from the epoch's start of each sub-epoch
+ * (compute, 2 nb2 values) and of each transfer group posted before the epoch
+ * and after sub-epochs 0 .. nb2-2 (transfer, 2 nb2 values; NaN where the
+ * rank's transfer stream carried none of the group: emulated ranks copy on
+ * the receiver's stream, NCCL sends and receives on both ranks'). */
+int dsgdpp_shard_set_timeline(dsgdpp_shard* sh, int on);
+int dsgdpp_shard_timeline(dsgdpp_shard* sh, uint32_t index, double* compute, double* transfer);
+/* The hand-off plan of one epoch (host only, no GPU): moves as (group, block,
+ * from rank, to rank) quadruples, group 0 = before the epoch and s + 1 = after
+ * sub-epoch s; holder[nb2] (-1 = every rank) is the state before the epoch and
+ * is updated.  Returns the number of moves (written when out is not null). */
+uint64_t dsgdpp_shard_plan(uint32_t d, uint32_t nb2, int world, const uint32_t* schedule,
+                           int32_t* holder, uint32_t* out);
 /* How long one dependency wait of the persistent epoch (DSGDPP_LAUNCH_PERSISTENT)
  * may last before the epoch gives up, in seconds (default 1; 0 gives up at the
  * first unmet dependency).  A wait that runs out sets an error flag; every

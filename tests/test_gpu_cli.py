@@ -68,3 +68,43 @@ def test_cli_replay_matches_oracle(tmp_path, blocked, tool):
     if dsgd:
         assert "Starting DSGD on" in r.stdout and "DSGD options" in r.stdout
         assert "Slow MapReduce implementation: 1" in r.stdout
+
+
+@pytest.mark.parametrize("tool", ["mfdsgdpp", "mfdsgd"])
+def test_cli_multirank_path_with_one_rank_matches_oracle(tmp_path, tool):
+    # the tool's path for several ranks (task range, counts of the whole
+    # matrix, NCCL hand-off, losses summed over the ranks), run with one rank
+    p = synth.make(400, 300, 6000, 600, rank_true=4, r=5, noise=0.1, seed=4)
+    _write(tmp_path, p)
+    d = 3
+    dsgd = tool == "mfdsgd"
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([os.path.join(os.path.dirname(CLI), tool),
+                        f"--input-file={tmp_path}/train.mmc", f"--input-test-file={tmp_path}/test.mmc",
+                        f"--input-row-file={tmp_path}/W.mma", f"--input-col-file={tmp_path}/H.mma",
+                        "--rank=5", f"--tasks-per-rank={d}", "--update=Nzsl_L2(1)",
+                        "--regularize=None", "--loss=Nzsl_L2(1)", "--decay=BoldDriver(0.01)",
+                        "--epochs=4", "--seed=1499881717", "--precision=fp64", "--exec=replay",
+                        f"--shard-id-file={tmp_path}/nccl.id",
+                        f"--output-row-file={tmp_path}/Wout.mma",
+                        f"--output-col-file={tmp_path}/Hout.mma"],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "1 ranks, one GPU each" in r.stdout
+    assert not os.path.exists(tmp_path / "nccl.id")  # removed once every rank joined
+    W0 = P.read_mm_array(str(tmp_path / "W.mma"))
+    H0 = P.read_mm_array(str(tmp_path / "H.mma")).T
+    _, _, tr, tc, tv = P.read_sparse(str(tmp_path / "train.mmc"))
+    _, _, sr, sc, sv = P.read_sparse(str(tmp_path / "test.mmc"))
+    ref = O.Problem(p.m, p.n, 5, d, tr, tc, tv, sr, sc, sv,
+                    method="dsgd" if dsgd else "dsgdpp").configure()
+    ref.set_factors(W0, H0)
+    ref.seed(1499881717)
+    trace = ref.run(4, "BoldDriver", 0.01)
+    W, H = ref.get_factors()
+    np.testing.assert_allclose(P.read_mm_array(str(tmp_path / "Wout.mma")), W, rtol=1e-14, atol=1e-15)
+    np.testing.assert_allclose(P.read_mm_array(str(tmp_path / "Hout.mma")).T, H, rtol=1e-14, atol=1e-15)
+    losses = [float(x) for x in re.findall(r"\| Loss: ([0-9.e+-]+)", r.stdout)]
+    np.testing.assert_allclose(losses, trace[:, 0], rtol=1e-5)
+    tests = [float(x) for x in re.findall(r"\| Test loss: ([0-9.e+-]+)", r.stdout)]
+    np.testing.assert_allclose(tests, trace[:, 1], rtol=1e-5)

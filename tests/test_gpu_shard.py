@@ -214,3 +214,184 @@ def test_torchrun_job_matches_the_single_context_run(tmp_path):
         assert got["test_loss"] == pytest.approx(want["test_loss"], rel=1e-11)
         if got["epoch"] > 0:
             assert got["eps"] == pytest.approx(want["eps"], rel=1e-15)
+
+
+# ---- the library's hand-off (dsgdpp_shard_*): transfers on a stream of their own ----
+def _shard_contexts(p, d, world, kw, seed):
+    """Rank r's context: its tasks' rows of the training and test entries, the
+    counts of the whole matrix, its own W rows (the others zero)."""
+    off1 = list(P.block_offsets(p.m, d)) + [p.m]
+    n1 = np.bincount(p.rows, minlength=p.m).astype(np.uint64)
+    n2 = np.bincount(p.cols, minlength=p.n).astype(np.uint64)
+    ctxs = []
+    for r in range(world):
+        lo, hi = shard.rank_rows(off1, d, world, r)
+        keep = (p.rows >= lo) & (p.rows < hi)
+        tkeep = (p.trows >= lo) & (p.trows < hi)
+        c = P.Context(P.Config(**kw))
+        c.set_tasks(r * (d // world), d // world)
+        c.set_matrix(P.TRAIN, p.rows[keep], p.cols[keep], p.vals[keep])
+        c.set_matrix(P.TEST, p.trows[tkeep], p.tcols[tkeep], p.tvals[tkeep])
+        c.set_counts(n1, n2)
+        Wz = np.zeros_like(p.W0)
+        Wz[lo:hi] = p.W0[lo:hi]
+        c.set_factors(Wz, p.H0)
+        c.seed(seed)
+        ctxs.append(c)
+    return ctxs, off1
+
+
+def _gather(ctxs, off1, d, world):
+    W = ctxs[0].get_factors()[0].copy()
+    for r, c in enumerate(ctxs):
+        lo, hi = shard.rank_rows(off1, d, world, r)
+        W[lo:hi] = c.get_factors()[0][lo:hi]
+    return W, ctxs[0].get_factors()[1]
+
+
+@pytest.mark.parametrize("method", ["dsgdpp", "dsgd"])
+@pytest.mark.parametrize("regularize", ["None", "L2"])
+@pytest.mark.parametrize("world", [2, 4])
+def test_library_shard_replay_equals_one_context(world, regularize, method):
+    p = synth.make(900, 700, 20000, 2000, rank_true=6, r=8, noise=0.1, seed=8)
+    d, eps = 4, 0.02
+    kw = dict(m=p.m, n=p.n, rank=8, d=d, precision="fp64", exec="replay", launch="stream",
+              regularize=regularize, regularize_lambda=0.05 if regularize == "L2" else 0.0,
+              loss="Nzsl_L2", loss_lambda=0.1, method=method)
+    ctxs, off1 = _shard_contexts(p, d, world, kw, seed=3)
+    ref = P.Context(P.Config(**kw))
+    try:
+        ref.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ref.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ref.set_factors(p.W0, p.H0)
+        ref.seed(3)
+        with P.Shard.local(ctxs) as sh:
+            moved = 0
+            for _ in range(3):
+                ref.epoch(eps)  # both draw from a master generator seeded 3
+                sh.epoch(eps)
+                moved += sh.moved()[0]
+                sh.share()
+                loss, test = sh.losses()
+                assert loss == pytest.approx(ref.loss(), rel=1e-12)
+                assert test == pytest.approx(ref.nzsl(P.TEST), rel=1e-12)
+            assert moved > 0
+        W, H = _gather(ctxs, off1, d, world)
+        Wr, Hr = ref.get_factors()
+        np.testing.assert_array_equal(W, Wr)
+        np.testing.assert_array_equal(H, Hr)
+        for c in ctxs[1:]:  # after share every rank holds all of H
+            np.testing.assert_array_equal(c.get_factors()[1], Hr)
+    finally:
+        ref.close()
+        for c in ctxs:
+            c.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", 0.005), ("bf16", 0.01)])
+def test_library_shard_hogwild_tracks_one_context(precision, tol):
+    p = synth.make(40000, 20000, 800000, 20000, rank_true=8, r=16, noise=0.1, seed=9)
+    d, world = 8, 4
+    kw = dict(m=p.m, n=p.n, rank=16, d=d, precision=precision, exec="hogwild",
+              launch="stream", regularize="L2", regularize_lambda=0.05)
+    ctxs, off1 = _shard_contexts(p, d, world, kw, seed=5)
+    ref = P.Context(P.Config(**dict(kw, launch="graph")))
+    try:
+        ref.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ref.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ref.set_factors(p.W0, p.H0)
+        ref.seed(5)
+        with P.Shard.local(ctxs) as sh:
+            for _ in range(6):
+                ref.epoch(0.01)
+                sh.epoch(0.01)
+                sh.share()
+            _, test = sh.losses()
+        got = np.sqrt(test / len(p.tvals))
+        want = np.sqrt(ref.nzsl(P.TEST) / len(p.tvals))
+        assert abs(got - want) <= tol * want, (got, want)
+    finally:
+        ref.close()
+        for c in ctxs:
+            c.close()
+
+
+def test_library_shard_transfers_overlap_the_next_sub_epoch():
+    # two emulated ranks: a block used at sub-epoch s travels on the transfer
+    # stream while sub-epoch s + 1 (the other colour) computes, and sub-epoch
+    # s + 1 does not wait for it
+    p = synth.make(200000, 400000, 2000000, 100, rank_true=8, r=32, noise=0.1, seed=4)
+    d, world = 4, 2
+    kw = dict(m=p.m, n=p.n, rank=32, d=d, precision="fp32", exec="hogwild", launch="stream")
+    ctxs, _ = _shard_contexts(p, d, world, kw, seed=2)
+    try:
+        with P.Shard.local(ctxs) as sh:
+            sh.epoch(0.01)
+            sh.share()
+            sh.set_timeline(True)
+            sh.epoch(0.01)
+            moves, nbytes = sh.moved()
+            assert moves > 0 and nbytes > 0
+            overlapped = total = 0
+            for r in range(world):
+                comp, xfer = sh.timeline(r, 2 * d)
+                for g in range(1, 2 * d - 1):  # posted after sub-epoch g - 1
+                    if np.isnan(xfer[g, 0]):
+                        continue
+                    total += 1
+                    assert xfer[g, 0] >= comp[g - 1, 1] - 1e-3  # after the sub-epoch that used it
+                    # it travels while sub-epoch g computes: it begins before g ends
+                    if xfer[g, 0] < comp[g, 1] and xfer[g, 1] > comp[g, 0]:
+                        overlapped += 1
+            assert total > 0 and overlapped >= total // 2, (overlapped, total)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_library_shard_checks_its_contexts():
+    p = synth.make(300, 200, 3000, 100, rank_true=4, r=8, noise=0.1, seed=1)
+    kw = dict(m=p.m, n=p.n, rank=8, d=4, launch="stream")
+    a, b = P.Context(P.Config(**kw)), P.Context(P.Config(**kw))
+    try:
+        with pytest.raises(P.DsgdppError):  # the task ranges were not set
+            P.Shard.local([a, b])
+        a.set_tasks(0, 2)
+        b.set_tasks(2, 2)
+        a.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)  # rows of rank 1 in rank 0's context
+        a.set_factors(p.W0, p.H0)
+        b.set_matrix(P.TRAIN, [], [], [])
+        b.set_factors(p.W0, p.H0)
+        with P.Shard.local([a, b]) as sh:
+            with pytest.raises(P.DsgdppError, match="does not run here"):
+                sh.epoch(0.01)
+        with pytest.raises(P.DsgdppError):
+            a.set_tasks(3, 2)
+    finally:
+        a.close()
+        b.close()
+
+
+def test_library_shard_over_nccl_with_one_rank_equals_one_context():
+    # the NCCL transport's plumbing on one GPU (one rank: nothing moves)
+    p = synth.make(900, 700, 20000, 2000, rank_true=6, r=8, noise=0.1, seed=8)
+    kw = dict(m=p.m, n=p.n, rank=8, d=4, precision="fp64", exec="replay", launch="stream")
+    ctxs, _ = _shard_contexts(p, 4, 1, kw, seed=3)
+    ref = P.Context(P.Config(**kw))
+    try:
+        ref.set_matrix(P.TRAIN, p.rows, p.cols, p.vals)
+        ref.set_matrix(P.TEST, p.trows, p.tcols, p.tvals)
+        ref.set_factors(p.W0, p.H0)
+        ref.seed(3)
+        with P.Shard.nccl(ctxs[0], 0, 1, P.shard_unique_id()) as sh:
+            for _ in range(2):
+                ref.epoch(0.02)
+                sh.epoch(0.02)
+                sh.share()
+                loss, test = sh.losses()
+                assert loss == pytest.approx(ref.loss(), rel=1e-12)
+                assert test == pytest.approx(ref.nzsl(P.TEST), rel=1e-12)
+        np.testing.assert_array_equal(ctxs[0].get_factors()[1], ref.get_factors()[1])
+    finally:
+        ref.close()
+        ctxs[0].close()

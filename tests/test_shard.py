@@ -39,6 +39,47 @@ def test_plan_puts_every_block_on_its_task_rank():
         assert where == holder
 
 
+@pytest.mark.parametrize("world", [1, 2, 4])
+@pytest.mark.parametrize("method", ["dsgdpp", "dsgd"])
+def test_library_plan_matches_the_python_plan(world, method):
+    # dsgdpp_shard_plan (the C++ hand-off) posts each move right after the
+    # block's previous use; its moves are the Python plan's, block for block
+    import dsgdpp_b200 as P
+    d = 8
+    nb2 = 2 * d if method == "dsgdpp" else d
+    rng = P.Random32(11)
+    holder_py = shard.new_holders(nb2)
+    holder_c = np.full(nb2, -1, np.int32)
+    for e in range(3):
+        if method == "dsgdpp":
+            sched, _ = P.draw_schedule(rng, d, "COWOR")
+        else:
+            sched = P.dsgd_schedule(rng, 1, d, "COWOR")
+        before = holder_c.copy()
+        plan = shard.handoff_plan(sched, d, world, holder_py)
+        moves, holder_c = P.shard_plan(d, nb2, world, sched, holder_c)
+        assert list(holder_c) == holder_py
+        # the group of a move = one past the block's previous use in the epoch
+        last = {}
+        want = []
+        for s in range(nb2):
+            for b2, src, dst in plan[s]:
+                want.append((last.get(b2, -1) + 1, b2, src, dst))
+            for t in range(d):
+                last[int(sched[s, t])] = s
+        assert sorted(map(tuple, moves.tolist())) == sorted(want)
+        if method == "dsgdpp":
+            # red/blue: inside an epoch a block moves while the other colour computes
+            inner = [m for m in moves.tolist() if m[0] > 0]
+            for g, b2, _, _ in inner:
+                nxt = min(s for s in range(g, nb2) if b2 in set(sched[s].tolist()))
+                assert nxt >= g + 1  # used again no earlier than two sub-epochs later
+        if (before == -1).all():  # every rank holds every block: nothing moves before the epoch
+            assert all(m[0] > 0 for m in moves.tolist())
+        if world == 1:
+            assert len(moves) == 0
+
+
 def test_task_ranges_need_a_multiple():
     with pytest.raises(ValueError):
         shard.task_owner(5, 2)
