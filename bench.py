@@ -73,6 +73,7 @@ WORKLOADS = {
                     "Nzsl_L2(1) update, no regularize"),
 }
 CPU_SAMPLE = 10_000_000
+C5_SEED = 4242  # held out: the controller was trained on other matrices
 
 
 def peaks():
@@ -238,6 +239,72 @@ def _synth_gpu():
     return mod
 
 
+def arm_oracle_errors(P, data, wl, arms, epochs, device, layout, threads=None):
+    """Test RMSE error against the FP64 oracle of every time-to-target arm:
+    on the CPU baseline's sample, each arm's first `epochs` step sizes run on
+    the oracle (FP64, sequential per block) and on this implementation in the
+    arm's precision, with the same d, seed and schedules."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
+    l2 = wl["s"] is not None and wl.get("kind") != "ratings"
+    conf = dict(update="Nzsl_L2", update_lambda=1.0, regularize="L2" if l2 else "None",
+                regularize_lambda=0.05 if l2 else 0.0, loss="Nzsl_L2", loss_lambda=1.0)
+    prob = O.Problem(wl["m"], wl["n"], wl["rank"], threads, rows, cols, vals,
+                     data["trows"], data["tcols"], data["tvals"])
+    prob.configure(**conf)
+    ntest = len(data["tvals"])
+    out = {}
+    for name, arm in arms.items():
+        steps = [e for e in arm["eps"] if np.isfinite(e)][:epochs]
+        prob.set_factors(data["W0"], data["H0"])
+        prob.seed(1)
+        for eps in steps:
+            prob.epoch(eps, threads=threads)
+        want = float(np.sqrt(prob.nzsl(1) / ntest))
+        cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=threads,
+                       precision=arm["precision"], device=device, layout=layout, **conf)
+        with P.Context(cfg) as ctx:
+            ctx.set_matrix(P.TRAIN, rows, cols, vals)
+            ctx.set_matrix(P.TEST, data["trows"], data["tcols"], data["tvals"])
+            ctx.set_factors(data["W0"], data["H0"])
+            ctx.seed(1)
+            for eps in steps:
+                ctx.epoch(eps)
+            got = float(np.sqrt(ctx.nzsl(P.TEST) / ntest))
+        out[name] = {"precision": arm["precision"], "epochs": len(steps),
+                     "oracle_fp64_test_rmse": want, "test_rmse": got,
+                     "rel_error": (got - want) / want}
+    return {"sample": f"{len(vals):,} entries of the workload (the CPU baseline's sample), "
+                      f"d={threads}, each arm's first step sizes", "arms": out}
+
+
+def time_to_target_leg(P, wl, data, d, args, local, seed_note):
+    """BF16 + learned controller (and the other tuned arms) against plain FP32
+    BoldDriver(0.001) on `data`, with each arm's test RMSE error against the
+    FP64 oracle."""
+    from dsgdpp_b200 import ttt as TT
+    net = P.Mlp(device=local, seed=1)
+    net.params = np.load(TT.PARAMS)
+    r = TT.evaluate(P, wl, data, d, epochs=50, eps0=0.001, net=net, device=local,
+                    layout=args.layout)
+    net.close()
+    leg = {"workload": wl["text"], "data_seed": seed_note,
+           "target": "plain FP32 BoldDriver's test RMSE after 50 epochs, +0.5%",
+           "target_test_rmse": r["target_test_rmse"], "plain_fp32_s": r["plain_fp32_s_traced"]}
+    for k in ("bf16_bolddriver", "fp32_controller", "bf16_controller"):
+        leg[k] = {q: r[k][q] for q in ("epochs_to_target", "seconds_to_target",
+                                        "ratio_to_plain", "fallbacks", "final_test_rmse")}
+    if not args.no_cpu_baseline:
+        arms = {k: r[k] for k in ("plain_fp32", "bf16_bolddriver", "fp32_controller",
+                                  "bf16_controller")}
+        errs = arm_oracle_errors(P, data, wl, arms, 4, local, args.layout)
+        leg["vs_fp64_oracle"] = errs
+        for k, v in errs["arms"].items():
+            leg.setdefault(k, {})["test_rmse_rel_error_vs_fp64_oracle"] = v["rel_error"]
+    return leg
+
+
 def generate(wl, seed):
     import torch
     synth_gpu = _synth_gpu()
@@ -379,6 +446,97 @@ def run_reference(args):
     return 0
 
 
+def run_shard(args, world, rank, local, pg):
+    """One job over the ranks (`--mode shard`): rank r runs tasks r d/N ..
+    (r+1) d/N - 1 on its GPU and the H column blocks move between the ranks
+    over NCCL, each transfer overlapping the next sub-epoch (dsgdpp_shard_*).
+    A step is one epoch plus the broadcast of every block from its holder
+    (what the per-epoch losses need).  value = the job's updates / the
+    slowest rank's device time of the epochs; scaling is strong (the job is
+    the same at every N)."""
+    import torch
+    import dsgdpp_b200 as P
+    wl = WORKLOADS[args.workload]
+    d = args.d or wl["d"]
+    d = world * ((d + world - 1) // world)  # d a multiple of the ranks
+    data, gen_s = generate(wl, args.seed)  # the same matrix on every rank
+    m, n = wl["m"], wl["n"]
+    off1 = list(P.block_offsets(m, d)) + [m]
+    per = d // world
+    lo, hi = int(off1[rank * per]), int(off1[(rank + 1) * per])
+    l2 = wl["s"] is not None and wl.get("kind") != "ratings"
+    cfg = P.Config(m=m, n=n, rank=wl["rank"], d=d, precision=args.precision, exec="hogwild",
+                   launch="stream", update="Nzsl_L2", update_lambda=1.0,
+                   regularize="L2" if l2 else "None", regularize_lambda=0.05 if l2 else 0.0,
+                   loss="Nzsl_L2", loss_lambda=1.0, lanes_per_nnz=args.lanes,
+                   vecs_per_lane=args.vecs, ctas_per_sm=args.ctas_per_sm, device=local,
+                   write_mode=args.write_mode, layout=args.layout)
+    keep = (data["rows"] >= lo) & (data["rows"] < hi)
+    tkeep = (data["trows"] >= lo) & (data["trows"] < hi)
+    n1 = np.bincount(data["rows"], minlength=m).astype(np.uint64)
+    n2 = np.bincount(data["cols"], minlength=n).astype(np.uint64)
+    W = np.zeros_like(data["W0"])
+    W[lo:hi] = data["W0"][lo:hi]
+    ctx = P.Context(cfg)
+    ctx.set_tasks(rank * per, per)
+    ctx.set_matrix(P.TRAIN, data["rows"][keep], data["cols"][keep], data["vals"][keep])
+    ctx.set_matrix(P.TEST, data["trows"][tkeep], data["tcols"][tkeep], data["tvals"][tkeep])
+    ctx.set_counts(n1, n2)
+    ctx.set_factors(W, data["H0"])
+    ctx.seed(args.seed)
+    nnz_rank = int(keep.sum())
+    del data
+    uid = [P.shard_unique_id() if rank == 0 else None]
+    if pg is not None:
+        pg.broadcast_object_list(uid, src=0)
+    sh = P.Shard.nccl(ctx, rank, world, uid[0])
+    sh.set_wait_limit(120)
+    eps = 0.001
+    for _ in range(args.warmup):
+        sh.epoch(eps)
+        sh.share()
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ep_ms, moved = [], 0
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        sh.epoch(eps)
+        ep_ms.append(ctx.last_epoch_ms())
+        moved += sh.moved()[1]
+        sh.share()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    barrier(pg)
+    loss, test = sh.losses()
+    t_dev = allreduce_max(pg, sum(ep_ms) / 1e3)
+    value = job_rate(pg, nnz_rank * args.steps, sum(ep_ms) / 1e3)
+    wall = allreduce_max(pg, wall)
+    moved = allreduce_sum(pg, moved)
+    sh.close()
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": "SGD updates/s (DSGD++ epoch)", "value": value, "unit": "updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic (seeded; no public dataset)",
+            "config": workload_config(wl, args.precision),
+            "launch": {"d": d, "blocks": f"{d} x {2 * d}", "exec": "hogwild", "launch": "stream",
+                       "parallelism": f"one job over {world} ranks (tasks {per} per rank), "
+                                      "H blocks over NCCL"},
+            "shard": {"h_bytes_moved_per_epoch": moved / args.steps,
+                      "wall_s_with_share": wall, "final_loss": loss,
+                      "final_test_rmse": float(np.sqrt(test / wl["nnz_test"]))},
+            "e2e": None, "roofline": None, "cpu_baseline": None,
+            "gpu_launches": args.steps * 2 * d, "clocks": clk, "generate_s": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,6 +561,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ttt", action="store_true",
                     help="skip the time-to-target comparison (tuned vs plain FP32)")
+    ap.add_argument("--no-ttt-c5", action="store_true",
+                    help="skip the time-to-target comparison on the 300M-entry workload")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "shard"],
+                    help="under torchrun: independent replicas of the job, or one job whose "
+                         "tasks are spread over the ranks (H blocks handed over with NCCL)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -417,6 +580,12 @@ def main():
         return run_reference(args)
 
     world, rank, local, pg = dist_setup()
+    if args.mode == "shard":
+        rc = run_shard(args, world, rank, local, pg)
+        if pg is not None:
+            barrier(pg)
+            pg.destroy_process_group()
+        return rc
 
     import dsgdpp_b200 as P
     wl = WORKLOADS[args.workload]
@@ -536,17 +705,15 @@ def main():
     # ---- time to target test RMSE: BF16 + learned controller vs plain FP32 ----
     ttt = None
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_ttt:
-        from dsgdpp_b200 import ttt as TT
-        net = P.Mlp(device=local, seed=1)
-        net.params = np.load(TT.PARAMS)
-        r = TT.evaluate(P, wl, data, d, epochs=50, eps0=eps, net=net, device=local,
-                        layout=args.layout)
-        net.close()
-        ttt = {"target": "plain FP32 BoldDriver's test RMSE after 50 epochs, +0.5%",
-               "target_test_rmse": r["target_test_rmse"], "plain_fp32_s": r["plain_fp32_s_traced"]}
-        for k in ("bf16_bolddriver", "fp32_controller", "bf16_controller"):
-            ttt[k] = {q: r[k][q] for q in ("epochs_to_target", "seconds_to_target",
-                                            "ratio_to_plain", "fallbacks")}
+        ttt = time_to_target_leg(P, wl, data, d, args, local, args.seed)
+        if not args.no_ttt_c5:
+            # the controller's evaluation workload: 300M entries, rank 64, a data
+            # seed the controller was not trained on
+            del data, host
+            wl5 = WORKLOADS["c5"]
+            data5, _ = generate(wl5, C5_SEED)
+            ttt["c5"] = time_to_target_leg(P, wl5, data5, wl5["d"], args, local, C5_SEED)
+            del data5
     if rank == 0:
         line = {
             "metric": "SGD updates/s (DSGD++ epoch)", "value": value, "unit": "updates/s",

@@ -18,6 +18,7 @@
 #include "context.h"
 #include "rm_device.h"
 #include "kernels.cuh"
+#include "trace_ranges.h"
 #include "schedule.h"
 
 using namespace dsgdpp;
@@ -1148,6 +1149,7 @@ int dsgdpp_seed(dsgdpp_ctx* c, uint32_t seed) {
 }
 
 int dsgdpp_epoch(dsgdpp_ctx* c, double eps) {
+  TraceRange range("epoch");
   return guarded(c, [&]() {
     const uint32_t d = c->d;
     std::vector<uint32_t> sched((size_t)c->nb2 * d), seeds(d);
@@ -1159,6 +1161,7 @@ int dsgdpp_epoch(dsgdpp_ctx* c, double eps) {
 
 int dsgdpp_epoch_explicit(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
                           const uint32_t* task_seeds) {
+  TraceRange range("epoch");
   return guarded(c, [&]() {
     epoch_explicit_impl(c, eps, schedule, task_seeds);
     return DSGDPP_OK;
@@ -1167,6 +1170,7 @@ int dsgdpp_epoch_explicit(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
 
 int dsgdpp_epoch_part(dsgdpp_ctx* c, double eps, const uint32_t* schedule,
                       const uint32_t* task_seeds, uint32_t s_begin, uint32_t s_end) {
+  TraceRange range(s_end - s_begin == 1 ? "subepoch" : "epoch");
   return guarded(c, [&]() {
     epoch_part_impl(c, eps, schedule, task_seeds, s_begin, s_end);
     return DSGDPP_OK;
@@ -1269,6 +1273,7 @@ int dsgdpp_launch_shape(dsgdpp_ctx* c, uint32_t* lanes, uint32_t* vecs, uint32_t
 }
 
 int dsgdpp_loss(dsgdpp_ctx* c, double* out) {
+  TraceRange range("loss");
   return guarded(c, [&]() {
     if (!out) throw Error(DSGDPP_E_INVALID, "null output");
     *out = loss_impl(c);
@@ -1277,6 +1282,7 @@ int dsgdpp_loss(dsgdpp_ctx* c, double* out) {
 }
 
 int dsgdpp_nzsl(dsgdpp_ctx* c, int which, double* out) {
+  TraceRange range("loss");
   return guarded(c, [&]() {
     if (!out) throw Error(DSGDPP_E_INVALID, "null output");
     *out = nzsl_impl(c, which);
@@ -1285,6 +1291,7 @@ int dsgdpp_nzsl(dsgdpp_ctx* c, int which, double* out) {
 }
 
 int dsgdpp_l2(dsgdpp_ctx* c, double* w2, double* h2) {
+  TraceRange range("loss");
   return guarded(c, [&]() {
     check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
     if (w2) *w2 = sumsq_impl(c, c->W, c->cfg.m * c->rp);
@@ -1294,6 +1301,7 @@ int dsgdpp_l2(dsgdpp_ctx* c, double* w2, double* h2) {
 }
 
 int dsgdpp_nzl2(dsgdpp_ctx* c, double* w, double* h) {
+  TraceRange range("loss");
   return guarded(c, [&]() {
     if (!c->mat[0].present) throw Error(DSGDPP_E_STATE, "no training matrix");
     check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");

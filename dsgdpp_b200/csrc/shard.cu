@@ -50,6 +50,7 @@
 
 #include "../../include/dsgdpp.h"
 #include "context.h"
+#include "trace_ranges.h"
 
 using namespace dsgdpp;
 
@@ -212,6 +213,7 @@ char* h_block(dsgdpp_ctx* c, uint32_t b2, size_t* bytes) {
 // Waits for an event on the host, bounded; under NCCL an asynchronous NCCL
 // error or the limit aborts the communicator.
 void bounded_wait(dsgdpp_shard* sh, cudaEvent_t ev, const char* what) {
+  TraceRange range("barrier");
   const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     const cudaError_t e = cudaEventQuery(ev);
@@ -308,6 +310,7 @@ dsgdpp_shard* new_shard(uint32_t d, uint32_t nb2, int world, int device) {
 
 // The transfers of group g for every driven rank.
 void post_group(dsgdpp_shard* sh, const Plan& plan, uint32_t g) {
+  TraceRange range("communication");
   const auto& moves = plan.groups[g];
   for (auto& R : sh->ranks) {
     cudaEvent_t after = g == 0 ? R.start : R.sub_end[g - 1];
@@ -367,6 +370,7 @@ void post_group(dsgdpp_shard* sh, const Plan& plan, uint32_t g) {
 
 void shard_epoch_impl(dsgdpp_shard* sh, double eps, const uint32_t* schedule,
                       const uint32_t* seeds) {
+  TraceRange range("epoch");
   require_comm(sh);
   check_cuda(cudaSetDevice(sh->device), "cudaSetDevice");
   const uint32_t d = sh->d, nb2 = sh->nb2;
@@ -405,7 +409,10 @@ void shard_epoch_impl(dsgdpp_shard* sh, double eps, const uint32_t* schedule,
           check_cuda(cudaStreamWaitEvent(R.ctx->stream, Q.group_done[s], 0), "transfer drain");
       }
       if (sh->timeline) check_cuda(cudaEventRecord(R.tc0[s], R.ctx->stream), "event");
-      check_ctx(R.ctx, dsgdpp_epoch_part(R.ctx, eps, schedule, seeds, s, s + 1), "sub-epoch");
+      {
+        TraceRange range("computation");
+        check_ctx(R.ctx, dsgdpp_epoch_part(R.ctx, eps, schedule, seeds, s, s + 1), "sub-epoch");
+      }
       if (sh->timeline) check_cuda(cudaEventRecord(R.tc1[s], R.ctx->stream), "event");
       check_cuda(cudaEventRecord(R.sub_end[s], R.ctx->stream), "event");
     }
@@ -419,6 +426,7 @@ void shard_epoch_impl(dsgdpp_shard* sh, double eps, const uint32_t* schedule,
 // Every block's latest version to every rank, on the compute streams after
 // the epoch.
 void share_impl(dsgdpp_shard* sh) {
+  TraceRange range("communication");
   require_comm(sh);
   check_cuda(cudaSetDevice(sh->device), "cudaSetDevice");
   if (sh->use_nccl) {

@@ -20,6 +20,12 @@ After an epoch, ``share_local`` / ``share_torch`` give every rank every
 block's latest version; the training loss is then the sum of the ranks'
 losses over their own entries.
 
+With NCCL, ``main`` runs the job through the library's own hand-off
+(:class:`dsgdpp_b200.Shard`, ``dsgdpp_shard_*`` in C++): blocks move from H
+to H on a transfer stream while the next sub-epoch computes.  The transports
+here (``torch_exchange`` over gloo through pinned host buffers,
+``local_exchange``) stay for CPU process groups and for tests.
+
 Transports: ``torch_exchange`` moves blocks with torch.distributed
 point-to-point operations (NCCL between GPUs; gloo works for host buffers),
 ``local_exchange`` moves them between contexts of one process (several
@@ -168,6 +174,35 @@ def _bold_driver(eps: float, prev: float, cur: float, dec: float = 0.5, inc: flo
     return eps * (dec if prev <= cur else inc)
 
 
+def _run_library_shard(args, ctx, rank, world, d, dist):
+    """The job over NCCL through the library's hand-off (dsgdpp_shard_*): the
+    transfers overlap the sub-epochs in between, the schedule comes from every
+    rank's master generator seeded alike."""
+    import json
+    from . import Shard, shard_unique_id
+    per = d // world
+    ctx.set_tasks(rank * per, per)
+    ctx.seed(args.seed)
+    uid = [shard_unique_id() if rank == 0 else None]
+    dist.broadcast_object_list(uid, src=0)
+    with Shard.nccl(ctx, rank, world, uid[0]) as sh:
+        sh.share()
+        loss, test = sh.losses()
+        if rank == 0:
+            print(json.dumps({"epoch": 0, "loss": loss, "test_loss": test}), flush=True)
+        eps, prev = args.eps0, None
+        for e in range(1, args.epochs + 1):
+            if prev is not None:
+                eps = _bold_driver(eps, prev, loss)
+            sh.epoch(eps)
+            sh.share()
+            prev = loss
+            loss, test = sh.losses()
+            if rank == 0:
+                print(json.dumps({"epoch": e, "loss": loss, "test_loss": test, "eps": eps}),
+                      flush=True)
+
+
 def main(argv=None):
     """DSGD++ over torchrun ranks with BoldDriver, one GPU per rank:
 
@@ -232,6 +267,10 @@ def main(argv=None):
         Wz = np.zeros_like(W0)  # rows of other ranks stay zero: they add nothing to L2 here
         Wz[lo:hi] = W0[lo:hi]
         ctx.set_factors(Wz, H0)
+        if args.backend == "nccl":
+            _run_library_shard(args, ctx, rank, world, d, dist)
+            ctx.close()
+            return
         holder = new_holders(2 * d)
 
         def job_losses():

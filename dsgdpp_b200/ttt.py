@@ -73,7 +73,11 @@ def evaluate(P, wl, data, d, epochs=50, eps0=0.001, net=None, seed=777, device=0
         ep, secs = time_to_target(tr, target_loss)
         out[name] = {"epochs_to_target": ep, "seconds_to_target": secs, "wall_s": wall,
                      "final_test_rmse": rmse(tr[-1]["test_loss"]), "fallbacks": fb,
-                     "ratio_to_plain": (secs / out["plain_fp32_s_traced"]) if ep else None}
+                     "ratio_to_plain": (secs / out["plain_fp32_s_traced"]) if ep else None,
+                     "precision": prec,
+                     # the step sizes of the kept epochs, in order
+                     "eps": [r["eps"] for r in tr[1:]]}
+    out["plain_fp32"] = {"precision": "fp32", "eps": [r["eps"] for r in plain[1:]]}
     if log_dump:
         with open(log_dump, "w") as f:
             json.dump(dump, f)
