@@ -219,13 +219,96 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   }
 }
 
+// Records of a chunk in the shuffled order: 32/LPN records at a time, one per
+// group of LPN lanes, each W/H vector loaded right before it is used.
+template <typename T, int LPN, int VPL, bool ATOMIC>
+__device__ __forceinline__ void shuffled_chunk(const HogwildArgs& a, T* W, T* H, uint32_t nrec,
+                                               uint32_t my_row, uint32_t my_col,
+                                               typename Elem<T>::C my_x, typename Elem<T>::C my_a,
+                                               typename Elem<T>::C my_b, typename Elem<T>::C eps,
+                                               typename Elem<T>::C cwh, typename Elem<T>::C rw,
+                                               typename Elem<T>::C rh, typename Elem<T>::C tmin,
+                                               typename Elem<T>::C tmax, const Philox4& base,
+                                               uint32_t grp, uint32_t gl) {
+  using E = Elem<T>;
+  using C = typename E::C;
+  constexpr int VW = E::VW;
+  constexpr int NG = 32 / LPN;
+  for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
+    const uint32_t ri = t0 + grp;
+    const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
+    const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
+    const C x = __shfl_sync(kFullMask, my_x, ri);
+    const C ca = __shfl_sync(kFullMask, my_a, ri);
+    const C cb = __shfl_sync(kFullMask, my_b, ri);
+    const bool valid = ri < nrec;
+    T* wp = W + (size_t)row * a.rp;
+    T* hp = H + (size_t)col * a.rp;
+    uint4 wv[VPL], hv[VPL];
+    bool live[VPL];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      live[v] = valid && e0 < a.rp;
+      if (live[v]) {
+        wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
+        hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
+      } else {
+        wv[v] = make_uint4(0, 0, 0, 0);
+        hv[v] = make_uint4(0, 0, 0, 0);
+      }
+    }
+    C dot = 0;
+    C wf[VPL][VW], hf[VPL][VW];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      E::unpack(wv[v], wf[v]);
+      E::unpack(hv[v], hf[v]);
+#pragma unroll
+      for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
+    }
+#pragma unroll
+    for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
+    const C f1 = (C)-2 * eps * (x - dot * cwh);
+    const C fw = f1 * rw, fh = f1 * rh;
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      if (!live[v]) continue;
+      C nw[VW], nh[VW];
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
+        nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
+      }
+      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+      if (!ATOMIC && a.truncate) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          if (e0 + e < a.r) {
+            nw[e] = clampw(nw[e], tmin, tmax, eps);
+            nh[e] = clampw(nh[e], tmin, tmax, eps);
+          }
+      }
+      // tags: iteration t0 / NG of this group, vector v, side
+      const uint32_t tg = 2u * ((t0 / NG) * VPL + v);
+      write_vec<T, ATOMIC>(wp + e0, wv[v], wf[v], nw, base, tg);
+      write_vec<T, ATOMIC>(hp + e0, hv[v], hf[v], nh, base, tg + 1u);
+    }
+  }
+}
+
 // One launch = one work list of segments (a segment = one conflict-free block
-// of a sub-epoch; several problems' segments in the batched form).  Warps take
-// 32-entry chunks from the launch's work counter; a chunk's entries are loaded
-// one per lane, and 32/LPN entries are updated at once, each W/H vector loaded
-// right before it is used.  (Prefetching the next chunk's rows into registers
-// or into shared memory with cp.async measured slower on B200: the extra
-// registers or shared memory cost more resident warps than the prefetch gains.)
+// of a sub-epoch; several problems' segments in the batched form), cut into
+// 32-entry chunks.  Warp w of the grid takes chunks w, w + (warps in the
+// grid), ... of the list (in the epoch's chunk permutation), so no chunk
+// counter is needed and the next chunk is known in advance: its entries (one
+// per lane) are loaded while the current chunk is updated, and its inverse
+// counts at the end, so a chunk costs about one memory round trip per record
+// of a group.  32/LPN entries are updated at once, each W/H vector loaded
+// right before it is used.  (Prefetching the next chunk's factor rows into
+// registers or shared memory measured slower on B200: the registers or shared
+// memory cost more resident warps than the prefetch gains; its entries take
+// five registers.)
 // One vector per lane: BF16 is held to 64 registers (4 CTAs per SM; 70
 // unconstrained, where 3 CTAs per SM left it latency-bound; up to 16 lanes
 // per entry the cap costs no spills), FP32 to 48 (5 CTAs per SM; a few bytes
@@ -236,8 +319,6 @@ __global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeo
     hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
-  constexpr int VW = E::VW;
-  constexpr int NG = 32 / LPN;
   constexpr bool kSR = sizeof(T) == 2;
 
   const LaunchDesc ld = a.launches[li];
@@ -255,7 +336,10 @@ __global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeo
   }
   const uint32_t total = seg[nseg].chunk_begin;
   if (total == 0 || nseg == 0) return;
-  uint32_t* counter = a.counters + ld.counter;
+  const uint32_t warps = blockDim.x >> 5;
+  const uint32_t stride = gridDim.x * warps;  // warps in the grid
+  uint32_t lc = blockIdx.x * warps + (threadIdx.x >> 5);
+  if (lc >= total) return;
 
   const EpochParams ep = *a.params;
   const C lambda2 = (C)(2.0 * a.lambda);
@@ -271,143 +355,99 @@ __global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeo
   const C* vals = reinterpret_cast<const C*>(a.val);
   T* W = reinterpret_cast<T*>(a.W);
   T* H = reinterpret_cast<T*>(a.H);
+  const bool weighted = a.update == kUpdNzslL2;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t grp = lane / LPN, gl = lane % LPN;
 
-  for (;;) {
-    uint32_t lc = 0;
-    if (lane == 0) lc = atomicAdd(counter, 1u);
-    lc = __shfl_sync(kFullMask, lc, 0);
-    if (lc >= total) break;
+  // chunk c of the list -> its segment, first record and record count
+  auto locate = [&](uint32_t c, uint32_t& lo, uint64_t& rb, uint32_t& nrec) {
     uint32_t pc;
     if (a.sgd_order == 1)  // WR: chunks drawn with replacement
-      pc = (uint32_t)(mix64(h ^ ((uint64_t)lc << 20)) % total);
+      pc = (uint32_t)(mix64(h ^ ((uint64_t)c << 20)) % total);
     else
-      pc = (uint32_t)((mulA * lc + addB) % total);
-    uint32_t lo = 0, hi = nseg - 1;  // the last segment with chunk_begin <= pc
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi + 1) >> 1;
-      if (seg[mid].chunk_begin <= pc) lo = mid; else hi = mid - 1;
+      pc = (uint32_t)((mulA * c + addB) % total);
+    uint32_t l = 0, hi = nseg - 1;  // the last segment with chunk_begin <= pc
+    while (l < hi) {
+      const uint32_t mid = (l + hi + 1) >> 1;
+      if (seg[mid].chunk_begin <= pc) l = mid; else hi = mid - 1;
     }
-    const uint32_t cin = pc - seg[lo].chunk_begin;
-    const uint64_t rb = seg[lo].rec_begin + (uint64_t)cin * kChunk;
-    const uint32_t nrec = min((uint32_t)kChunk, seg[lo].count - cin * kChunk);
+    lo = l;
+    const uint32_t cin = pc - seg[l].chunk_begin;
+    rb = seg[l].rec_begin + (uint64_t)cin * kChunk;
+    nrec = min((uint32_t)kChunk, seg[l].count - cin * kChunk);
+  };
+
+  // the chunk in hand: its entries, one per lane, and their inverse counts
+  uint32_t lo, nrec;
+  uint64_t rb;
+  locate(lc, lo, rb, nrec);
+  uint32_t my_row = 0, my_col = 0;
+  C my_x = 0, my_ia = 0, my_ib = 0;
+  if (lane < nrec) {
+    my_row = a.row[rb + lane];
+    my_col = a.col[rb + lane];
+    my_x = vals[rb + lane];
+    if (weighted) {
+      my_ia = inv1[my_row];
+      my_ib = inv2[my_col];
+    }
+  }
+  for (;;) {
+    // the next chunk's entries travel while this chunk is updated
+    const uint32_t nlc = lc + stride;
+    uint32_t nlo = 0, nnrec = 0;
+    uint64_t nrb = 0;
+    uint32_t n_row = 0, n_col = 0;
+    C n_x = 0;
+    if (nlc < total) {
+      locate(nlc, nlo, nrb, nnrec);
+      if (lane < nnrec) {
+        n_row = a.row[nrb + lane];
+        n_col = a.col[nrb + lane];
+        n_x = vals[nrb + lane];
+      }
+    }
+
     const C eps = (C)seg[lo].eps, f2 = eps * lambda2;
     const C cwh = (C)seg[lo].cwh;
     const C rw = (C)(a.swap_sides ? seg[lo].rho_h : seg[lo].rho_w);
     const C rh = (C)(a.swap_sides ? seg[lo].rho_w : seg[lo].rho_h);
-
-    uint32_t my_row = 0, my_col = 0;
-    C my_x = 0, my_a = 0, my_b = 0;
-    if (lane < nrec) {
-      my_row = a.row[rb + lane];
-      my_col = a.col[rb + lane];
-      my_x = vals[rb + lane];
-      if (a.update == kUpdNzslL2) {
-        my_a = f2 * inv1[my_row];
-        my_b = f2 * inv2[my_col];
-      } else if (a.update == kUpdNzslNzl2) {
-        my_a = f2;
-        my_b = f2;
-      }
+    C my_a = 0, my_b = 0;
+    if (weighted) {
+      my_a = f2 * my_ia;
+      my_b = f2 * my_ib;
+    } else if (a.update == kUpdNzslNzl2) {
+      my_a = f2;
+      my_b = f2;
     }
-
     // stochastic rounding: one Philox block per chunk and lane (counter:
     // first record of the chunk, epoch, lane; key: the epoch's key)
     Philox4 base{};
     if constexpr (kSR)
       base = philox4x32_10((uint32_t)rb, (uint32_t)(rb >> 32), ep.epoch, lane, ep.key0, ep.key1);
-    if constexpr (RUNS) {
+    if constexpr (RUNS)
       run_chunk<T, LPN, VPL, ATOMIC>(a, W, H, rb, nrec, my_row, my_col, my_x, my_a, my_b, eps,
                                      cwh, rw, rh, tmin, tmax, base, grp, gl);
-    } else {
-      for (uint32_t t0 = 0; t0 < nrec; t0 += NG) {
-        const uint32_t ri = t0 + grp;
-        const uint32_t row = __shfl_sync(kFullMask, my_row, ri);
-        const uint32_t col = __shfl_sync(kFullMask, my_col, ri);
-        const C x = __shfl_sync(kFullMask, my_x, ri);
-        const C ca = __shfl_sync(kFullMask, my_a, ri);
-        const C cb = __shfl_sync(kFullMask, my_b, ri);
-        const bool valid = ri < nrec;
-        T* wp = W + (size_t)row * a.rp;
-        T* hp = H + (size_t)col * a.rp;
-        uint4 wv[VPL], hv[VPL];
-        bool live[VPL];
-  #pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-          const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-          live[v] = valid && e0 < a.rp;
-          if (live[v]) {
-            wv[v] = *reinterpret_cast<const uint4*>(wp + e0);
-            hv[v] = *reinterpret_cast<const uint4*>(hp + e0);
-          } else {
-            wv[v] = make_uint4(0, 0, 0, 0);
-            hv[v] = make_uint4(0, 0, 0, 0);
-          }
-        }
-        C dot = 0;
-        C wf[VPL][VW], hf[VPL][VW];
-  #pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-          E::unpack(wv[v], wf[v]);
-          E::unpack(hv[v], hf[v]);
-  #pragma unroll
-          for (int e = 0; e < VW; ++e) dot += wf[v][e] * hf[v][e];
-        }
-  #pragma unroll
-        for (int off = LPN / 2; off > 0; off >>= 1) dot += __shfl_xor_sync(kFullMask, dot, off);
-        const C f1 = (C)-2 * eps * (x - dot * cwh);
-        const C fw = f1 * rw, fh = f1 * rh;
-  #pragma unroll
-        for (int v = 0; v < VPL; ++v) {
-          if (!live[v]) continue;
-          C nw[VW], nh[VW];
-  #pragma unroll
-          for (int e = 0; e < VW; ++e) {
-            nw[e] = wf[v][e] - (fw * hf[v][e] + ca * wf[v][e]);
-            nh[e] = hf[v][e] - (fh * wf[v][e] + cb * hf[v][e]);
-          }
-          const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-          if (!ATOMIC && a.truncate) {
-  #pragma unroll
-            for (int e = 0; e < VW; ++e)
-              if (e0 + e < a.r) {
-                nw[e] = clampw(nw[e], tmin, tmax, eps);
-                nh[e] = clampw(nh[e], tmin, tmax, eps);
-              }
-          }
-          if constexpr (ATOMIC && !kSR) {
-            // add the update, so concurrent updates of one row are not lost
-            if constexpr (sizeof(T) == 4) {
-              atomicAdd(reinterpret_cast<float4*>(wp + e0),
-                        make_float4(nw[0] - wf[v][0], nw[1] - wf[v][1], nw[2] - wf[v][2], nw[3] - wf[v][3]));
-              atomicAdd(reinterpret_cast<float4*>(hp + e0),
-                        make_float4(nh[0] - hf[v][0], nh[1] - hf[v][1], nh[2] - hf[v][2], nh[3] - hf[v][3]));
-            } else {
-  #pragma unroll
-              for (int e = 0; e < VW; ++e) {
-                atomicAdd(reinterpret_cast<double*>(wp + e0) + e, (double)(nw[e] - wf[v][e]));
-                atomicAdd(reinterpret_cast<double*>(hp + e0) + e, (double)(nh[e] - hf[v][e]));
-              }
-            }
-          } else {
-            Philox4 r1, r2;
-            if constexpr (kSR) {  // tags: iteration t0 / NG of this group, vector v, side
-              const uint32_t tg = 2u * ((t0 / NG) * VPL + v);
-              r1 = sr_expand(base, tg);
-              r2 = sr_expand(base, tg + 1u);
-            }
-            if constexpr (ATOMIC && kSR) {
-              red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(wp + e0), wv[v], nw, r1);
-              red_bf16_increment(reinterpret_cast<__nv_bfloat16*>(hp + e0), hv[v], nh, r2);
-            } else {
-              store_vec<T>(wp + e0, nw, &r1);
-              store_vec<T>(hp + e0, nh, &r2);
-            }
-          }
-        }
-      }
+    else
+      shuffled_chunk<T, LPN, VPL, ATOMIC>(a, W, H, nrec, my_row, my_col, my_x, my_a, my_b, eps,
+                                          cwh, rw, rh, tmin, tmax, base, grp, gl);
+    if (nlc >= total) break;
+    // the next chunk's inverse counts: their round trip overlaps the first
+    // factor loads of that chunk
+    C n_ia = 0, n_ib = 0;
+    if (weighted && lane < nnrec) {
+      n_ia = inv1[n_row];
+      n_ib = inv2[n_col];
     }
+    lc = nlc;
+    lo = nlo;
+    rb = nrb;
+    nrec = nnrec;
+    my_row = n_row;
+    my_col = n_col;
+    my_x = n_x;
+    my_ia = n_ia;
+    my_ib = n_ib;
   }
 }
 
