@@ -255,7 +255,13 @@ void make_events(dsgdpp_shard* sh, ShardRank& R) {
     check_cuda(cudaEventCreateWithFlags(e, timed ? cudaEventDefault : cudaEventDisableTiming),
                "event");
   };
-  check_cuda(cudaStreamCreateWithFlags(&R.xfer, cudaStreamNonBlocking), "transfer stream");
+  // the transfer stream outranks the compute stream, so a transfer's kernel
+  // (NCCL's) takes the SMs that the running sub-epoch frees before the next
+  // sub-epoch's CTAs do
+  int least = 0, greatest = 0;
+  check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+  check_cuda(cudaStreamCreateWithPriority(&R.xfer, cudaStreamNonBlocking, greatest),
+             "transfer stream");
   mk(&R.start, false);
   R.sub_end.resize(sh->nb2);
   R.group_done.resize(sh->nb2 + 1);
