@@ -58,7 +58,8 @@ extern "C" int dsgdpp_autotune(const dsgdpp_config* base, uint64_t nnz, const ui
   if (base->exec != DSGDPP_EXEC_HOGWILD) return DSGDPP_E_UNSUPPORTED;
   std::vector<uint32_t> ds(d_candidates, d_candidates + nd);
   if (ds.empty()) ds = {64, 128, 256, 512};
-  // lane mappings: the automatic one, and half the lanes with twice the vectors
+  // lane mappings: the automatic one, and the other of (one vector per lane,
+  // two vectors per lane on half the lanes)
   const std::vector<Shape> shapes = {{0, 0, 0}, {0, 0, 4}, {0, 0, 3}};
   double top = -1;
   dsgdpp_config chosen = *base;
@@ -83,9 +84,12 @@ extern "C" int dsgdpp_autotune(const dsgdpp_config* base, uint64_t nnz, const ui
       uint32_t lanes = 0, vecs = 0, grid = 0;
       dsgdpp_launch_shape(probe, &lanes, &vecs, &grid);
       dsgdpp_destroy(probe);
-      if (lanes >= 4) {
-        c.lanes_per_nnz = lanes / 2;
-        c.vecs_per_lane = vecs * 2;
+      // the other mapping: back to one vector per lane where the automatic
+      // one takes two, else half the lanes with twice the vectors
+      const bool wide = vecs == 2 && lanes <= 16;
+      if (wide || lanes >= 4) {
+        c.lanes_per_nnz = wide ? lanes * 2 : lanes / 2;
+        c.vecs_per_lane = wide ? 1 : vecs * 2;
         const double t = time_config(c, nnz, rows, cols, vals, W, H, epochs, eps);
         if (t > 0 && (top < 0 || t < top)) {
           top = t;

@@ -129,6 +129,47 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   C h0[VPL][VW];         // ... unpacked as loaded
   C hf[VPL][VW];         // ... as updated so far
   uint32_t last_t = 0;  // the run's last record in the group (its H write tag)
+  constexpr int NG = 32 / LPN;
+  // A full chunk of one column: a hot column's records fill whole chunks.
+  // Then every group runs on the same H row and writes it back at the same
+  // steps (every kRunCap records), and with atomic writes the groups add
+  // their changes up with a butterfly and the first writes the sum: one
+  // atomic per warp and write-back instead of one per group eases the queue
+  // at that row's L2 slice.
+  // (BF16 rows are half as wide and their increments measured no gain from
+  // the summing, whose registers cost the BF16 instances spills.)
+  bool one_col = false;
+  if constexpr (ATOMIC && NG > 1 && sizeof(T) != 2)
+    one_col = nrec == (uint32_t)kChunk &&
+              __all_sync(kFullMask, my_col == __shfl_sync(kFullMask, my_col, 0));
+  // Writes back the open run of the groups with wb set; called by every lane.
+  auto write_back = [&](bool wb) {
+    if (one_col && __all_sync(kFullMask, wb)) {
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          C dsum = hf[v][e] - h0[v][e];
+#pragma unroll
+          for (int off = LPN; off < 32; off <<= 1) dsum += __shfl_xor_sync(kFullMask, dsum, off);
+          hf[v][e] = h0[v][e] + dsum;  // the run's end state with every group's changes
+        }
+        if (grp == 0 && e0 < a.rp)
+          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
+                               2u * (last_t * VPL + v) + 1u);
+      }
+    } else if (wb) {
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        if (e0 < a.rp)
+          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
+                               2u * (last_t * VPL + v) + 1u);
+      }
+    }
+    if (wb) cur = kNone;
+  };
   // write tags: record t of the group, vector v: 2 (t VPL + v) for W, + 1 for H
 #pragma unroll 1
   for (int t = 0; t < LPN; ++t) {
@@ -144,16 +185,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
     // this group at least every kRunCap records (longer runs measured less
     // stable: on the 100M-entry Zipf matrix, runs of 4 or 8 diverged within
     // 60 BoldDriver epochs where runs of 2 and the shuffled order did not)
-    if (cur != kNone && (!valid || col != cur || (t % kRunCap) == 0)) {
-#pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-        if (e0 < a.rp)
-          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
-                               2u * (last_t * VPL + v) + 1u);
-      }
-      cur = kNone;
-    }
+    write_back(cur != kNone && (!valid || col != cur || (t % kRunCap) == 0));
     if (valid && cur == kNone) {  // a run starts: load its H row
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
@@ -208,15 +240,7 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
     }
     last_t = (uint32_t)t;
   }
-  if (cur != kNone) {
-#pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
-      if (e0 < a.rp)
-        write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
-                             2u * (last_t * VPL + v) + 1u);
-    }
-  }
+  write_back(cur != kNone);
 }
 
 // Records of a chunk in the shuffled order: 32/LPN records at a time, one per
