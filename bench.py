@@ -659,35 +659,6 @@ def main():
     traffic = (traffic_per_launch(f"hogwild_subepoch_{args.workload}{suffix}.md", shape)
                if args.launch != "persistent" else None)
 
-    # ---- the precision form: the same epochs with BF16 factors ----
-    bf16 = None
-    if args.precision == "fp32" and not args.no_bf16 and args.launch != "persistent":
-        import dataclasses
-        cfg16 = dataclasses.replace(cfg, precision="bf16", lanes_per_nnz=0, vecs_per_lane=0,
-                                    ctas_per_sm=0)
-        with P.Context(cfg16) as c16:
-            c16.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
-            c16.set_factors(host["W0"], host["H0"])
-            c16.seed(args.seed)
-            for _ in range(args.warmup):
-                c16.epoch(eps)
-            ms16 = []
-            for _ in range(args.steps):
-                c16.epoch(eps)
-                ms16.append(c16.last_epoch_ms())
-            c16.set_kernel_timing(True)
-            for _ in range(2):
-                c16.epoch(eps)
-            k16, kl16 = c16.kernel_timing()
-            l16, v16, g16 = c16.launch_shape()
-        bpu16 = algorithmic_bytes_per_update(wl["rank"], "bf16", "Nzsl_L2")
-        ach16 = 2 * nnz * bpu16 / max(kl16, 1) / (k16 / 1e3 / max(kl16, 1)) / 1e9
-        bf16 = {"epoch_ms": sum(ms16) / len(ms16), "updates_per_s": nnz / (sum(ms16) / len(ms16) / 1e3),
-                "lanes_per_nnz": l16, "vecs_per_lane": v16, "grid": g16,
-                "roofline": {"bound": "hbm", "achieved": ach16, "peak": hbm, "unit": "GB/s",
-                             "frac": ach16 / hbm, "bytes_per_update": bpu16,
-                             "avg_launch_us": k16 * 1e3 / max(kl16, 1)}}
-
     # ---- end to end through the C ABI from pinned host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -732,6 +703,35 @@ def main():
                      "test_rmse": got, "rel_error": (got - ref["test_rmse"]) / ref["test_rmse"]}
 
     ctx.close()
+
+    # ---- the precision form: the same epochs with BF16 factors (FP32 context closed) ----
+    bf16 = None
+    if args.precision == "fp32" and not args.no_bf16 and args.launch != "persistent":
+        import dataclasses
+        cfg16 = dataclasses.replace(cfg, precision="bf16", lanes_per_nnz=0, vecs_per_lane=0,
+                                    ctas_per_sm=0)
+        with P.Context(cfg16) as c16:
+            c16.set_matrix(P.TRAIN, host["rows"], host["cols"], host["vals"])
+            c16.set_factors(host["W0"], host["H0"])
+            c16.seed(args.seed)
+            for _ in range(args.warmup):
+                c16.epoch(eps)
+            ms16 = []
+            for _ in range(args.steps):
+                c16.epoch(eps)
+                ms16.append(c16.last_epoch_ms())
+            c16.set_kernel_timing(True)
+            for _ in range(2):
+                c16.epoch(eps)
+            k16, kl16 = c16.kernel_timing()
+            l16, v16, g16 = c16.launch_shape()
+        bpu16 = algorithmic_bytes_per_update(wl["rank"], "bf16", "Nzsl_L2")
+        ach16 = 2 * nnz * bpu16 / max(kl16, 1) / (k16 / 1e3 / max(kl16, 1)) / 1e9
+        bf16 = {"epoch_ms": sum(ms16) / len(ms16), "updates_per_s": nnz / (sum(ms16) / len(ms16) / 1e3),
+                "lanes_per_nnz": l16, "vecs_per_lane": v16, "grid": g16,
+                "roofline": {"bound": "hbm", "achieved": ach16, "peak": hbm, "unit": "GB/s",
+                             "frac": ach16 / hbm, "bytes_per_update": bpu16,
+                             "avg_launch_us": k16 * 1e3 / max(kl16, 1)}}
 
     # ---- time to target test RMSE: BF16 + learned controller vs plain FP32 ----
     ttt = None
