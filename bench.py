@@ -764,8 +764,10 @@ def main():
                          "kernel": ("hogwild_epoch_kernel" if args.launch == "persistent"
                                     else "hogwild_subepoch_kernel"),
                          "avg_launch_us": avg_launch_s * 1e6,
-                         "timing": "CUDA events around each sub-epoch launch of 2 epochs "
-                                   "launched on the library stream (not from the graph)"},
+                         "timing": ("CUDA events around each one-launch epoch of 2 epochs"
+                                    if args.launch == "persistent" else
+                                    "CUDA events around each sub-epoch launch of 2 epochs "
+                                    "launched on the library stream (not from the graph)")},
             "cpu_baseline": cpu,
             "test_rmse_vs_fp64_oracle": vs_oracle,
             "bf16_factors": bf16,
