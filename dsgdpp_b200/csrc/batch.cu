@@ -366,7 +366,8 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
       throw Error(DSGDPP_E_INVALID, "no Hogwild kernel for lanes_per_nnz=" +
                                         std::to_string(G.lanes) + ", vecs_per_lane=" +
                                         std::to_string(G.vecs));
-    if (common->ctas_per_sm) per_sm = std::min<int>(per_sm, (int)common->ctas_per_sm);
+    if (common->ctas_per_sm)  // counted in CTAs of 256 threads
+      per_sm = std::min<int>(per_sm, (int)common->ctas_per_sm * hogwild_cta_scale(prec));
     G.grid = (uint32_t)per_sm * (uint32_t)b->num_sms;
   }
   b->nsegs = seg;

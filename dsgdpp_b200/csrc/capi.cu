@@ -95,7 +95,11 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
     per_sm = hogwild_epoch_ctas_per_sm(c->cfg.precision, lanes, vecs, c->nb2);
     if (per_sm <= 0) throw Error(DSGDPP_E_INVALID, "no persistent epoch kernel for this rank");
   }
-  if (c->cfg.ctas_per_sm) per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm);
+  if (c->cfg.ctas_per_sm) {  // counted in CTAs of 256 threads
+    const int scale =
+        c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT ? 1 : hogwild_cta_scale(c->cfg.precision);
+    per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm * scale);
+  }
   c->grid = (uint32_t)(per_sm * c->num_sms);
 }
 

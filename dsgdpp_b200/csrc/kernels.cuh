@@ -91,6 +91,15 @@ struct EpochDeps {
   uint64_t wait_ns;        // a dependency wait gives up after this long
 };
 
+// Threads per CTA of the Hogwild sub-epoch kernel: 128 for FP32 and FP64
+// (finer register allocation: 72 registers fit 28 warps per SM in CTAs of 4
+// warps, 24 in CTAs of 8; measured 6.9 against 7.5 ms per epoch at rank 32),
+// 256 for BF16 (its 64-register instances fit 32 warps either way; 128
+// measured 1-2% slower).  A cap of CTAs per SM in a configuration counts CTAs
+// of 256 threads, so it is scaled by hogwild_cta_scale.
+constexpr int hogwild_threads(int precision) { return precision == kBf16 ? 256 : 128; }
+constexpr int hogwild_cta_scale(int precision) { return 256 / hogwild_threads(precision); }
+
 // ---- launchers (return cudaError_t) -------------------------------------------
 cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);
 cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,

@@ -339,7 +339,9 @@ __device__ __forceinline__ void shuffled_chunk(const HogwildArgs& a, T* W, T* H,
 // of spill, and the rank-128 FP32 epoch 23.4 -> 21.6 ms).  Two vectors per
 // lane stay unconstrained (5 CTAs per SM measured slower at rank 32).
 template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM, bool RUNS>
-__global__ void __launch_bounds__(256, VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeof(T) == 4 ? 5 : 1)
+__global__ void __launch_bounds__(sizeof(T) == 2 ? 256 : 128,
+                                  (sizeof(T) == 2 ? 1 : 2) *
+                                      (VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeof(T) == 4 ? 5 : 1))
     hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
@@ -906,7 +908,8 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomi
   void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, smem_segs > 0, runs);
   if (!fn) return 0;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 256, sizeof(Segment) * smem_segs) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, hogwild_threads(precision),
+                                                    sizeof(Segment) * smem_segs) !=
       cudaSuccess)
     return 0;
   return n;
@@ -920,7 +923,8 @@ cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const H
   HogwildArgs args = a;
   uint32_t li = launch_index;
   void* params[] = {&args, &li};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(256), params, sizeof(Segment) * a.smem_segs, st);
+  return cudaLaunchKernel(fn, dim3(grid), dim3(hogwild_threads(precision)), params,
+                          sizeof(Segment) * a.smem_segs, st);
 }
 
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st) {

@@ -113,7 +113,8 @@ typedef struct dsgdpp_config {
   int32_t device;         /* CUDA device ordinal */
   uint32_t lanes_per_nnz; /* Hogwild lanes per record: 0 = auto, else 2..32 */
   uint32_t vecs_per_lane; /* Hogwild 16-byte vectors per lane: 0 = auto */
-  uint32_t ctas_per_sm;   /* Hogwild CTAs per SM: 0 = occupancy limit */
+  uint32_t ctas_per_sm;   /* Hogwild CTAs of 256 threads per SM (FP32/FP64 launch CTAs of
+                             128, twice as many): 0 = occupancy limit */
   uint64_t layout_seed;   /* seeds the one-off shuffle of the Hogwild record layout */
   int32_t write_mode;     /* Hogwild factor writes: DSGDPP_WRITE_* */
   int32_t layout;         /* Hogwild record order in a block: DSGDPP_LAYOUT_* */

@@ -108,6 +108,11 @@ def _zipf_case(r):
     return _cache[r]
 
 
+def _threads(precision):
+    """Threads per CTA of the sub-epoch kernel."""
+    return 256 if precision == "bf16" else 128
+
+
 def _auto_shape(precision, r):
     """The lane mapping the library picks by itself for this rank."""
     p = _Data(64, 64, {})
@@ -137,8 +142,8 @@ def test_hogwild_benchmarked_shapes_track_fp64_oracle(r, precision, half, ctas):
                   lanes_per_nnz=lanes, vecs_per_lane=vecs, ctas_per_sm=ctas) as ctx:
         got_lanes, got_vecs, grid = ctx.launch_shape()
         assert (got_lanes, got_vecs) == (lanes, vecs)
-        if ctas:
-            assert grid <= ctas * 148
+        if ctas:  # a cap counts CTAs of 256 threads (FP32 CTAs hold 128)
+            assert grid * _threads(precision) <= ctas * 256 * 148
         ctx.seed(3)
         trace = ctx.run(EPOCHS, "BoldDriver", EPS0)
     got = float(np.sqrt(trace[-1]["test_loss"] / NTEST))
@@ -149,12 +154,13 @@ def test_hogwild_benchmarked_shapes_track_fp64_oracle(r, precision, half, ctas):
 
 
 def test_benchmark_autotuned_instance_tracks_fp64_oracle():
-    # the instance the 100M-entry benchmark line ran: FP32, rank 32, 4 lanes x
-    # 2 vectors per entry, 3 CTAs per SM (grid 444 on 148 SMs)
+    # the instance the 100M-entry benchmark line runs: FP32, rank 32, 4 lanes x
+    # 2 vectors per entry, 7 CTAs of 128 threads per SM (the register limit at
+    # 72 registers; grid 1036 on 148 SMs)
     p, tr = _zipf_case(32)
     with _context(p, 32, D, precision="fp32", exec="hogwild", launch="graph", layout="runs",
-                  lanes_per_nnz=4, vecs_per_lane=2, ctas_per_sm=3) as ctx:
-        assert ctx.launch_shape() == (4, 2, 3 * 148)
+                  lanes_per_nnz=4, vecs_per_lane=2) as ctx:
+        assert ctx.launch_shape() == (4, 2, 7 * 148)
         ctx.seed(3)
         trace = ctx.run(EPOCHS, "BoldDriver", EPS0)
     got = float(np.sqrt(trace[-1]["test_loss"] / NTEST))
