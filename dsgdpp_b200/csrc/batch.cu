@@ -367,7 +367,7 @@ void create_impl(dsgdpp_batch* b, const dsgdpp_config* common, uint32_t count,
                                         std::to_string(G.lanes) + ", vecs_per_lane=" +
                                         std::to_string(G.vecs));
     if (common->ctas_per_sm)  // counted in CTAs of 256 threads
-      per_sm = std::min<int>(per_sm, (int)common->ctas_per_sm * hogwild_cta_scale(prec));
+      per_sm = std::min<int>(per_sm, (int)common->ctas_per_sm * hogwild_cta_scale(prec, G.lanes));
     G.grid = (uint32_t)per_sm * (uint32_t)b->num_sms;
   }
   b->nsegs = seg;

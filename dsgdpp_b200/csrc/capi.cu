@@ -97,7 +97,7 @@ void choose_hogwild_shape(dsgdpp_ctx* c) {
   }
   if (c->cfg.ctas_per_sm) {  // counted in CTAs of 256 threads
     const int scale =
-        c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT ? 1 : hogwild_cta_scale(c->cfg.precision);
+        c->cfg.launch == DSGDPP_LAUNCH_PERSISTENT ? 1 : hogwild_cta_scale(c->cfg.precision, lanes);
     per_sm = std::min<int>(per_sm, (int)c->cfg.ctas_per_sm * scale);
   }
   c->grid = (uint32_t)(per_sm * c->num_sms);

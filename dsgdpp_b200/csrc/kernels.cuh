@@ -91,14 +91,22 @@ struct EpochDeps {
   uint64_t wait_ns;        // a dependency wait gives up after this long
 };
 
-// Threads per CTA of the Hogwild sub-epoch kernel: 128 for FP32 and FP64
-// (finer register allocation: 72 registers fit 28 warps per SM in CTAs of 4
-// warps, 24 in CTAs of 8; measured 6.9 against 7.5 ms per epoch at rank 32),
-// 256 for BF16 (its 64-register instances fit 32 warps either way; 128
-// measured 1-2% slower).  A cap of CTAs per SM in a configuration counts CTAs
-// of 256 threads, so it is scaled by hogwild_cta_scale.
-constexpr int hogwild_threads(int precision) { return precision == kBf16 ? 256 : 128; }
-constexpr int hogwild_cta_scale(int precision) { return 256 / hogwild_threads(precision); }
+// Threads per CTA of a Hogwild sub-epoch kernel instance.  Registers are
+// allocated per warp, so small CTAs pack more warps onto an SM when a
+// CTA's registers do not divide the SM's: CTAs of 4 warps for FP32 and FP64
+// (72 registers fit 28 warps per SM in CTAs of 4 warps, 24 in CTAs of 8;
+// measured 6.9 against 7.5 ms per epoch at rank 32) and for BF16 with up to
+// 4 lanes per entry (held to 73 registers without spills: 6.55 against 6.81
+// ms at rank 32); CTAs of 8 warps for wider BF16 mappings (held to 64
+// registers, 4 CTAs per SM, which measured faster at ranks 64 and 128).  A
+// cap of CTAs per SM in a configuration counts CTAs of 256 threads, so it is
+// scaled by hogwild_cta_scale.
+constexpr int hogwild_threads(int precision, uint32_t lanes) {
+  return precision == kBf16 && lanes > 4 ? 256 : 128;
+}
+constexpr int hogwild_cta_scale(int precision, uint32_t lanes) {
+  return 256 / hogwild_threads(precision, lanes);
+}
 
 // ---- launchers (return cudaError_t) -------------------------------------------
 cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);

@@ -333,15 +333,27 @@ __device__ __forceinline__ void shuffled_chunk(const HogwildArgs& a, T* W, T* H,
 // registers or shared memory measured slower on B200: the registers or shared
 // memory cost more resident warps than the prefetch gains; its entries take
 // five registers.)
-// One vector per lane: BF16 is held to 64 registers (4 CTAs per SM; 70
-// unconstrained, where 3 CTAs per SM left it latency-bound; up to 16 lanes
-// per entry the cap costs no spills), FP32 to 48 (5 CTAs per SM; a few bytes
-// of spill, and the rank-128 FP32 epoch 23.4 -> 21.6 ms).  Two vectors per
-// lane stay unconstrained (5 CTAs per SM measured slower at rank 32).
+// Register bounds: see HogwildLaunch (FP32 one vector per lane at 48
+// registers took the rank-128 FP32 epoch 23.4 -> 21.6 ms; two vectors per
+// lane stay unconstrained: capping them measured slower).
+// CTA size and register bound of an instance (hogwild_threads has the why):
+// FP32 one vector per lane held to 48 registers (10 CTAs of 128), BF16 with
+// up to 4 lanes to 73 (7 CTAs of 128), wider BF16 to 64 (4 CTAs of 256);
+// two vectors per lane unconstrained.
+template <typename T, int LPN, int VPL>
+struct HogwildLaunch {
+  static constexpr bool kBig = sizeof(T) == 2 && LPN > 4;
+  static constexpr int threads = kBig ? 256 : 128;
+  static constexpr int min_blocks = VPL != 1         ? (kBig ? 1 : 2)
+                                    : sizeof(T) == 4 ? 10
+                                    : sizeof(T) == 8 ? 2
+                                    : kBig           ? 4
+                                                     : 7;
+};
+
 template <typename T, int LPN, int VPL, bool ATOMIC, bool SMEM, bool RUNS>
-__global__ void __launch_bounds__(sizeof(T) == 2 ? 256 : 128,
-                                  (sizeof(T) == 2 ? 1 : 2) *
-                                      (VPL != 1 ? 1 : sizeof(T) == 2 ? 4 : sizeof(T) == 4 ? 5 : 1))
+__global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
+                                  HogwildLaunch<T, LPN, VPL>::min_blocks)
     hogwild_subepoch_kernel(HogwildArgs a, uint32_t li) {
   using E = Elem<T>;
   using C = typename E::C;
@@ -908,7 +920,7 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomi
   void* fn = hogwild_kernel_ptr(precision, lanes, vecs, atomic, smem_segs > 0, runs);
   if (!fn) return 0;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, hogwild_threads(precision),
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, hogwild_threads(precision, lanes),
                                                     sizeof(Segment) * smem_segs) !=
       cudaSuccess)
     return 0;
@@ -923,7 +935,7 @@ cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const H
   HogwildArgs args = a;
   uint32_t li = launch_index;
   void* params[] = {&args, &li};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(hogwild_threads(precision)), params,
+  return cudaLaunchKernel(fn, dim3(grid), dim3(hogwild_threads(precision, lanes)), params,
                           sizeof(Segment) * a.smem_segs, st);
 }
 

@@ -108,9 +108,9 @@ def _zipf_case(r):
     return _cache[r]
 
 
-def _threads(precision):
-    """Threads per CTA of the sub-epoch kernel."""
-    return 256 if precision == "bf16" else 128
+def _threads(precision, lanes):
+    """Threads per CTA of the sub-epoch kernel instance."""
+    return 256 if precision == "bf16" and lanes > 4 else 128
 
 
 def _auto_shape(precision, r):
@@ -143,7 +143,7 @@ def test_hogwild_benchmarked_shapes_track_fp64_oracle(r, precision, half, ctas):
         got_lanes, got_vecs, grid = ctx.launch_shape()
         assert (got_lanes, got_vecs) == (lanes, vecs)
         if ctas:  # a cap counts CTAs of 256 threads (FP32 CTAs hold 128)
-            assert grid * _threads(precision) <= ctas * 256 * 148
+            assert grid * _threads(precision, lanes) <= ctas * 256 * 148
         ctx.seed(3)
         trace = ctx.run(EPOCHS, "BoldDriver", EPS0)
     got = float(np.sqrt(trace[-1]["test_loss"] / NTEST))
