@@ -239,11 +239,15 @@ def _synth_gpu():
     return mod
 
 
-def arm_oracle_errors(P, data, wl, arms, epochs, device, layout, threads=None):
-    """Test RMSE error against the FP64 oracle of every time-to-target arm:
-    on the CPU baseline's sample, each arm's first `epochs` step sizes run on
-    the oracle (FP64, sequential per block) and on this implementation in the
-    arm's precision, with the same d, seed and schedules."""
+def arm_oracle_errors(P, data, wl, arms, epochs, device, layout, net=None, threads=None):
+    """Test RMSE error against the FP64 oracle of every time-to-target arm, on
+    the CPU baseline's sample: the arm runs its own step rule there for
+    `epochs` decisions in its precision (BoldDriver(0.001), or the controller
+    with its rollbacks), and the oracle (FP64, sequential per block) replays
+    the steps the arm kept, with the same d and seed.  (Steps chosen on the
+    full workload are not replayed on the sample: a step the controller kept
+    there can be past the sample's stable range, where BF16 Hogwild and the
+    sequential oracle part ways.)"""
     from oracle import oracle as O
     threads = threads or os.cpu_count() or 1
     rows, cols, vals = cpu_sample(data, CPU_SAMPLE)
@@ -256,12 +260,6 @@ def arm_oracle_errors(P, data, wl, arms, epochs, device, layout, threads=None):
     ntest = len(data["tvals"])
     out = {}
     for name, arm in arms.items():
-        steps = [e for e in arm["eps"] if np.isfinite(e)][:epochs]
-        prob.set_factors(data["W0"], data["H0"])
-        prob.seed(1)
-        for eps in steps:
-            prob.epoch(eps, threads=threads)
-        want = float(np.sqrt(prob.nzsl(1) / ntest))
         cfg = P.Config(m=wl["m"], n=wl["n"], rank=wl["rank"], d=threads,
                        precision=arm["precision"], device=device, layout=layout, **conf)
         with P.Context(cfg) as ctx:
@@ -269,14 +267,23 @@ def arm_oracle_errors(P, data, wl, arms, epochs, device, layout, threads=None):
             ctx.set_matrix(P.TEST, data["trows"], data["tcols"], data["tvals"])
             ctx.set_factors(data["W0"], data["H0"])
             ctx.seed(1)
-            for eps in steps:
-                ctx.epoch(eps)
-            got = float(np.sqrt(ctx.nzsl(P.TEST) / ntest))
-        out[name] = {"precision": arm["precision"], "epochs": len(steps),
-                     "oracle_fp64_test_rmse": want, "test_rmse": got,
+            if arm["controller"]:
+                trace, fallbacks = ctx.run_controlled(net, epochs, 0.001)
+            else:
+                trace, fallbacks = ctx.run(epochs, "BoldDriver", 0.001), None
+            got = float(np.sqrt(trace[-1]["test_loss"] / ntest))
+        steps = [row["eps"] for row in trace[1:]]
+        prob.set_factors(data["W0"], data["H0"])
+        prob.seed(1)
+        for eps in steps:
+            prob.epoch(eps, threads=threads)
+        want = float(np.sqrt(prob.nzsl(1) / ntest))
+        out[name] = {"precision": arm["precision"], "epochs": len(steps), "steps": steps,
+                     "fallbacks": fallbacks, "oracle_fp64_test_rmse": want, "test_rmse": got,
                      "rel_error": (got - want) / want}
     return {"sample": f"{len(vals):,} entries of the workload (the CPU baseline's sample), "
-                      f"d={threads}, each arm's first step sizes", "arms": out}
+                      f"d={threads}; each arm's own step rule for {epochs} decisions, "
+                      "the oracle replaying the steps it kept", "arms": out}
 
 
 def time_to_target_leg(P, wl, data, d, args, local, seed_note):
@@ -288,7 +295,6 @@ def time_to_target_leg(P, wl, data, d, args, local, seed_note):
     net.params = np.load(TT.PARAMS)
     r = TT.evaluate(P, wl, data, d, epochs=50, eps0=0.001, net=net, device=local,
                     layout=args.layout)
-    net.close()
     leg = {"workload": wl["text"], "data_seed": seed_note,
            "target": "plain FP32 BoldDriver's test RMSE after 50 epochs, +0.5%",
            "target_test_rmse": r["target_test_rmse"], "plain_fp32_s": r["plain_fp32_s_traced"]}
@@ -296,12 +302,13 @@ def time_to_target_leg(P, wl, data, d, args, local, seed_note):
         leg[k] = {q: r[k][q] for q in ("epochs_to_target", "seconds_to_target",
                                         "ratio_to_plain", "fallbacks", "final_test_rmse")}
     if not args.no_cpu_baseline:
-        arms = {k: r[k] for k in ("plain_fp32", "bf16_bolddriver", "fp32_controller",
-                                  "bf16_controller")}
-        errs = arm_oracle_errors(P, data, wl, arms, 4, local, args.layout)
+        arms = {k: {"precision": r[k]["precision"], "controller": k.endswith("controller")}
+                for k in ("plain_fp32", "bf16_bolddriver", "fp32_controller", "bf16_controller")}
+        errs = arm_oracle_errors(P, data, wl, arms, 4, local, args.layout, net=net)
         leg["vs_fp64_oracle"] = errs
         for k, v in errs["arms"].items():
             leg.setdefault(k, {})["test_rmse_rel_error_vs_fp64_oracle"] = v["rel_error"]
+    net.close()
     return leg
 
 

@@ -350,27 +350,29 @@ void post_group(dsgdpp_shard* sh, const Plan& plan, uint32_t g) {
     return;
   }
   // emulated ranks: the receiver's transfer stream copies once both ranks are
-  // past the sub-epoch that last used the block
-  for (auto& R : sh->ranks) {
-    R.group_used[g] = 0;  // the copies run on the receivers' transfer streams
-    for (const Move& m : moves) R.group_used[g] |= m.dst == R.rank;
-    if (sh->timeline) check_cuda(cudaEventRecord(R.tx0[g], R.xfer), "event");
-  }
-  for (const Move& m : moves) {
-    ShardRank& S = sh->ranks[m.src];
-    ShardRank& D = sh->ranks[m.dst];
-    cudaEvent_t after = g == 0 ? S.start : S.sub_end[g - 1];
-    check_cuda(cudaStreamWaitEvent(D.xfer, after, 0), "transfer wait");
-    size_t bytes = 0;
-    const char* from = h_block(S.ctx, m.b2, &bytes);
-    char* to = h_block(D.ctx, m.b2, &bytes);
-    check_cuda(cudaMemcpyAsync(to, from, bytes, cudaMemcpyDeviceToDevice, D.xfer), "block copy");
-    sh->moved_bytes += bytes;
-    sh->moves += 1;
-  }
-  for (auto& R : sh->ranks) {
-    if (sh->timeline) check_cuda(cudaEventRecord(R.tx1[g], R.xfer), "event");
-    check_cuda(cudaEventRecord(R.group_done[g], R.xfer), "event");
+  // past the sub-epoch that last used the block (the timeline's start is
+  // taken after those waits, when the copies can begin)
+  for (auto& D : sh->ranks) {
+    D.group_used[g] = 0;  // the copies run on the receivers' transfer streams
+    for (const Move& m : moves) {
+      if (m.dst != D.rank) continue;
+      const ShardRank& S = sh->ranks[m.src];
+      check_cuda(cudaStreamWaitEvent(D.xfer, g == 0 ? S.start : S.sub_end[g - 1], 0),
+                 "transfer wait");
+      D.group_used[g] = 1;
+    }
+    if (sh->timeline) check_cuda(cudaEventRecord(D.tx0[g], D.xfer), "event");
+    for (const Move& m : moves) {
+      if (m.dst != D.rank) continue;
+      size_t bytes = 0;
+      const char* from = h_block(sh->ranks[m.src].ctx, m.b2, &bytes);
+      char* to = h_block(D.ctx, m.b2, &bytes);
+      check_cuda(cudaMemcpyAsync(to, from, bytes, cudaMemcpyDeviceToDevice, D.xfer), "block copy");
+      sh->moved_bytes += bytes;
+      sh->moves += 1;
+    }
+    if (sh->timeline) check_cuda(cudaEventRecord(D.tx1[g], D.xfer), "event");
+    check_cuda(cudaEventRecord(D.group_done[g], D.xfer), "event");
   }
 }
 
