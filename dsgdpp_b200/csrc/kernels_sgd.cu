@@ -136,10 +136,12 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
   // their changes up with a butterfly and the first writes the sum: one
   // atomic per warp and write-back instead of one per group eases the queue
   // at that row's L2 slice.
-  // (BF16 rows are half as wide and their increments measured no gain from
-  // the summing, whose registers cost the BF16 instances spills.)
+  // BF16 sums too where a group spans at most 4 lanes (rank 32 and below):
+  // there it measured slightly faster and kept a hot column's row stable at
+  // large steps, where one rounded increment per group drifts; the wider BF16
+  // mappings (ranks 64 and 128) measured slower with it.
   bool one_col = false;
-  if constexpr (ATOMIC && NG > 1 && sizeof(T) != 2)
+  if constexpr (ATOMIC && NG > 1 && (sizeof(T) != 2 || LPN <= 4))
     one_col = nrec == (uint32_t)kChunk &&
               __all_sync(kFullMask, my_col == __shfl_sync(kFullMask, my_col, 0));
   // Writes back the open run of the groups with wb set; called by every lane.
@@ -148,15 +150,22 @@ __device__ __forceinline__ void run_chunk(const HogwildArgs& a, T* W, T* H, uint
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const uint32_t e0 = (uint32_t)(v * LPN + gl) * VW;
+        C hb[VW];  // the run's base (BF16: unpacked again rather than kept live)
+        if constexpr (sizeof(T) == 2) {
+          E::unpack(hv0[v], hb);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VW; ++e) hb[e] = h0[v][e];
+        }
 #pragma unroll
         for (int e = 0; e < VW; ++e) {
-          C dsum = hf[v][e] - h0[v][e];
+          C dsum = hf[v][e] - hb[e];
 #pragma unroll
           for (int off = LPN; off < 32; off <<= 1) dsum += __shfl_xor_sync(kFullMask, dsum, off);
-          hf[v][e] = h0[v][e] + dsum;  // the run's end state with every group's changes
+          hf[v][e] = hb[e] + dsum;  // the run's end state with every group's changes
         }
         if (grp == 0 && e0 < a.rp)
-          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], h0[v], hf[v], base,
+          write_vec<T, ATOMIC>(H + (size_t)cur * a.rp + e0, hv0[v], hb, hf[v], base,
                                2u * (last_t * VPL + v) + 1u);
       }
     } else if (wb) {
