@@ -206,7 +206,7 @@ void create_impl(dsgdpp_ctx* c, const dsgdpp_config* cfg) {
   // of the context is reduced in the same order
   const int loss_per_sm = nzsl_ctas_per_sm(cfg->precision, c->rp);
   c->loss_grid = (uint32_t)c->num_sms * (uint32_t)std::max(2, std::min(8, loss_per_sm));
-  c->d_partials = dalloc<double>(2 * (size_t)c->loss_grid, "partials");
+  c->d_partials = dalloc<double>(3 * (size_t)c->loss_grid, "partials");
   c->d_out = dalloc<double>(4, "loss out");
   c->h_out = halloc<double>(4, "loss out");
   check_cuda(cudaEventCreate(&c->ev_begin), "event");
@@ -838,15 +838,37 @@ double finish_sum(dsgdpp_ctx* c, uint32_t count) {
   return c->h_out[0];
 }
 
-double nzsl_impl(dsgdpp_ctx* c, int which) {
+// Sums n consecutive runs of loss_grid partials into d_out[0..n) and reads
+// them back with one copy and one synchronisation.
+void finish_sums(dsgdpp_ctx* c, uint32_t n, double* out) {
+  for (uint32_t k = 0; k < n; ++k)
+    check_cuda(launch_sum_partials(c->d_partials + (size_t)k * c->loss_grid, c->loss_grid,
+                                   c->d_out + k, c->stream), "sum_partials");
+  check_cuda(cudaMemcpyAsync(c->h_out, c->d_out, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream),
+             "D2H");
+  check_cuda(cudaStreamSynchronize(c->stream), "sync");
+  for (uint32_t k = 0; k < n; ++k) out[k] = c->h_out[k];
+}
+
+// The squared errors of the training or test entries as loss_grid partials.
+void nzsl_partials(dsgdpp_ctx* c, int which, double* partials) {
   if (which != DSGDPP_TRAIN && which != DSGDPP_TEST) throw Error(DSGDPP_E_INVALID, "which");
   const DevMatrix& M = c->mat[which];
   if (!M.present) throw Error(DSGDPP_E_STATE, which ? "no test matrix" : "no training matrix");
   check_cuda(cudaSetDevice(c->cfg.device), "cudaSetDevice");
-  if (M.nnz == 0) return 0.0;
+  if (M.nnz == 0) {
+    check_cuda(cudaMemsetAsync(partials, 0, sizeof(double) * c->loss_grid, c->stream), "memset");
+    return;
+  }
   check_cuda(launch_nzsl_partials(c->cfg.precision, M.row, M.col, M.val, M.nnz, c->W, c->H, c->r,
-                                  c->rp, c->d_partials, c->loss_grid, c->stream), "nzsl");
-  return finish_sum(c, c->loss_grid);
+                                  c->rp, partials, c->loss_grid, c->stream), "nzsl");
+}
+
+double nzsl_impl(dsgdpp_ctx* c, int which) {
+  nzsl_partials(c, which, c->d_partials);
+  double v = 0;
+  finish_sums(c, 1, &v);
+  return v;
 }
 
 double sumsq_impl(dsgdpp_ctx* c, const void* X, uint64_t count) {
@@ -861,17 +883,29 @@ double nzl2_impl(dsgdpp_ctx* c, const void* X, uint64_t rows, const uint32_t* cn
   return finish_sum(c, c->loss_grid);
 }
 
+// The configured loss (mf/loss/loss.h:88-112 SumLoss of Nzsl and L2/Nzl2):
+// its two or three reductions run back to back and come back in one copy.
 double loss_impl(dsgdpp_ctx* c) {
-  double l = nzsl_impl(c, DSGDPP_TRAIN);
+  const uint32_t G = c->loss_grid;
+  nzsl_partials(c, DSGDPP_TRAIN, c->d_partials);
+  uint32_t n = 1;
   if (c->cfg.loss == DSGDPP_LOSS_NZSL_L2) {
-    const double w = sumsq_impl(c, c->W, c->cfg.m * c->rp);
-    const double h = sumsq_impl(c, c->H, c->cfg.n * c->rp);
-    l = l + c->cfg.loss_lambda * (w + h);
+    check_cuda(launch_sumsq_partials(c->cfg.precision, c->W, c->cfg.m * c->rp, c->d_partials + G,
+                                     G, c->stream), "l2");
+    check_cuda(launch_sumsq_partials(c->cfg.precision, c->H, c->cfg.n * c->rp,
+                                     c->d_partials + 2 * (size_t)G, G, c->stream), "l2");
+    n = 3;
   } else if (c->cfg.loss == DSGDPP_LOSS_NZSL_NZL2) {
-    const double w = nzl2_impl(c, c->W, c->cfg.m, c->cnt1);
-    const double h = nzl2_impl(c, c->H, c->cfg.n, c->cnt2);
-    l = l + c->cfg.loss_lambda * (w + h);
+    check_cuda(launch_nzl2_partials(c->cfg.precision, c->W, c->cfg.m, c->rp, c->cnt1,
+                                    c->d_partials + G, G, c->stream), "nzl2");
+    check_cuda(launch_nzl2_partials(c->cfg.precision, c->H, c->cfg.n, c->rp, c->cnt2,
+                                    c->d_partials + 2 * (size_t)G, G, c->stream), "nzl2");
+    n = 3;
   }
+  double v[3] = {0, 0, 0};
+  finish_sums(c, n, v);
+  double l = v[0];
+  if (n == 3) l = l + c->cfg.loss_lambda * (v[1] + v[2]);
   return l;
 }
 
