@@ -69,8 +69,22 @@ __global__ void __launch_bounds__(256) nzsl_partials_kernel(const uint32_t* row,
 // sums its elements in z order and the group adds the lane sums by a fixed
 // butterfly.  Entries [begin, end) are dealt to warps warp, warp + nwarps, ...
 // 32 at a time; a warp loads its next 32 entries before it sums the current
-// ones (training loss at rank 32: 2.97 -> 2.30 ms FP32, 2.21 -> 2.10 ms BF16
-// on 100M entries, with the register bounds of nzsl_lanes_kernel)
+// ones.  Training loss on 100M entries at rank 32: 2.97 -> 2.30 ms (FP32) and
+// 2.21 -> 2.10 ms (BF16) with the entries in flight, then 2.15 and 1.83 ms
+// with H built by f32_scaled (99M entries at rank 128: 8.17 -> 6.97 ms FP32,
+// 6.81 -> 5.05 ms BF16).
+// f * 2^-896 as a double, exactly, built from the float's bits with integer
+// operations: the 8-bit exponent field and 23-bit fraction move into the low
+// bits of the double's exponent field and the top of its fraction, so an
+// exponent field e reads as 2^(e-1023) where the float meant 2^(e-127) --
+// for normal and subnormal floats alike.  The conversion unit, which bounds
+// the loss kernels (two conversions per product), then converts only W.
+__device__ __forceinline__ double f32_scaled(float f) {
+  const uint32_t b = __float_as_uint(f);
+  const uint32_t hi = ((b >> 3) & 0x0fffffffu) | (b & 0x80000000u);
+  return __hiloint2double((int)hi, (int)(b << 29));
+}
+
 template <typename T, int LPN, int VPL>
 __device__ __forceinline__ double nzsl_lanes(const uint32_t* row, const uint32_t* col,
                                              const float* val, const T* W, const T* H,
@@ -134,12 +148,22 @@ __device__ __forceinline__ double nzsl_lanes(const uint32_t* row, const uint32_t
           E::unpack(wv[u][v], wf);
           E::unpack(hv[u][v], hf);
           const uint32_t z0 = (v * LPN + gl) * VW;
+          // The product of two floats is exact in FP64, so the fused
+          // multiply-add rounds exactly like the separate add.  The sum is
+          // formed with H scaled by 2^-896 and scaled back once: a power of
+          // two, so it rounds exactly as unscaled wherever the scaled terms
+          // stay normal doubles (magnitudes of 2^-126 and up; below that the
+          // absolute error stays under 2^-178).
+          if (z0 + VW <= r) {
 #pragma unroll
-          for (int e = 0; e < VW; ++e)
-            // the product of two floats is exact in FP64, so the fused
-            // multiply-add rounds exactly like the separate add
-            if (z0 + e < r) ip = fma((double)wf[e], (double)hf[e], ip);
+            for (int e = 0; e < VW; ++e) ip = fma((double)wf[e], f32_scaled(hf[e]), ip);
+          } else {
+#pragma unroll
+            for (int e = 0; e < VW; ++e)
+              if (z0 + e < r) ip = fma((double)wf[e], f32_scaled(hf[e]), ip);
+          }
         }
+        ip = __dmul_rn(ip, 0x1p896);
 #pragma unroll
         for (int off = LPN / 2; off > 0; off >>= 1)
           ip = __dadd_rn(ip, __shfl_xor_sync(kFullMask, ip, off));
@@ -154,10 +178,8 @@ __device__ __forceinline__ double nzsl_lanes(const uint32_t* row, const uint32_t
   return acc;
 }
 
-// FP32 instances are bounded loosely (the compiler then takes 80 registers
-// without spills at rank 32, 3 CTAs per SM; held to 85 it spilled); BF16 to 85.
 template <typename T, int LPN, int VPL>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 3)
+__global__ void __launch_bounds__(256, 3)
     nzsl_lanes_kernel(const uint32_t* row, const uint32_t* col, const float* val, uint64_t nnz,
                       const T* W, const T* H, uint32_t r, uint32_t rp, double* partials) {
   __shared__ double sh[32];
