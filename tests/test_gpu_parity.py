@@ -142,6 +142,39 @@ def test_loss_parity_fp32_and_bf16_factors():
             assert ctx.loss() == pytest.approx(ref.loss(), rel=LOSS_RTOL)
 
 
+def _extreme(rng, shape):
+    """Factor values over the whole float range: zeros, subnormals, tiny,
+    ordinary and large magnitudes, both signs."""
+    kind = rng.choice(5, size=shape, p=[0.2, 0.1, 0.1, 0.58, 0.02])
+    mag = np.select([kind == 0, kind == 1, kind == 2, kind == 3, kind == 4],
+                    [0.0, rng.uniform(1e-42, 1e-39, shape), rng.uniform(1e-22, 1e-18, shape),
+                     rng.uniform(0.0, 2.0, shape), rng.uniform(1e3, 1e4, shape)])
+    return mag * rng.choice([-1.0, 1.0], size=shape)
+
+
+@pytest.mark.parametrize("r", [7, 32, 100])
+def test_loss_parity_extreme_factor_values(r):
+    # the FP32/BF16 loss kernels form exact FP64 products (H's values built
+    # from their bits, scaled by a power of two and back): zeros, subnormal,
+    # tiny and large factor values give the oracle's loss of the same stored
+    # factors, at ranks with and without a partial last vector
+    p = _problem(m=300, n=200, nnz=6000, ntest=500, r=r)
+    p.vals = p.vals.astype(np.float32).astype(np.float64)
+    p.tvals = p.tvals.astype(np.float32).astype(np.float64)
+    rng = np.random.default_rng(r)
+    p.W0 = _extreme(rng, p.W0.shape)
+    p.H0 = _extreme(rng, p.H0.shape)
+    for prec in ("fp32", "bf16"):
+        ref, ctx = _pair(p, r, 4, precision=prec, exec="hogwild")
+        with ctx:
+            W, H = ctx.get_factors()
+            assert np.count_nonzero((W != 0) & (np.abs(W) < 1.1754944e-38)) > 0  # subnormals stored
+            ref.set_factors(W, H)
+            assert ctx.nzsl(P.TRAIN) == pytest.approx(ref.nzsl(0), rel=LOSS_RTOL)
+            assert ctx.nzsl(P.TEST) == pytest.approx(ref.nzsl(1), rel=LOSS_RTOL)
+            assert ctx.loss() == pytest.approx(ref.loss(), rel=LOSS_RTOL)
+
+
 def test_blocking_and_counts():
     p = _problem(m=1001, n=997, nnz=20000, kind="zipf")
     for d in (1, 3, 8):
