@@ -814,47 +814,65 @@ __global__ void regularize_exact_kernel(double* W, double* H, uint64_t m, uint64
   }
 }
 
-// scales[b2] scales H column block b2, scales[nb2] scales all of W
+// One 16-byte vector of factor values times s, rounded back to the storage
+// type as a store of the scaled value would be (BF16: to nearest).
 template <typename T>
-__global__ void normalize_kernel(T* W, T* H, uint64_t m, uint64_t n, uint32_t rp,
-                                 const float* scales, const uint64_t* off2, uint32_t nb2) {
-  const float sw = scales[nb2];
-  const float* sh = scales;
-  const uint64_t wtot = m * rp, htot = n * rp;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < wtot + htot; q += stride) {
-    if (q < wtot) {
-      W[q] = (T)((float)W[q] * sw);
-    } else {
-      const uint64_t hq = q - wtot, j = hq / rp;
-      uint32_t lo = 0, hi = nb2 - 1;
-      while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (off2[mid] <= j) lo = mid; else hi = mid - 1;
-      }
-      H[hq] = (T)((float)H[hq] * sh[lo]);
-    }
-  }
+__device__ __forceinline__ uint4 scale_vec(const uint4& v, float s) {
+  float f[4];
+  Elem<float>::unpack(v, f);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) f[e] *= s;
+  return Elem<float>::pack(f);
 }
 template <>
-__global__ void normalize_kernel<double>(double* W, double* H, uint64_t m, uint64_t n,
-                                         uint32_t rp, const float* scales,
-                                         const uint64_t* off2, uint32_t nb2) {
+__device__ __forceinline__ uint4 scale_vec<double>(const uint4& v, float s) {
+  double f[2];
+  Elem<double>::unpack(v, f);
+  f[0] *= (double)s;
+  f[1] *= (double)s;
+  return Elem<double>::pack(f);
+}
+template <>
+__device__ __forceinline__ uint4 scale_vec<__nv_bfloat16>(const uint4& v, float s) {
+  float f[8];
+  Elem<__nv_bfloat16>::unpack(v, f);
+  uint32_t w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const __nv_bfloat162 b = __floats2bfloat162_rn(f[2 * k] * s, f[2 * k + 1] * s);
+    w[k] = *reinterpret_cast<const uint32_t*>(&b);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// The epoch's lazy L2 scales, applied once: scales[b2] to H column block b2,
+// scales[nb2] to all of W.  16-byte vectors (rows are padded to whole
+// vectors), the column-block offsets staged in shared memory for the block
+// search of each H row.
+template <typename T>
+__global__ void __launch_bounds__(256) normalize_kernel(T* W, T* H, uint64_t m, uint64_t n,
+                                                        uint32_t rp, const float* scales,
+                                                        const uint64_t* off2, uint32_t nb2) {
+  extern __shared__ __align__(16) uint64_t s_off[];  // nb2 + 1 offsets
+  for (uint32_t k = threadIdx.x; k <= nb2; k += blockDim.x) s_off[k] = off2[k];
+  __syncthreads();
   const float sw = scales[nb2];
-  const float* sh = scales;
-  const uint64_t wtot = m * rp, htot = n * rp;
+  const uint32_t vpr = rp / (16 / sizeof(T));  // vectors per row
+  const uint64_t wv = m * vpr, tot = wv + n * vpr;
+  uint4* Wv = reinterpret_cast<uint4*>(W);
+  uint4* Hv = reinterpret_cast<uint4*>(H);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < wtot + htot; q += stride) {
-    if (q < wtot) {
-      W[q] *= (double)sw;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < tot; q += stride) {
+    if (q < wv) {
+      Wv[q] = scale_vec<T>(Wv[q], sw);
     } else {
-      const uint64_t hq = q - wtot, j = hq / rp;
-      uint32_t lo = 0, hi = nb2 - 1;
+      const uint64_t hq = q - wv, j = hq / vpr;
+      uint32_t lo = 0, hi = nb2 - 1;  // the last block with off2[b] <= j
       while (lo < hi) {
-        uint32_t mid = (lo + hi + 1) >> 1;
-        if (off2[mid] <= j) lo = mid; else hi = mid - 1;
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= j) lo = mid; else hi = mid - 1;
       }
-      H[hq] *= (double)sh[lo];
+      Hv[hq] = scale_vec<T>(Hv[hq], scales[lo]);
     }
   }
 }
@@ -969,14 +987,15 @@ cudaError_t launch_regularize_exact(double* W, double* H, uint64_t m, uint64_t n
 cudaError_t launch_normalize(int precision, void* W, void* H, uint64_t m, uint64_t n,
                              uint32_t rp, const float* scales, const uint64_t* off2,
                              uint32_t nb2, cudaStream_t st) {
+  const size_t smem = sizeof(uint64_t) * (nb2 + 1);
   if (precision == kFp64)
-    normalize_kernel<double><<<1184, 256, 0, st>>>((double*)W, (double*)H, m, n, rp, scales,
-                                                    off2, nb2);
+    normalize_kernel<double><<<1184, 256, smem, st>>>((double*)W, (double*)H, m, n, rp, scales,
+                                                       off2, nb2);
   else if (precision == kFp32)
-    normalize_kernel<float><<<1184, 256, 0, st>>>((float*)W, (float*)H, m, n, rp, scales, off2,
-                                                   nb2);
+    normalize_kernel<float><<<1184, 256, smem, st>>>((float*)W, (float*)H, m, n, rp, scales, off2,
+                                                      nb2);
   else
-    normalize_kernel<__nv_bfloat16><<<1184, 256, 0, st>>>(
+    normalize_kernel<__nv_bfloat16><<<1184, 256, smem, st>>>(
         (__nv_bfloat16*)W, (__nv_bfloat16*)H, m, n, rp, scales, off2, nb2);
   return cudaGetLastError();
 }
