@@ -362,7 +362,8 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   plan.take<uint64_t>(nnz); plan.take<uint64_t>(nnz);                          // keys
   plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz);                          // idx
   plan.take<uint32_t>(nnz);                                                    // pos
-  plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz); plan.take<double>(nnz);  // merged
+  plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz); plan.take<uint32_t>(nnz);  // merged
+  plan.take<uint64_t>(nnz);                                                    // layout keys
   plan.take<unsigned long long>(1);
   plan.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
   if (plan.off > c->scratch_bytes) {
@@ -380,14 +381,18 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   uint32_t* pos = cv.take<uint32_t>(nnz);
   uint32_t* urow = cv.take<uint32_t>(nnz);
   uint32_t* ucol = cv.take<uint32_t>(nnz);
-  double* uval = cv.take<double>(nnz);
+  uint32_t* head_at = cv.take<uint32_t>(nnz);
+  uint64_t* lkeys = cv.take<uint64_t>(nnz);
   unsigned long long* d_bad = cv.take<unsigned long long>(1);
   void* tmp = cv.take<char>(std::max({sort_bytes, sort2_bytes, scan_bytes}));
 
   // The coordinates are copied first; the values (half the bytes) follow on
-  // a side stream while the keys are built and sorted, and are waited for
-  // only where the merge needs them.  The guard waits for that copy on every
-  // exit, so no copy outlives the call (the caller may free its arrays).
+  // a side stream while everything that needs only the coordinates runs --
+  // keys, both sorts, duplicate runs, block pointers, the in-block layout,
+  // the final coordinates and the counts -- and are waited for only by the
+  // last step, which sums each record's run of values into place.  The guard
+  // waits for that copy on every exit, so no copy outlives the call (the
+  // caller may free its arrays).
   struct SideGuard {
     cudaStream_t s = nullptr;
     ~SideGuard() {
@@ -439,30 +444,27 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   check_cuda(cudaStreamSynchronize(st), "sync");
   const uint64_t u = (uint64_t)last_pos + last_flag;
 
-  if (vals_on_side) check_cuda(cudaStreamWaitEvent(st, c->ev_vals, 0), "wait values");
-  check_cuda(launch_merge_runs(g, skeys, sidx, pos, nnz, t_vals, t_rows, t_cols, okeys, urow,
-                               ucol, uval, st), "merge_runs");
+  // duplicate runs -> one record each (key, coordinates, where its run starts)
   uint64_t* ukeys = okeys;
+  check_cuda(launch_merge_keys(skeys, sidx, pos, nnz, t_rows, t_cols, ukeys, urow, ucol, head_at,
+                               st), "merge_keys");
   check_cuda(launch_block_ptr(ukeys, u, span, nblocks, M.block_ptr, st), "block_ptr");
 
   reserve_records(M, u, as_double);
+  const uint32_t* perm = nullptr;  // final record k = merged record perm[k]
   if (shuffled) {
     // in-block layout: key = (block, 32-bit hash(layout_seed, k)), or
-    // (block, local column | local row, hash) for runs
-    uint64_t* k2 = skeys;  // free now
-    uint32_t* i2 = sidx;
-    check_cuda(launch_shuffle_keys(ukeys, u, span, nB, c->layout_key, c->cfg.layout_seed, k2,
-                                   i2, st), "shuffle");
-    cub::DoubleBuffer<uint64_t> kb2(k2, ukeys);
-    cub::DoubleBuffer<uint32_t> vb2(i2, flags);
+    // (block, local column | local row, hash) for runs; the sorted keys and
+    // indices of the first sort stay for the values
+    check_cuda(launch_shuffle_keys(ukeys, u, span, nB, c->layout_key, c->cfg.layout_seed, lkeys,
+                                   pos, st), "shuffle");
+    cub::DoubleBuffer<uint64_t> kb2(lkeys, ukeys);
+    cub::DoubleBuffer<uint32_t> vb2(pos, flags);
     check_cuda(cub::DeviceRadixSort::SortPairs(tmp, sort2_bytes, kb2, vb2, (int)u, 0,
                                                shuffle_bits, st), "sort");
-    check_cuda(launch_gather_records(vb2.Current(), u, urow, ucol, uval, M.row, M.col, M.val,
-                                     as_double, st), "gather");
-  } else {
-    check_cuda(launch_gather_records(nullptr, u, urow, ucol, uval, M.row, M.col, M.val,
-                                     as_double, st), "gather");
+    perm = vb2.Current();
   }
+  check_cuda(launch_gather_coords(perm, u, urow, ucol, M.row, M.col, st), "gather");
   check_cuda(cudaMemcpyAsync(M.h_block_ptr.data(), M.block_ptr, (nblocks + 1) * 8,
                              cudaMemcpyDeviceToHost, st), "D2H block_ptr");
   if (which == DSGDPP_TRAIN) {
@@ -474,6 +476,9 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
       check_cuda(launch_inverse_counts(c->cnt2, c->cfg.n, c->inv2, as_double, st), "inv2");
     }
   }
+  if (vals_on_side) check_cuda(cudaStreamWaitEvent(st, c->ev_vals, 0), "wait values");
+  check_cuda(launch_gather_values(perm, u, head_at, skeys, sidx, nnz, t_vals, M.val, as_double,
+                                  st), "gather values");
   check_cuda(cudaStreamSynchronize(st), "sync");
   M.nnz = u;
   M.present = true;

@@ -196,10 +196,10 @@ cudaError_t launch_make_keys(const BlockingGeom& g, const uint32_t* rows, const 
 cudaError_t launch_head_flags(const uint64_t* keys, uint64_t nnz, uint32_t* flags,
                               cudaStream_t st);
 // merges runs of equal keys (values summed in input order) into compact arrays
-cudaError_t launch_merge_runs(const BlockingGeom& g, const uint64_t* keys, const uint32_t* idx,
-                              const uint32_t* pos, uint64_t nnz, const double* vals_in,
-                              const uint32_t* rows_in, const uint32_t* cols_in, uint64_t* ukeys,
-                              uint32_t* urow, uint32_t* ucol, double* uval, cudaStream_t st);
+cudaError_t launch_merge_keys(const uint64_t* keys, const uint32_t* idx, const uint32_t* pos,
+                              uint64_t nnz, const uint32_t* rows_in, const uint32_t* cols_in,
+                              uint64_t* ukeys, uint32_t* urow, uint32_t* ucol, uint32_t* head_at,
+                              cudaStream_t st);
 cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
                              uint32_t nblocks, uint64_t* block_ptr, cudaStream_t st);
 // in-block layout keys of the Hogwild matrix: (block, hash) for a shuffled
@@ -208,9 +208,13 @@ enum LayoutKey : int { kLayoutShuffled = 0, kLayoutColRuns = 1, kLayoutRowRuns =
 cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
                                 uint64_t nB, int mode, uint64_t seed, uint64_t* keys2,
                                 uint32_t* idx2, cudaStream_t st);
-cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
-                                  const uint32_t* ucol, const double* uval, uint32_t* row,
-                                  uint32_t* col, void* val, int val_is_double, cudaStream_t st);
+cudaError_t launch_gather_coords(const uint32_t* perm, uint64_t u, const uint32_t* urow,
+                                 const uint32_t* ucol, uint32_t* row, uint32_t* col,
+                                 cudaStream_t st);
+cudaError_t launch_gather_values(const uint32_t* perm, uint64_t u, const uint32_t* head_at,
+                                 const uint64_t* keys, const uint32_t* idx, uint64_t nnz,
+                                 const double* vals_in, void* val, int val_is_double,
+                                 cudaStream_t st);
 // rows_out[k] = rows_in[k] + row0, cols_out[k] = cols_in[k] + col0
 cudaError_t launch_offset_copy(const uint32_t* rows_in, const uint32_t* cols_in, uint64_t nnz,
                                uint32_t row0, uint32_t col0, uint32_t* rows_out,

@@ -54,21 +54,21 @@ __global__ void head_flags_kernel(const uint64_t* keys, uint64_t nnz, uint32_t* 
     flags[k] = (k == 0 || keys[k] != keys[k - 1]) ? 1u : 0u;
 }
 
-__global__ void merge_runs_kernel(BlockingGeom g, const uint64_t* keys, const uint32_t* idx,
-                                  const uint32_t* pos, uint64_t nnz, const double* vals_in,
-                                  const uint32_t* rows_in, const uint32_t* cols_in,
+// Runs of equal keys in the sorted order -> one record each, in run order:
+// its key, its coordinates and the sorted position where the run starts (the
+// values are summed later, once they have arrived: gather_values_kernel).
+__global__ void merge_keys_kernel(const uint64_t* keys, const uint32_t* idx, const uint32_t* pos,
+                                  uint64_t nnz, const uint32_t* rows_in, const uint32_t* cols_in,
                                   uint64_t* ukeys, uint32_t* urow, uint32_t* ucol,
-                                  double* uval) {
+                                  uint32_t* head_at) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz; k += stride) {
     if (!(k == 0 || keys[k] != keys[k - 1])) continue;
     const uint64_t o = pos[k];
-    double v = vals_in[idx[k]];
-    for (uint64_t q = k + 1; q < nnz && keys[q] == keys[k]; ++q) v += vals_in[idx[q]];
     ukeys[o] = keys[k];
     urow[o] = rows_in[idx[k]];
     ucol[o] = cols_in[idx[k]];
-    uval[o] = v;
+    head_at[o] = (uint32_t)k;
   }
 }
 
@@ -113,16 +113,30 @@ __global__ void shuffle_keys_kernel(const uint64_t* ukeys, uint64_t u, uint64_t 
   }
 }
 
-__global__ void gather_records_kernel(const uint32_t* idx, uint64_t u, const uint32_t* urow,
-                                      const uint32_t* ucol, const double* uval, uint32_t* row,
-                                      uint32_t* col, void* val, int val_is_double) {
+// Record k of the final order is merged record perm[k] (k without perm).
+__global__ void gather_coords_kernel(const uint32_t* perm, uint64_t u, const uint32_t* urow,
+                                     const uint32_t* ucol, uint32_t* row, uint32_t* col) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
-    const uint32_t q = idx ? idx[k] : (uint32_t)k;
+    const uint32_t q = perm ? perm[k] : (uint32_t)k;
     row[k] = urow[q];
     col[k] = ucol[q];
-    if (val_is_double) reinterpret_cast<double*>(val)[k] = uval[q];
-    else reinterpret_cast<float*>(val)[k] = (float)uval[q];
+  }
+}
+
+// The value of record k: the sum of its run's values in sorted (stable, so
+// input) order, as ReadMatrixBlocksMm's coordinate sort sums duplicates.
+__global__ void gather_values_kernel(const uint32_t* perm, uint64_t u, const uint32_t* head_at,
+                                     const uint64_t* keys, const uint32_t* idx, uint64_t nnz,
+                                     const double* vals_in, void* val, int val_is_double) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < u; k += stride) {
+    const uint32_t q = perm ? perm[k] : (uint32_t)k;
+    const uint64_t s = head_at[q];
+    double v = vals_in[idx[s]];
+    for (uint64_t t = s + 1; t < nnz && keys[t] == keys[s]; ++t) v += vals_in[idx[t]];
+    if (val_is_double) reinterpret_cast<double*>(val)[k] = v;
+    else reinterpret_cast<float*>(val)[k] = (float)v;
   }
 }
 
@@ -233,13 +247,13 @@ cudaError_t launch_head_flags(const uint64_t* keys, uint64_t nnz, uint32_t* flag
   return cudaGetLastError();
 }
 
-cudaError_t launch_merge_runs(const BlockingGeom& g, const uint64_t* keys, const uint32_t* idx,
-                              const uint32_t* pos, uint64_t nnz, const double* vals_in,
-                              const uint32_t* rows_in, const uint32_t* cols_in, uint64_t* ukeys,
-                              uint32_t* urow, uint32_t* ucol, double* uval, cudaStream_t st) {
+cudaError_t launch_merge_keys(const uint64_t* keys, const uint32_t* idx, const uint32_t* pos,
+                              uint64_t nnz, const uint32_t* rows_in, const uint32_t* cols_in,
+                              uint64_t* ukeys, uint32_t* urow, uint32_t* ucol, uint32_t* head_at,
+                              cudaStream_t st) {
   if (nnz == 0) return cudaSuccess;
-  merge_runs_kernel<<<kGrid, 256, 0, st>>>(g, keys, idx, pos, nnz, vals_in, rows_in, cols_in,
-                                           ukeys, urow, ucol, uval);
+  merge_keys_kernel<<<kGrid, 256, 0, st>>>(keys, idx, pos, nnz, rows_in, cols_in, ukeys, urow,
+                                           ucol, head_at);
   return cudaGetLastError();
 }
 
@@ -262,12 +276,21 @@ cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t bloc
   return cudaGetLastError();
 }
 
-cudaError_t launch_gather_records(const uint32_t* idx, uint64_t u, const uint32_t* urow,
-                                  const uint32_t* ucol, const double* uval, uint32_t* row,
-                                  uint32_t* col, void* val, int val_is_double, cudaStream_t st) {
+cudaError_t launch_gather_coords(const uint32_t* perm, uint64_t u, const uint32_t* urow,
+                                 const uint32_t* ucol, uint32_t* row, uint32_t* col,
+                                 cudaStream_t st) {
   if (u == 0) return cudaSuccess;
-  gather_records_kernel<<<kGrid, 256, 0, st>>>(idx, u, urow, ucol, uval, row, col, val,
-                                               val_is_double);
+  gather_coords_kernel<<<kGrid, 256, 0, st>>>(perm, u, urow, ucol, row, col);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_values(const uint32_t* perm, uint64_t u, const uint32_t* head_at,
+                                 const uint64_t* keys, const uint32_t* idx, uint64_t nnz,
+                                 const double* vals_in, void* val, int val_is_double,
+                                 cudaStream_t st) {
+  if (u == 0) return cudaSuccess;
+  gather_values_kernel<<<kGrid, 256, 0, st>>>(perm, u, head_at, keys, idx, nnz, vals_in, val,
+                                              val_is_double);
   return cudaGetLastError();
 }
 
