@@ -607,8 +607,9 @@ void enqueue_hogwild_epoch(dsgdpp_ctx* c, uint32_t s0, uint32_t s1) {
   }
   for (uint32_t s = s0; s < s1 && !persistent; ++s) {
     if (prof) check_cuda(cudaEventRecord(c->prof_ev[s], st), "event");
-    check_cuda(launch_hogwild(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st),
-               "hogwild_subepoch");
+    // launches back to back (no timing event between) overlap start and end
+    check_cuda(launch_hogwild(c->cfg.precision, c->lanes, c->vecs, a, s, c->grid, st,
+                              s > s0 && !prof), "hogwild_subepoch");
   }
   if (prof && !persistent) check_cuda(cudaEventRecord(c->prof_ev[d2], st), "event");
   if (l2 && s1 == d2)

@@ -110,8 +110,13 @@ constexpr int hogwild_cta_scale(int precision, uint32_t lanes) {
 
 // ---- launchers (return cudaError_t) -------------------------------------------
 cudaError_t launch_build_segments(const SegBuildArgs& a, cudaStream_t st);
+// after_subepoch: the launch directly follows the sub-epoch launch before it
+// in the stream (nothing in between), so its start may overlap that launch's
+// end (programmatic dependent launch; the kernel waits for the previous grid
+// before it touches a factor)
 cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
-                           uint32_t launch_index, uint32_t grid, cudaStream_t st);
+                           uint32_t launch_index, uint32_t grid, cudaStream_t st,
+                           bool after_subepoch = false);
 // CTAs per SM that the Hogwild kernel sustains for this configuration
 int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomic,
                         uint32_t smem_segs, bool runs);

@@ -368,6 +368,13 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
   using C = typename E::C;
   constexpr bool kSR = sizeof(T) == 2;
 
+  // Launched after another sub-epoch of the same epoch (programmatic
+  // dependent launch), this grid's CTAs take the SM slots the previous
+  // grid's CTAs free as they finish, stage the segment table and their first
+  // chunk's entries -- none of which that grid writes -- and wait for it to
+  // complete (griddepcontrol.wait) before they touch a factor.  Otherwise the
+  // wait returns at once.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const LaunchDesc ld = a.launches[li];
   const Segment* gseg = a.segs + ld.seg_begin;
   const uint32_t nseg = ld.nseg;
@@ -439,6 +446,7 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
       my_ib = inv2[my_col];
     }
   }
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // the previous sub-epoch is complete
   for (;;) {
     // the next chunk's entries travel while this chunk is updated
     const uint32_t nlc = lc + stride;
@@ -955,15 +963,27 @@ int hogwild_ctas_per_sm(int precision, uint32_t lanes, uint32_t vecs, bool atomi
 }
 
 cudaError_t launch_hogwild(int precision, uint32_t lanes, uint32_t vecs, const HogwildArgs& a,
-                           uint32_t launch_index, uint32_t grid, cudaStream_t st) {
+                           uint32_t launch_index, uint32_t grid, cudaStream_t st,
+                           bool after_subepoch) {
   void* fn = hogwild_kernel_ptr(precision, lanes, vecs, a.atomic != 0, a.smem_segs > 0,
                                 a.runs != 0);
   if (!fn) return cudaErrorInvalidValue;
   HogwildArgs args = a;
   uint32_t li = launch_index;
   void* params[] = {&args, &li};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(hogwild_threads(precision, lanes)), params,
-                          sizeof(Segment) * a.smem_segs, st);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(hogwild_threads(precision, lanes));
+  cfg.dynamicSmemBytes = sizeof(Segment) * a.smem_segs;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  if (after_subepoch) {  // overlap this launch's start with the previous one's end
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  return cudaLaunchKernelExC(&cfg, fn, params);
 }
 
 cudaError_t launch_replay_subepoch(const ReplayArgs& a, uint32_t s, cudaStream_t st) {
