@@ -738,7 +738,10 @@ def main():
                 "lanes_per_nnz": l16, "vecs_per_lane": v16, "grid": g16,
                 "roofline": {"bound": "hbm", "achieved": ach16, "peak": hbm, "unit": "GB/s",
                              "frac": ach16 / hbm, "bytes_per_update": bpu16,
-                             "avg_launch_us": k16 * 1e3 / max(kl16, 1)}}
+                             "avg_launch_us": k16 * 1e3 / max(kl16, 1),
+                             "achieved_epoch": nnz * bpu16 / (sum(ms16) / len(ms16) / 1e3) / 1e9,
+                             "frac_epoch": nnz * bpu16 / (sum(ms16) / len(ms16) / 1e3) / 1e9
+                             / hbm}}
 
     # ---- time to target test RMSE: BF16 + learned controller vs plain FP32 ----
     ttt = None
@@ -774,7 +777,12 @@ def main():
                          "timing": ("CUDA events around each one-launch epoch of 2 epochs"
                                     if args.launch == "persistent" else
                                     "CUDA events around each sub-epoch launch of 2 epochs "
-                                    "launched on the library stream (not from the graph)")},
+                                    "launched on the library stream (not from the graph; "
+                                    "the events keep the launches from overlapping)"),
+                         # the timed epochs themselves: the epoch's algorithmic bytes over
+                         # its device time, every kernel of the epoch included
+                         "achieved_epoch": nnz * bpu / (t_dev / args.steps) / 1e9,
+                         "frac_epoch": nnz * bpu / (t_dev / args.steps) / 1e9 / hbm},
             "cpu_baseline": cpu,
             "test_rmse_vs_fp64_oracle": vs_oracle,
             "bf16_factors": bf16,
