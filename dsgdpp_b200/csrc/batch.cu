@@ -489,9 +489,9 @@ void enqueue_epoch(dsgdpp_batch* b) {
     a.update = b->cfg.update; a.truncate = 0; a.sgd_order = b->cfg.sgd_order;
     a.atomic = b->cfg.write_mode != DSGDPP_WRITE_STORE;
     a.lambda = b->cfg.update_lambda;
-    for (uint32_t s = 0; s < G.nlaunch; ++s)
-      check_cuda(launch_hogwild(b->cfg.precision, G.lanes, G.vecs, a, G.launch0 + s, G.grid, st),
-                 "batched hogwild");
+    for (uint32_t s = 0; s < G.nlaunch; ++s)  // a group's launches overlap start and end
+      check_cuda(launch_hogwild(b->cfg.precision, G.lanes, G.vecs, a, G.launch0 + s, G.grid, st,
+                                s > 0), "batched hogwild");
     if (l2)
       check_cuda(launch_scale_rows(b->cfg.precision, G.W, G.wrows, G.H, G.hrows, G.rp, G.w_slot,
                                    G.h_slot, G.d_scales, st), "scales");
