@@ -81,25 +81,24 @@ __host__ __device__ inline Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
   return r;
 }
 
-// 32-bit finalizer of MurmurHash3 (Appleby): a bijection with full avalanche.
-__host__ __device__ inline uint32_t fmix32(uint32_t h) {
-  h ^= h >> 16;
-  h *= 0x85ebca6bu;
-  h ^= h >> 13;
-  h *= 0xc2b2ae35u;
-  h ^= h >> 16;
-  return h;
-}
-
 // Random bits of one stochastically rounded vector write: a Philox-4x32-10
-// block drawn once per chunk and lane (`base`) is expanded per write by
-// fmix32(word + tag * golden ratio), the tag distinct per record, vector and
-// side within the chunk -- 128 fresh bits per vector for two multiplies per
-// word instead of a 10-round Philox call.
+// block drawn once per chunk and lane (`base`) is expanded per write by one
+// multiply and xor-shift of (word xor tag * golden ratio), the tag distinct
+// per record, vector and side within the chunk.  For each tag the map is a
+// bijection of the uniform Philox word, so every write's bits are uniform;
+// the xor-shift folds the product's well-mixed high half into the low half
+// that rounds the lower value of each pair.  (MurmurHash3's 32-bit
+// finalizer per word -- two multiplies and three xor-shifts -- cost the
+// BF16 epochs 7-19%: C2 5.90 vs 5.50 ms, C3 16.1 vs 13.5 ms, C5 29.2 vs
+// 23.6 ms, at the same test RMSE.)
 __host__ __device__ inline Philox4 sr_expand(const Philox4& base, uint32_t tag) {
   Philox4 r;
+  const uint32_t tg = tag * 0x9E3779B9u;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) r.v[k] = fmix32(base.v[k] + tag * 0x9E3779B9u);
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t x = (base.v[k] ^ tg) * 0x85EBCA6Bu;
+    r.v[k] = x ^ (x >> 16);
+  }
   return r;
 }
 
