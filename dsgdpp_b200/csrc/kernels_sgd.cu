@@ -404,6 +404,18 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
     mulA = kPrimes[h & 7u] % total;
     addB = (h >> 8) % total;
   }
+  // position of chunk c of the list in the epoch's order: WR draws it, the
+  // affine order (WOR; SEQ with A = 1, B = 0) steps from c to c + stride by
+  // adding A * stride mod total, which saves a 64-bit remainder per chunk
+  // (C2 BF16 epoch 5.50 -> 5.25 ms).  The wide BF16 mappings (CTAs of 256
+  // threads at 64 registers) keep the remainder: their register allocation
+  // with the step measured 12% slower at rank 64.
+  const bool wr = a.sgd_order == 1 || HogwildLaunch<T, LPN, VPL>::kBig;
+  auto position = [&](uint32_t c) -> uint32_t {
+    return a.sgd_order == 1 ? (uint32_t)(mix64(h ^ ((uint64_t)c << 20)) % total)
+                            : (uint32_t)((mulA * c + addB) % total);
+  };
+  const uint32_t step = (uint32_t)((mulA * stride) % total);
   const C* inv1 = reinterpret_cast<const C*>(a.inv1);
   const C* inv2 = reinterpret_cast<const C*>(a.inv2);
   const C* vals = reinterpret_cast<const C*>(a.val);
@@ -413,13 +425,8 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t grp = lane / LPN, gl = lane % LPN;
 
-  // chunk c of the list -> its segment, first record and record count
-  auto locate = [&](uint32_t c, uint32_t& lo, uint64_t& rb, uint32_t& nrec) {
-    uint32_t pc;
-    if (a.sgd_order == 1)  // WR: chunks drawn with replacement
-      pc = (uint32_t)(mix64(h ^ ((uint64_t)c << 20)) % total);
-    else
-      pc = (uint32_t)((mulA * c + addB) % total);
+  // chunk at position pc -> its segment, first record and record count
+  auto locate = [&](uint32_t pc, uint32_t& lo, uint64_t& rb, uint32_t& nrec) {
     uint32_t l = 0, hi = nseg - 1;  // the last segment with chunk_begin <= pc
     while (l < hi) {
       const uint32_t mid = (l + hi + 1) >> 1;
@@ -434,7 +441,8 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
   // the chunk in hand: its entries, one per lane, and their inverse counts
   uint32_t lo, nrec;
   uint64_t rb;
-  locate(lc, lo, rb, nrec);
+  uint32_t pc = position(lc);
+  locate(pc, lo, rb, nrec);
   uint32_t my_row = 0, my_col = 0;
   C my_x = 0, my_ia = 0, my_ib = 0;
   if (lane < nrec) {
@@ -450,12 +458,13 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
   for (;;) {
     // the next chunk's entries travel while this chunk is updated
     const uint32_t nlc = lc + stride;
-    uint32_t nlo = 0, nnrec = 0;
+    uint32_t nlo = 0, nnrec = 0, npc = 0;
     uint64_t nrb = 0;
     uint32_t n_row = 0, n_col = 0;
     C n_x = 0;
     if (nlc < total) {
-      locate(nlc, nlo, nrb, nnrec);
+      npc = wr ? position(nlc) : (pc + step >= total ? pc + step - total : pc + step);
+      locate(npc, nlo, nrb, nnrec);
       if (lane < nnrec) {
         n_row = a.row[nrb + lane];
         n_col = a.col[nrb + lane];
@@ -495,6 +504,7 @@ __global__ void __launch_bounds__(HogwildLaunch<T, LPN, VPL>::threads,
       n_ib = inv2[n_col];
     }
     lc = nlc;
+    pc = npc;
     lo = nlo;
     rb = nrb;
     nrec = nnrec;
