@@ -341,9 +341,31 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
     return;
   }
 
+  // The blocking key (kernels.cuh: BlockingGeom).  For the Hogwild training
+  // records its position part is the in-block layout order, so the one sort
+  // both blocks and lays out the records; a key that would pass 64 bits keeps
+  // the plain positions and lays the records out with a second sort.
+  BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
+  g.stride = span;
+  bool layout_in_key = false;
+  if (shuffled) {
+    const int mode = c->layout_key;
+    const uint64_t permuted = mode == kLayoutColRuns ? mB : mode == kLayoutRowRuns ? nB : span;
+    const uint64_t major = mode == kLayoutColRuns ? nB : mode == kLayoutRowRuns ? mB : 1;
+    const int pb = bit_length(permuted - 1);
+    if (pb + bit_length(major) < 63 &&
+        (double)nblocks * (double)(major << pb) < 1.8e19) {
+      g.layout = mode;
+      g.pbits = pb;
+      g.stride = major << pb;
+      g.seed = c->cfg.layout_seed;
+      layout_in_key = true;
+    }
+  }
+
   // Scratch for the blocking: sized for nnz, kept by the context and reused
   // by later calls (a matrix of the same size allocates nothing).
-  const int end_bit = bit_length((uint64_t)nblocks * span - 1);
+  const int end_bit = bit_length((uint64_t)nblocks * g.stride - 1);
   const int blk_bits = bit_length((uint64_t)nblocks - 1);
   const int shuffle_bits = 32 + blk_bits;  // (block, 32-bit hash) layout keys
   size_t sort_bytes = 0, sort2_bytes = 0, scan_bytes = 0;
@@ -388,8 +410,9 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
 
   // The coordinates are copied first; the values (half the bytes) follow on
   // a side stream while everything that needs only the coordinates runs --
-  // keys, both sorts, duplicate runs, block pointers, the in-block layout,
-  // the final coordinates and the counts -- and are waited for only by the
+  // keys, the sort, duplicate runs, block pointers, the in-block layout (on
+  // the key, or a second sort), the final coordinates and the counts -- and
+  // are waited for only by the
   // last step, which sums each record's run of values into place.  The guard
   // waits for that copy on every exit, so no copy outlives the call (the
   // caller may free its arrays).
@@ -418,7 +441,6 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
     vals_on_side = true;
   }
   check_cuda(cudaMemsetAsync(d_bad, 0, 8, st), "memset");
-  BlockingGeom g{c->cfg.m, c->cfg.n, d, d2, mB, nB, c->d_off1, c->d_off2};
   check_cuda(launch_make_keys(g, t_rows, t_cols, nnz, keys[0], idx[0], d_bad, st), "make_keys");
   unsigned long long bad = 0;
   check_cuda(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, st), "D2H");
@@ -448,11 +470,11 @@ void set_matrix_impl(dsgdpp_ctx* c, int which, uint64_t nnz, const uint32_t* row
   uint64_t* ukeys = okeys;
   check_cuda(launch_merge_keys(skeys, sidx, pos, nnz, t_rows, t_cols, ukeys, urow, ucol, head_at,
                                st), "merge_keys");
-  check_cuda(launch_block_ptr(ukeys, u, span, nblocks, M.block_ptr, st), "block_ptr");
+  check_cuda(launch_block_ptr(ukeys, u, g.stride, nblocks, M.block_ptr, st), "block_ptr");
 
   reserve_records(M, u, as_double);
   const uint32_t* perm = nullptr;  // final record k = merged record perm[k]
-  if (shuffled) {
+  if (shuffled && !layout_in_key) {
     // in-block layout: key = (block, 32-bit hash(layout_seed, k)), or
     // (block, local column | local row, hash) for runs; the sorted keys and
     // indices of the first sort stay for the values

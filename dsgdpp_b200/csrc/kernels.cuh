@@ -188,12 +188,26 @@ cudaError_t launch_adam(float* P, const float* g, float* m, float* v, float lr, 
                         float b2, float eps, int step, cudaStream_t st);
 
 // ---- data preparation -----------------------------------------------------------
+// The blocking key of an entry is block * stride + its position in the block.
+// The position is local row * nB + local column (the reference's (i, j) order
+// within a block; stride = mB * nB), or, for the Hogwild training records, the
+// in-block layout order itself: (local column, keyed permutation of the local
+// row) for column runs, (local row, permuted local column) for row runs, a
+// permutation of local row * nB + local column for the shuffled layout, the
+// permuted part `pbits` wide.  A permutation keeps one position per (i, j), so
+// duplicate entries still meet, and the one sort both blocks the entries and
+// lays them out.
+constexpr int kKeyPlain = -1;
 struct BlockingGeom {
   uint64_t m, n;
   uint32_t nb1, nb2;      // d, 2d
   uint64_t mB, nB;        // largest block extent in rows / columns
   const uint64_t* off1;   // nb1+1 (last = m)
   const uint64_t* off2;   // nb2+1 (last = n)
+  uint64_t stride = 0;    // key distance between consecutive blocks
+  int layout = kKeyPlain;  // kKeyPlain or a LayoutKey
+  int pbits = 0;           // width of the permuted part of the position
+  uint64_t seed = 0;       // layout seed (the permutation's key)
 };
 cudaError_t launch_make_keys(const BlockingGeom& g, const uint32_t* rows, const uint32_t* cols,
                              uint64_t nnz, uint64_t* keys, uint32_t* idx,
@@ -207,8 +221,10 @@ cudaError_t launch_merge_keys(const uint64_t* keys, const uint32_t* idx, const u
                               cudaStream_t st);
 cudaError_t launch_block_ptr(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
                              uint32_t nblocks, uint64_t* block_ptr, cudaStream_t st);
-// in-block layout keys of the Hogwild matrix: (block, hash) for a shuffled
-// layout; (block, local column, hash) or (block, local row, hash) for runs
+// in-block layout keys of the Hogwild matrix for a second sort, when the
+// layout cannot ride on the blocking key (more than 64 key bits): (block,
+// hash) for a shuffled layout; (block, local column, hash) or (block, local
+// row, hash) for runs
 enum LayoutKey : int { kLayoutShuffled = 0, kLayoutColRuns = 1, kLayoutRowRuns = 2 };
 cudaError_t launch_shuffle_keys(const uint64_t* ukeys, uint64_t u, uint64_t block_span,
                                 uint64_t nB, int mode, uint64_t seed, uint64_t* keys2,

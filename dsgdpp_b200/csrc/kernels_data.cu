@@ -5,8 +5,10 @@
 // coordinates; coordinate_matrix::sort (read_impl.h:162-164) orders each block
 // by (i, j) and sums duplicate entries.  Here the entries arrive as one
 // global COO array and are blocked on the GPU: a 64-bit key
-// (block, local row, local column) is radix-sorted stably, runs of equal keys
-// are merged, and block boundaries are found by binary search.
+// (block, local row, local column) -- for the Hogwild training records
+// (block, position in the in-block layout), a permutation of the same
+// positions -- is radix-sorted stably, runs of equal keys are merged, and
+// block boundaries are found by binary search.
 #include <algorithm>
 
 #include "kernels.cuh"
@@ -21,6 +23,31 @@ __device__ __forceinline__ uint32_t find_block(const uint64_t* off, uint32_t nb,
     if (off[mid] <= x) lo = mid; else hi = mid - 1;
   }
   return lo;
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// A keyed permutation of [0, 2^b): xor with the key, then three rounds of a
+// multiply by an odd constant and a xor-shift by half the width, all modulo
+// 2^b -- each step is invertible on b-bit values, so distinct positions keep
+// distinct images.
+__device__ __forceinline__ uint64_t permute_bits(uint64_t x, int b, uint64_t key) {
+  if (b == 0) return 0;
+  const uint64_t mask = b >= 64 ? ~0ull : (1ull << b) - 1;
+  const int s = (b + 1) / 2;
+  x = (x ^ key) & mask;
+  x = (x * 0x9E3779B97F4A7C15ull) & mask;
+  x ^= x >> s;
+  x = (x * ((key >> 1) | 1ull)) & mask;
+  x ^= x >> s;
+  x = (x * 0xBF58476D1CE4E5B9ull) & mask;
+  x ^= x >> s;
+  return x;
 }
 
 __global__ void make_keys_kernel(BlockingGeom g, const uint32_t* rows, const uint32_t* cols,
@@ -43,7 +70,17 @@ __global__ void make_keys_kernel(BlockingGeom g, const uint32_t* rows, const uin
     }
     const uint32_t b1 = find_block(o1, g.nb1, i), b2 = find_block(o2, g.nb2, j);
     const uint64_t blk = (uint64_t)b1 * g.nb2 + b2;
-    keys[k] = (blk * g.mB + (i - o1[b1])) * g.nB + (j - o2[b2]);
+    const uint64_t li = i - o1[b1], lj = j - o2[b2];
+    uint64_t pos;
+    if (g.layout == kLayoutColRuns)  // a column's records together, its rows permuted
+      pos = lj << g.pbits | permute_bits(li, g.pbits, mix64(g.seed ^ (j * 0xD6E8FEB86659FD93ull)));
+    else if (g.layout == kLayoutRowRuns)
+      pos = li << g.pbits | permute_bits(lj, g.pbits, mix64(g.seed ^ (i * 0xD6E8FEB86659FD93ull)));
+    else if (g.layout == kLayoutShuffled)
+      pos = permute_bits(li * g.nB + lj, g.pbits, mix64(g.seed));
+    else
+      pos = li * g.nB + lj;
+    keys[k] = blk * g.stride + pos;
     idx[k] = (uint32_t)k;
   }
 }
@@ -84,13 +121,6 @@ __global__ void block_ptr_kernel(const uint64_t* ukeys, uint64_t u, uint64_t spa
     if (ukeys[mid] < target) lo = mid + 1; else hi = mid;
   }
   ptr[b] = lo;
-}
-
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-  z += 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
 }
 
 // 32 low bits of the key: a hash of the record (shuffled), or the local

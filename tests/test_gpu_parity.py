@@ -204,6 +204,33 @@ def test_duplicates_are_summed():
         assert ctx.nzsl() == pytest.approx(ref.nzsl(), rel=LOSS_RTOL)
 
 
+@pytest.mark.parametrize("layout", ["shuffled", "col_runs", "row_runs"])
+def test_hogwild_layouts_block_and_merge_like_the_oracle(layout):
+    """Hogwild training records are blocked and laid out by one sort whose key
+    permutes the positions inside a block.  On a matrix where nearly every
+    position of every block holds one or more entries (uneven block extents,
+    so the permuted ranges are not powers of two), two positions sharing a key
+    would merge distinct entries: the block counts and the training loss must
+    still equal the oracle's, which merges exact duplicates only
+    (ReadMatrixBlocksMm's coordinate sort, mf/matrix/io/read_impl.h:162-164)."""
+    rng = np.random.default_rng(3)
+    m, n, d, r = 203, 181, 3, 5
+    rows = rng.integers(0, m, 150000).astype(np.uint32)
+    cols = rng.integers(0, n, 150000).astype(np.uint32)
+    vals = rng.normal(0, 1, 150000)
+    W0 = rng.uniform(-0.5, 0.5, (m, r))
+    H0 = rng.uniform(-0.5, 0.5, (n, r))
+    ref = O.Problem(m, n, r, d, rows, cols, vals).configure()
+    ref.set_factors(W0, H0)
+    assert len(set(zip(rows.tolist(), cols.tolist()))) > 0.98 * m * n
+    cfg = P.Config(m=m, n=n, rank=r, d=d, precision="fp64", exec="hogwild", layout=layout)
+    with P.Context(cfg) as ctx:
+        ctx.set_matrix(P.TRAIN, rows, cols, vals)
+        ctx.set_factors(W0, H0)
+        np.testing.assert_array_equal(ctx.block_nnz(), ref.block_nnz())
+        assert ctx.nzsl() == pytest.approx(ref.nzsl(), rel=LOSS_RTOL)
+
+
 def test_run_trace_matches_oracle():
     p = _problem(m=800, n=600, nnz=10000, ntest=1000)
     ref, ctx = _pair(p, 10, 2)
