@@ -82,7 +82,7 @@ typedef struct dsgdpp_ctx dsgdpp_ctx;
 #define DSGDPP_METHOD_DSGDPP 0 /* d x 2d blocks, 2d sub-epochs (mf/sgd/dsgdpp_impl.h)        */
 #define DSGDPP_METHOD_DSGD 1   /* d x d blocks, d sub-epochs (mf/sgd/dsgd_impl.h:80-234,328-350) */
 /* order of the Hogwild training records inside each block */
-#define DSGDPP_LAYOUT_SHUFFLED 0 /* random order (hash of layout_seed and the record) */
+#define DSGDPP_LAYOUT_SHUFFLED 0 /* random order (a permutation keyed by layout_seed) */
 #define DSGDPP_LAYOUT_COL_RUNS 1 /* by column, random within a column: runs of one H row */
 #define DSGDPP_LAYOUT_ROW_RUNS 2 /* by row, random within a row: runs of one W row */
 #define DSGDPP_LAYOUT_RUNS 3     /* COL_RUNS when n <= m (more records per column), else ROW_RUNS */
