@@ -408,10 +408,12 @@ int run(Args& args, const Job& job) {
     Wf.size1 = info_f[0]; Wf.size2 = info_f[2];
     Hf.size1 = info_f[2]; Hf.size2 = info_f[1];
   } else {
-    Log::info("mf", "File '" + args.inputRowFacFile + "' is not blocked; it will be blocked automatically");
-    Wf = read_mm_array(args.inputRowFacFile);
-    Log::info("mf", "File '" + args.inputColFacFile + "' is not blocked; it will be blocked automatically");
-    Hf = read_mm_array(args.inputColFacFile);
+    // .mma, or the .xml of .mma blocks that mfdblock writes for a dense matrix
+    for (const std::string* f : {&args.inputRowFacFile, &args.inputColFacFile})
+      if (!ends_with(*f, ".xml"))
+        Log::info("mf", "File '" + *f + "' is not blocked; it will be blocked automatically");
+    Wf = read_dense(args.inputRowFacFile);
+    Hf = read_dense(args.inputColFacFile);
   }
   Log::info("mf", "Row factor matrix: " + std::to_string(Wf.size1) + " x " +
                       std::to_string(Wf.size2) + ", " + std::to_string(d) + " x 1 blocks");

@@ -563,6 +563,32 @@ Coo read_sparse(const std::string& path, BlockedDescriptor* desc_out) {
   return all;
 }
 
+Dense read_dense(const std::string& path) {
+  if (!ends_with(path, ".xml")) return read_mm_array(path);
+  const BlockedDescriptor d = read_descriptor(path);
+  if (d.format != "mma") throw MmError("blocked dense files must be in mma format: " + path);
+  Dense all;
+  all.size1 = d.size1;
+  all.size2 = d.size2;
+  all.colmajor.assign(d.size1 * d.size2, 0.0);
+  for (uint64_t b1 = 0; b1 < d.blocks1; ++b1)
+    for (uint64_t b2 = 0; b2 < d.blocks2; ++b2) {
+      const std::string f = d.path + d.filenames[b1 * d.blocks2 + b2];
+      const Dense blk = read_mm_array(f);
+      const uint64_t r0 = d.offsets1[b1], c0 = d.offsets2[b2];
+      const uint64_t r1 = b1 + 1 < d.blocks1 ? d.offsets1[b1 + 1] : d.size1;
+      const uint64_t c1 = b2 + 1 < d.blocks2 ? d.offsets2[b2 + 1] : d.size2;
+      if (blk.size1 != r1 - r0 || blk.size2 != c1 - c0)
+        throw MmError("block " + f + " is " + std::to_string(blk.size1) + " x " +
+                      std::to_string(blk.size2) + ", the descriptor says " +
+                      std::to_string(r1 - r0) + " x " + std::to_string(c1 - c0));
+      for (uint64_t j = 0; j < blk.size2; ++j)
+        for (uint64_t i = 0; i < blk.size1; ++i)
+          all.colmajor[(c0 + j) * d.size1 + r0 + i] = blk.colmajor[j * blk.size1 + i];
+    }
+  return all;
+}
+
 }  // namespace dsgdpp
 
 // ---- C ABI of the file I/O (include/dsgdpp.h) ----------------------------------------
@@ -623,7 +649,7 @@ int dsgdpp_write_mm_coord(const char* path, uint64_t m, uint64_t n, uint64_t nnz
 
 int dsgdpp_read_mm_array(const char* path, uint64_t* m, uint64_t* n, double** colmajor) {
   return io_guard([&]() {
-    dsgdpp::Dense d = dsgdpp::read_mm_array(path);
+    dsgdpp::Dense d = dsgdpp::read_dense(path);
     *m = d.size1;
     *n = d.size2;
     *colmajor = copy_out(d.colmajor);

@@ -66,5 +66,8 @@ void write_descriptor(const std::string& path, const BlockedDescriptor& d);
 // A sparse matrix file: .mmc, or .xml whose blocks are .mmc files (block-local
 // coordinates are shifted by the block offsets to global ones).
 Coo read_sparse(const std::string& path, BlockedDescriptor* desc_out = nullptr);
+// A dense matrix file: .mma, or .xml whose blocks are .mma files (each block
+// placed at its offsets).
+Dense read_dense(const std::string& path);
 
 }  // namespace dsgdpp

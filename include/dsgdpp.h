@@ -490,7 +490,8 @@ int dsgdpp_read_sparse(const char* path, uint64_t* m, uint64_t* n, uint64_t* nnz
                        uint32_t** rows, uint32_t** cols, double** vals);
 int dsgdpp_write_mm_coord(const char* path, uint64_t m, uint64_t n, uint64_t nnz,
                           const uint32_t* rows, const uint32_t* cols, const double* vals);
-/* .mma: entries column by column */
+/* .mma (entries column by column), or an .xml descriptor of .mma blocks (each
+ * block placed at its offsets): the whole matrix, column by column */
 int dsgdpp_read_mm_array(const char* path, uint64_t* m, uint64_t* n, double** colmajor);
 int dsgdpp_write_mm_array(const char* path, uint64_t m, uint64_t n, const double* colmajor);
 /* the blocked form written by tools/mfdblock.cc: per-block .mmc files with

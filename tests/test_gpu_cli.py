@@ -70,6 +70,42 @@ def test_cli_replay_matches_oracle(tmp_path, blocked, tool):
         assert "Slow MapReduce implementation: 1" in r.stdout
 
 
+def test_cli_runs_on_mfdblock_output(tmp_path):
+    # the reference's pipeline: mfdblock blocks the data matrix d x 2d and the
+    # factors d x 1 / 1 x 2d (.xml descriptors with an empty path, so both
+    # tools run in the directory of the blocks); mfdsgdpp on those files gives
+    # the run on the plain files, up to the values' 16-digit rewrite
+    p = synth.make(400, 300, 6000, 600, rank_true=4, r=5, noise=0.1, seed=4)
+    _write(tmp_path, p)
+    d = 3
+    block = os.path.join(os.path.dirname(CLI), "mfdblock")
+    for args in (["--blocks1=3", "--blocks2=6", "train.mmc", "V"],
+                 ["--blocks1=3", "W.mma", "Wb"], ["--blocks2=6", "H.mma", "Hb"]):
+        r = subprocess.run([block] + args, cwd=str(tmp_path), capture_output=True, text=True,
+                           timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+    outs = {}
+    for tag, (v, w, h) in {"plain": ("train.mmc", "W.mma", "H.mma"),
+                           "blocked": ("V.xml", "Wb.xml", "Hb.xml")}.items():
+        r = subprocess.run([CLI, f"--input-file={v}", "--input-test-file=test.mmc",
+                            f"--input-row-file={w}", f"--input-col-file={h}", "--rank=5",
+                            f"--tasks-per-rank={d}", "--update=Nzsl_L2(1)", "--regularize=None",
+                            "--loss=Nzsl_L2(1)", "--decay=BoldDriver(0.01)", "--epochs=3",
+                            "--seed=7", "--precision=fp64", "--exec=replay",
+                            f"--output-row-file=W-{tag}.mma", f"--output-col-file=H-{tag}.mma"],
+                           cwd=str(tmp_path), capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        losses = [float(x) for x in re.findall(r"\| Loss: ([0-9.e+-]+)", r.stdout)]
+        outs[tag] = (losses, P.read_mm_array(str(tmp_path / f"W-{tag}.mma")),
+                     P.read_mm_array(str(tmp_path / f"H-{tag}.mma")))
+        if tag == "blocked":
+            for f in (v, w, h):
+                assert f"File '{f}' is not blocked" not in r.stdout
+    assert len(outs["plain"][0]) == 4
+    for a, b in zip(outs["plain"], outs["blocked"]):
+        np.testing.assert_allclose(np.asarray(b), np.asarray(a), rtol=1e-12, atol=1e-14)
+
+
 @pytest.mark.parametrize("tool", ["mfdsgdpp", "mfdsgd"])
 def test_cli_multirank_path_with_one_rank_matches_oracle(tmp_path, tool):
     # the tool's path for several ranks (task range, counts of the whole
