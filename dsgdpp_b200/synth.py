@@ -80,3 +80,58 @@ def make(m, n, nnz, nnz_test, rank_true, r, noise, seed, kind="uniform", s_row=1
     H0 = rng.uniform(-0.5, 0.5, (n, r))
     return Problem(m, n, rows[:nnz], cols[:nnz], vals[:nnz], rows[nnz:], cols[nnz:],
                    vals[nnz:], W0, H0)
+
+
+def quickstart(out_dir="/tmp/", size1=100000, size2=100000, nnz=1000000, nnz_test=100000,
+               r=10, seed=0):
+    """The four files of the reference's quick start, as tools/generateSyntheticData.cc
+    writes them (its sizes are the defaults here): truth factors W* (size1 x r)
+    and H* (r x size2) with N(0, 10) entries; train.mmc with `nnz` distinct
+    uniformly drawn cells, value w*_i . h*_j plus N(0, 1) noise; test.mmc with
+    `nnz_test` cells drawn apart, without noise; W.mma (size1 x r) and H.mma
+    (r x size2) with U[-0.5, 0.5] entries.  Cells are listed row by row, as
+    the reference's sequential sampling emits them.  The draws are this
+    module's own (seeded numpy), not the reference's generator: the same
+    shapes and distributions, not the same numbers."""
+    import os
+
+    import dsgdpp_b200 as P
+
+    if max(nnz, nnz_test) > size1 * size2:  # mf/matrix/op/generate.h:209-211
+        raise ValueError("nnz must be less than matrix size")
+    rng = np.random.default_rng(seed)
+    sigma = np.sqrt(10.0)
+    Ws = rng.normal(0.0, sigma, (size1, r))
+    Hs = rng.normal(0.0, sigma, (size2, r))
+
+    def cells(count):
+        keys = np.sort(_distinct_uniform(rng, size1, size2, count))
+        return (keys // np.uint64(size2)).astype(np.uint32), (keys % np.uint64(size2)).astype(np.uint32)
+
+    rows, cols = cells(nnz)
+    vals = np.einsum("ij,ij->i", Ws[rows], Hs[cols]) + rng.standard_normal(nnz)
+    trows, tcols = cells(nnz_test)
+    tvals = np.einsum("ij,ij->i", Ws[trows], Hs[tcols])
+    W0 = rng.uniform(-0.5, 0.5, (size1, r))
+    H0 = rng.uniform(-0.5, 0.5, (r, size2))
+    P.write_mm_coord(os.path.join(out_dir, "train.mmc"), size1, size2, rows, cols, vals)
+    P.write_mm_coord(os.path.join(out_dir, "test.mmc"), size1, size2, trows, tcols, tvals)
+    P.write_mm_array(os.path.join(out_dir, "W.mma"), W0)
+    P.write_mm_array(os.path.join(out_dir, "H.mma"), H0)
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(
+        description="write train.mmc, test.mmc, W.mma and H.mma as "
+                    "tools/generateSyntheticData.cc does (own seeded draws)")
+    ap.add_argument("--out-dir", default="/tmp/")
+    ap.add_argument("--size1", type=int, default=100000)
+    ap.add_argument("--size2", type=int, default=100000)
+    ap.add_argument("--nnz", type=int, default=1000000)
+    ap.add_argument("--nnz-test", type=int, default=100000)
+    ap.add_argument("--rank", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    quickstart(a.out_dir, a.size1, a.size2, a.nnz, a.nnz_test, a.rank, a.seed)

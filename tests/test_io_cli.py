@@ -225,3 +225,29 @@ def test_cli_rm_input_errors(tmp_path):
              f"--input-col-file={factors_only}", *base)
     assert r.returncode == 1 and "holds no data matrix" in r.stderr
     assert "generating data matrices on the fly" in r.stdout
+
+
+def test_quickstart_files_like_generate_synthetic_data(tmp_path):
+    # python -m dsgdpp_b200.synth writes the quick start's four files with the
+    # shapes and distributions of tools/generateSyntheticData.cc
+    import sys
+    r = subprocess.run([sys.executable, "-m", "dsgdpp_b200.synth", "--out-dir", str(tmp_path),
+                        "--size1", "300", "--size2", "200", "--nnz", "3000", "--nnz-test", "400",
+                        "--rank", "4", "--seed", "3"], cwd=ROOT, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    m, n, rows, cols, vals = P.read_sparse(str(tmp_path / "train.mmc"))
+    assert (m, n, len(vals)) == (300, 200, 3000)
+    keys = rows.astype(np.int64) * n + cols
+    assert np.all(np.diff(keys) > 0)  # distinct cells, row by row
+    assert 250 < vals.var() < 600  # 4 products of N(0, 10) entries, plus N(0, 1)
+    _, _, tr, tc, tv = P.read_sparse(str(tmp_path / "test.mmc"))
+    assert len(tv) == 400 and np.all(np.diff(tr.astype(np.int64) * n + tc) > 0)
+    W = P.read_mm_array(str(tmp_path / "W.mma"))
+    H = P.read_mm_array(str(tmp_path / "H.mma"))
+    assert W.shape == (300, 4) and H.shape == (4, 200)
+    assert np.abs(W).max() <= 0.5 and np.abs(H).max() <= 0.5
+    bad = subprocess.run([sys.executable, "-m", "dsgdpp_b200.synth", "--out-dir", str(tmp_path),
+                          "--size1", "3", "--size2", "3", "--nnz", "10"], cwd=ROOT,
+                         capture_output=True, text=True, timeout=300)
+    assert bad.returncode != 0 and "nnz must be less than matrix size" in bad.stderr
