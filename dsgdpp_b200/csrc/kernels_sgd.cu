@@ -730,22 +730,58 @@ __global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint
   const double em2 = __dmul_rn(eps, -2.0);
   const double f2 = __dmul_rn(__dmul_rn(eps, 2.0), a.lambda);
 
-  for (uint64_t q = 0; q < n; ++q) {
+  if (n == 0) return;
+  // The reads run ahead of the updates: the coordinates, value and counts of
+  // record q + 2 and the factor rows of record q + 1 are loaded while record q
+  // is updated.  Record q + 1 takes a row or column that record q writes from
+  // q's new values in registers (each lane reads back only the elements it
+  // writes itself, so rows written earlier are seen in program order); every
+  // update therefore reads the values the sequential order gives it, and the
+  // arithmetic below is the reference's, operation for operation.
+  struct Coord {
+    uint32_t i, j, c1, c2;
+    double x;
+  };
+  const bool counts = a.update == kUpdNzslL2;
+  auto load_coord = [&](uint64_t q) {
+    Coord e;
     const uint64_t rec = rb + pos[q];
-    const uint32_t i = a.row[rec], j = a.col[rec];
-    const double x = a.val[rec];
-    double* w = a.W + (size_t)i * a.rp;
-    double* h = a.H + (size_t)j * a.rp;
-    double wz[kReplayMaxK], hz[kReplayMaxK], pz[kReplayMaxK];
+    e.i = a.row[rec];
+    e.j = a.col[rec];
+    e.x = a.val[rec];
+    e.c1 = counts ? a.cnt1[e.i] : 1u;
+    e.c2 = counts ? a.cnt2[e.j] : 1u;
+    return e;
+  };
+  auto load_rows = [&](const Coord& e, double (&wz)[kReplayMaxK], double (&hz)[kReplayMaxK]) {
+    const double* w = a.W + (size_t)e.i * a.rp;
+    const double* h = a.H + (size_t)e.j * a.rp;
 #pragma unroll
     for (int k = 0; k < kReplayMaxK; ++k) {
       const uint32_t z = (uint32_t)k * 32 + lane;
-      wz[k] = 0; hz[k] = 0; pz[k] = 0;
+      wz[k] = 0;
+      hz[k] = 0;
       if (k < kmax && z < r) {
         wz[k] = w[z];
         hz[k] = h[z];
-        pz[k] = __dmul_rn(wz[k], hz[k]);
       }
+    }
+  };
+  Coord cur = load_coord(0);
+  Coord nxt = n > 1 ? load_coord(1) : cur;
+  double wz[kReplayMaxK], hz[kReplayMaxK];
+  load_rows(cur, wz, hz);
+
+#pragma unroll 1
+  for (uint64_t q = 0; q < n; ++q) {
+    const Coord after = q + 2 < n ? load_coord(q + 2) : nxt;
+    double nwz[kReplayMaxK], nhz[kReplayMaxK];
+    if (q + 1 < n) load_rows(nxt, nwz, nhz);
+    double pz[kReplayMaxK];
+#pragma unroll
+    for (int k = 0; k < kReplayMaxK; ++k) {
+      const uint32_t z = (uint32_t)k * 32 + lane;
+      pz[k] = (k < kmax && z < r) ? __dmul_rn(wz[k], hz[k]) : 0.0;
     }
     // wh = sum_z w[z] h[z] in z order (every lane computes the same sum)
     double wh = 0;
@@ -757,12 +793,14 @@ __global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint
         wh = __dadd_rn(wh, __shfl_sync(kFullMask, pz[k], l));
       }
     }
-    const double f1 = __dmul_rn(em2, __dsub_rn(x, wh));
+    const double f1 = __dmul_rn(em2, __dsub_rn(cur.x, wh));
     double f3 = 0, f4 = 0;
-    if (a.update == kUpdNzslL2) {
-      f3 = __ddiv_rn(1.0, (double)a.cnt1[i]);
-      f4 = __ddiv_rn(1.0, (double)a.cnt2[j]);
+    if (counts) {
+      f3 = __ddiv_rn(1.0, (double)cur.c1);
+      f4 = __ddiv_rn(1.0, (double)cur.c2);
     }
+    double* w = a.W + (size_t)cur.i * a.rp;
+    double* h = a.H + (size_t)cur.j * a.rp;
 #pragma unroll
     for (int k = 0; k < kReplayMaxK; ++k) {
       const uint32_t z = (uint32_t)k * 32 + lane;
@@ -787,8 +825,19 @@ __global__ void __launch_bounds__(128) replay_subepoch_kernel(ReplayArgs a, uint
       }
       w[z] = nw;
       h[z] = nh;
+      // record q + 1 on the same row or column reads these values
+      if (nxt.i == cur.i) nwz[k] = nw;
+      if (nxt.j == cur.j) nhz[k] = nh;
     }
     __syncwarp();
+    if (q + 1 == n) break;
+    cur = nxt;
+    nxt = after;
+#pragma unroll
+    for (int k = 0; k < kReplayMaxK; ++k) {
+      wz[k] = nwz[k];
+      hz[k] = nhz[k];
+    }
   }
 }
 
