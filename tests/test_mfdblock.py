@@ -129,3 +129,13 @@ def test_usage_and_errors(tmp_path, args, msg):
     r = _run(args, cwd=str(tmp_path))
     assert r.returncode == 1
     assert msg in r.stdout + r.stderr
+
+
+def test_dense_descriptor_with_a_wrong_block_is_rejected(tmp_path, monkeypatch):
+    W = np.arange(40, dtype=np.float64).reshape(8, 5)
+    P.write_mm_array(str(tmp_path / "W.mma"), W)
+    assert _run(["--blocks1=2", "W.mma", "Wb"], cwd=str(tmp_path)).returncode == 0
+    P.write_mm_array(str(tmp_path / "Wb-1-0.mma"), W[:3])  # the descriptor says 4 x 5
+    monkeypatch.chdir(tmp_path)
+    with pytest.raises(Exception, match="the descriptor says 4 x 5"):
+        P.read_mm_array("Wb.xml")
